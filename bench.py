@@ -1,0 +1,370 @@
+"""Benchmark of the B200 heliostat-field tracer: rays/s on the 1000-heliostat field.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload mid|small|large] [--impl b200|reference]
+
+One step = one pass of the hot path over one batch: aim the field for the
+step's sun position and rebuild the grid on the GPU, trace 2^28 rays (Buie
+sampling, shadow + block 3D-DDA, receiver deposition), scale the flux map and
+smooth the count map (trimmed mean).  Every step uses a fresh Philox stream
+and a slightly moved sun, so no output or geometry is reused.  Under torchrun
+each rank traces its own 2^28 rays (weak scaling) and the count/energy maps
+are summed across ranks with one NCCL all-reduce per step (the only exchange
+the path has).
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+FP64 oracle port, all host cores) on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "rays/s (shadow+block+hit)"
+UNIT = "rays/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="mid", choices=["small", "mid", "large"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the oracle sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ------------------------------------------------------------------ oracle
+def oracle_sample(w, seconds, threads=0):
+    """Time the FP64 oracle on ray ranges spread over the whole field."""
+    from oracle import oracle as O
+    sc = O.Scene(w.pos, w.size, w.sigma, w.receiver, w.grid.cell[0], w.grid.margin, list(w.sun.dir), aim=w.aim)
+    rpp = w.params.rays_per_point
+    total = int(w.params.rays)
+    xz, helio = O.points_poisson(w.size, total // rpp, w.params.point_spacing, w.params.seed)
+    weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
+    cores = threads or os.cpu_count()
+
+    def run(nranges, per):
+        starts = np.linspace(0, total - per, nranges).astype(np.int64)
+        st = np.zeros(7, np.uint64)
+        t0 = time.perf_counter()
+        for b in starts:
+            cfg = sc.cfg(w.sun.csr, w.params.seed, total, rpp, xz, helio, weight, threads=cores,
+                         ray_begin=int(b), ray_end=int(b) + per)
+            r = sc.trace_philox(cfg, records=False, maps=False)
+            st += np.array(r["stats"], np.uint64)
+        return time.perf_counter() - t0, st
+
+    dt, st = run(16, 4096)
+    rate = st[0] / dt
+    per = 8192
+    nr = int(max(16, min(4096, seconds * rate / per)))
+    dt, st = run(nr, per)
+    return {"rays_per_s": float(st[0] / dt), "rays": int(st[0]), "seconds": dt, "cores": cores,
+            "ranges": nr, "rays_per_range": per, "stats": [int(x) for x in st]}
+
+
+def flops_per_ray(stats):
+    """Algorithmic FP32 flops per ray of the reference algorithm: fixed per-ray
+    work 192, 30 per traversal set-up (one traversal for shadowed rays, two
+    otherwise), 54 per rectangle test and 4 per DDA cell step."""
+    rays, shadowed, rect, cells = stats[0], stats[1], stats[5], stats[6]
+    return 192.0 + 30.0 * (2.0 - shadowed / rays) + 54.0 * rect / rays + 4.0 * cells / rays
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu_id)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ arms
+def reference_arm(a, rank, world):
+    if rank != 0:
+        return
+    from onemirror_b200 import workloads as W
+    w = W.BUILDERS[a.workload]()
+    per_step = max(1.0, 60.0 / max(1, a.steps + a.warmup))
+    for _ in range(a.warmup):
+        oracle_sample(w, min(per_step, 2.0))
+    vals, rays, secs = [], 0, 0.0
+    for _ in range(a.steps):
+        r = oracle_sample(w, per_step)
+        vals.append(r["rays_per_s"])
+        rays += r["rays"]
+        secs += r["seconds"]
+    v = rays / secs
+    sample = ("%d ray ranges x %d rays spread over the %s field's %d rays per step (FP64 oracle, %d threads)"
+              % (r["ranges"], r["rays_per_range"], a.workload, int(w.params.rays), r["cores"]))
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * secs / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_name(w), "rays_per_step": int(w.params.rays)},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(w):
+    return {"small": "100 heliostats 2x2 m, flat 5x5 m receiver 128x128, 409600 rays",
+            "mid": "1000 heliostats 10x10 m to 600 m, flat 12x12 m receiver 256x256, 2^28 rays",
+            "large": "10000 heliostats 11x11 m to 1300 m, cylinder 8x18 m 512x256, 2^31 rays"}[w.name]
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def read_traffic(name):
+    """dram bytes per launch of the trace kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "trace_kernel_%s.md" % name)
+    try:
+        for ln in open(p):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def b200_arm(a, rank, world, local):
+    import torch
+    from onemirror_b200 import capi, workloads as W
+    from onemirror_b200.scene import SolarScene, image_smooth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    w = W.BUILDERS[a.workload]()
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    rays = int(p.rays)
+    base_az = 180.0
+
+    # FP32 issue-rate peak, measured live (best of 5 bursts)
+    sink = torch.zeros(8192, device=dev)
+    flops = C.c_double()
+    best = 0.0
+    for it in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        capi.check(capi.lib().qmcrt_fp32_peak_probe(C.c_void_p(sink.data_ptr()), 4096, C.byref(flops),
+                                                    C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        e1.record()
+        torch.cuda.synchronize()
+        if it:
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+
+    outs = sc._outputs(rays, False)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    def one(k, item, want_stats=False):
+        el, az = {"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload], base_az + 0.01 * k
+        sun = W.make_sun(el, az, w.sun.dni, w.sun.csr)
+        p.item = item
+        r = sc.trace(sun, p, stats=want_stats, outputs=outs)
+        sm = image_smooth(r["counts"], w.smooth_radius, w.smooth_ratio, capi.TRIM_SORTED)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(r["counts"])
+            dist.all_reduce(r["energy"])
+        return r, sm
+
+    for k in range(a.warmup):
+        one(k, 1000 + k)
+    r, _ = one(a.warmup, 5000, want_stats=True)
+    gst = r["stats"]
+    gpu_stats = [gst.rays, gst.shadowed, gst.blocked, gst.hit, gst.offmap, gst.rect_tests, gst.dda_cells]
+    torch.cuda.synchronize()
+
+    # timed region
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
+                       os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
+    clk.start()
+    time.sleep(0.3)
+    step_ms, kern_ms, setup_ms = [], [], []
+    for k in range(a.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        one(a.warmup + 1 + k, rank * 65536 + 1 + k)
+        e1.record()
+        t = sc.timing()
+        kern_ms.append(t.trace_kernel_ms)
+        setup_ms.append(t.setup_ms)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = clk.stop()
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = rays * world * a.steps / (total_ms * 1e-3)
+
+    # end to end through the host-buffer entry point (pinned host memory)
+    e2e = None
+    if a.e2e_steps > 0:
+        pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+               for k, v in (("pos", w.pos), ("size", w.size), ("aim", w.aim)) if v is not None}
+        counts = torch.zeros(w.res, dtype=torch.int32).pin_memory().numpy()
+        flux = torch.zeros(w.res, dtype=torch.float32).pin_memory().numpy()
+        f = capi.Field()
+        f.n = w.n
+        f.pos, f.size = capi.as_fp(pin["pos"]), capi.as_fp(pin["size"])
+        f.aim = capi.as_fp(pin["aim"]) if "aim" in pin else None
+        f.sigma = w.sigma
+        h2d = sum(v.nbytes for v in pin.values())
+        d2h = counts.nbytes + flux.nbytes
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for k in range(a.e2e_steps + 1):
+            if k == 1:
+                if world > 1:
+                    dist.barrier()
+                t0 = time.perf_counter()
+            sun = W.make_sun({"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload], base_az - 0.01 * (k + 1),
+                             w.sun.dni, w.sun.csr)
+            p.item = 900000 + k
+            capi.check(capi.lib().qmcrt_trace_host(sc.h, C.byref(f), C.byref(sun), C.byref(p),
+                                                   counts.ctypes.data_as(capi.u32p), capi.as_fp(flux), None, stream))
+        dt = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([dt], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            dt = float(tt.item())
+        e2e = {"value": rays * world * a.e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "call": "qmcrt_trace_host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        ob = oracle_sample(w, a.cpu_seconds)
+        cpu = {"value": ob["rays_per_s"], "unit": UNIT, "cores": ob["cores"], "kind": "port",
+               "sample": "%d ray ranges x %d rays spread over the field (%d rays, %.1f s), FP64 oracle"
+                         % (ob["ranges"], ob["rays_per_range"], ob["rays"], ob["seconds"])}
+        alg_stats = ob["stats"]
+        nbar_src = "oracle"
+    else:
+        alg_stats = gpu_stats
+        nbar_src = "gpu"
+    fpr = flops_per_ray(alg_stats)
+    kern_s = statistics.mean(kern_ms) * 1e-3
+    achieved = rays * fpr / kern_s / 1e12
+    traffic = read_traffic(a.workload)
+    peaks = measured_peaks()
+    roof = {"bound": "fp32", "achieved": achieved, "peak": best, "unit": "TFLOP/s", "frac": achieved / best,
+            "traffic": traffic, "kernel": "qm::trace_kernel", "kernel_ms": statistics.mean(kern_ms),
+            "peak_source": "measured live: FFMA chains (qmcrt_fp32_peak_probe), best of 5",
+            "flops_per_ray": fpr, "nbar_source": nbar_src,
+            "rect_tests_per_ray": alg_stats[5] / alg_stats[0], "dda_cells_per_ray": alg_stats[6] / alg_stats[0],
+            "gpu_rect_tests_per_ray": gpu_stats[5] / gpu_stats[0], "gpu_dda_cells_per_ray": gpu_stats[6] / gpu_stats[0],
+            "hbm_peak_gbs_of_measured": peaks.get("hbm_gbs")}
+    if traffic is not None:
+        roof["hbm_achieved_gbs"] = traffic / kern_s / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(w), "rays_per_step_per_gpu": rays, "heliostats": w.n,
+                       "parallelism": "ray shards per GPU + NCCL all-reduce of maps" if world > 1 else "1 GPU",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "step": "aim + grid build + trace + flux scaling + trimmed-mean smoothing"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 7 * a.steps,
+            "launches_per_step": {"aim": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "trace": 1,
+                                  "finalize": 1, "smooth": 1},
+            "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
+            "clocks": clocks,
+            "stats": {"shadowed": gst.shadowed / gst.rays, "blocked": gst.blocked / gst.rays,
+                      "hit": gst.hit / gst.rays, "intercept_ratio": gst.intercept_ratio}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_env()
+    if a.impl == "reference":
+        reference_arm(a, rank, world)
+        return
+    b200_arm(a, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

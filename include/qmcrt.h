@@ -1,0 +1,352 @@
+/*
+ * qmcrt.h — C-ABI of the B200 heliostat-field Monte Carlo ray tracer.
+ *
+ * Plain C, plain pointers and sizes, status-code returns, no exits.  Every
+ * entry point here replaces one call on the hot path of the reference
+ * (youxianru11/onemirror, Hu_smooth/ClassedSunRay); each declaration cites the
+ * reference interface it stands in for.
+ *
+ * Conventions
+ *  - World frame as in the reference driver (main.cpp:71-73): x = east,
+ *    y = up, z = south.  The sun direction is the INCIDENT direction (from the
+ *    sun toward the ground), as SunRay::sun_dir_ (sunray.h:41).
+ *  - A heliostat is a flat rectangle (RectangleHelio, heliostat.cuh:38-61):
+ *    size = (width along local x, thickness, height along local z); the mirror
+ *    plane sits at local y = thickness/2.
+ *  - Pointers named d_* are device pointers on the current device; h_* are
+ *    host pointers.  Everything else is host memory read during the call.
+ *  - Work is enqueued on the caller's `stream` (a cudaStream_t passed as
+ *    void*, NULL = legacy default stream).  Calls that return host values
+ *    synchronise that stream and say so.
+ *  - Errors: every call returns qmcrt_status; qmcrt_last_error() gives a
+ *    thread-local message for the last failure.  The reference exits the
+ *    process on any CUDA error (utils.h:13-22); this library never does.
+ */
+#ifndef QMCRT_H_
+#define QMCRT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QMCRT_ABI_VERSION 1
+
+typedef enum qmcrt_status {
+  QMCRT_OK = 0,
+  QMCRT_ERR_INVALID_ARGUMENT = 1, /* bad size, null pointer, out-of-range parameter */
+  QMCRT_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+  QMCRT_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
+  QMCRT_ERR_NOT_SUPPORTED = 4,    /* feature/receiver type not available */
+  QMCRT_ERR_TIMEOUT = 5,          /* a bounded device-side wait expired */
+  QMCRT_ERR_SAMPLING = 6,         /* Poisson-disk sampling could not place the requested points */
+  QMCRT_ERR_INTERNAL = 7
+} qmcrt_status;
+
+/* Reference behaviours that differ from the corrected method.  Each bit makes
+ * the tracer (and the oracle) reproduce one reference quirk exactly. */
+enum {
+  /* 3D-DDA steps before it tests, so the origin cell is never tested
+   * (rectgrid_raytracing.cu:70-114). */
+  QMCRT_QUIRK_SKIP_ORIGIN_CELL = 1u << 0,
+  /* Grid registration uses the cube of half-side sqrt(|size|)/2 around the
+   * heliostat centre (grid.cpp:55-59) instead of the rectangle's bounding box. */
+  QMCRT_QUIRK_AABB_RADIUS = 1u << 1,
+  /* The ray's own heliostat is not excluded; only t > 1e-6 rejects the
+   * self-hit (global_function.cuh:101-102). */
+  QMCRT_QUIRK_SELF_HIT = 1u << 2,
+  /* Table mode: the perturbation of point m uses the start offset of point
+   * max(m-1, 0) (rectgrid_raytracing.cu:183-184). */
+  QMCRT_QUIRK_PREV_PERTURB = 1u << 3,
+  /* local2world returns its input unchanged whenever the aligned normal is
+   * parallel to y, also for -y (global_function.cuh:29-30). */
+  QMCRT_QUIRK_ZENITH_FRAME = 1u << 4,
+  /* Pixel index int(u*res) without clamping: u == 1 lands one row/column past
+   * the map (rectgrid_raytracing.cu:144); such hits are counted, not written. */
+  QMCRT_QUIRK_PIXEL_EDGE = 1u << 5,
+  QMCRT_QUIRKS_REFERENCE = 0x3Fu
+};
+
+/* Receiver kinds (receiver.cuh:66-143). */
+enum { QMCRT_RECEIVER_FLAT = 0, QMCRT_RECEIVER_CYLINDER = 1 };
+
+/* Micro-heliostat sample point layouts (heliostat.cuh:6-10). */
+enum { QMCRT_POINTS_POISSON = 0, QMCRT_POINTS_GRID = 1 };
+
+/* Flux deposition: nearest pixel (reference) or bilinear (adjoint). */
+enum { QMCRT_DEPOSIT_NEAREST = 0, QMCRT_DEPOSIT_BILINEAR = 1 };
+
+/* Trimmed-mean definitions (image_smooth.cu:10-58). */
+enum {
+  QMCRT_TRIM_SORTED = 0, /* exact order statistics: drop the k lowest and k highest */
+  QMCRT_TRIM_HEAPS = 1   /* the reference's two-heap stream, else-if chain included */
+};
+
+/* Per-ray record flags (parity mode). */
+enum {
+  QMCRT_RAY_SHADOWED = 1u << 0, /* hit another heliostat on the way from the sun */
+  QMCRT_RAY_BLOCKED = 1u << 1,  /* reflected ray hit another heliostat */
+  QMCRT_RAY_HIT = 1u << 2,      /* reflected ray hit the receiver */
+  QMCRT_RAY_OFFMAP = 1u << 3    /* receiver hit whose pixel fell outside the map (quirk) */
+};
+
+/* Heliostat field, structure of arrays, n heliostats.
+ * Replaces vector<Heliostat*> (solar_scene.h:217) built by
+ * SceneFileProc::SceneFileRead (scene_file_proc.cpp:41-286). */
+typedef struct qmcrt_field {
+  int32_t n;
+  const float* pos;         /* [3n] mirror centre */
+  const float* size;        /* [3n] width, thickness, height */
+  const float* aim;         /* [3n] aim point; NULL: the receiver's focus centre */
+  const float* normal;      /* [3n] fixed normal (Heliostat::CRotate(dir), heliostat.cpp:23-28);
+                               NULL: aimed as the sun/target bisector (heliostat.cpp:51-58) */
+  const float* slope_sigma; /* [n] Gaussian slope error in rad; NULL: use `sigma` */
+  float sigma;              /* default slope error (common_var.cpp:18 uses 1 mrad) */
+  const float* tilt;        /* [2n] extra normal tilt (rad) about local x and z; NULL: none */
+} qmcrt_field;
+
+/* Receiver (RectangleReceiver receiver.cuh:66-101, receiver.cpp:24-118;
+ * CylinderReceiver receiver.cuh:103-122, a stub in the reference). */
+typedef struct qmcrt_receiver {
+  int32_t type;     /* QMCRT_RECEIVER_* */
+  float pos[3];     /* flat: box centre; cylinder: centre of the bottom circle */
+  float size[3];    /* flat: width (x), height (y), depth (z); cylinder: radius, height, unused */
+  float normal[3];  /* flat: facing direction, rotated about y only (receiver.cpp:85-97) */
+  int32_t face;     /* flat: face index 0..3 (receiver.cpp:30-83) */
+  int32_t res_x;    /* map columns (flat: along width; cylinder: around the circumference) */
+  int32_t res_y;    /* map rows (along height) */
+} qmcrt_receiver;
+
+/* Uniform grid over the field (RectGrid grid.h:25-48).  The bounds are taken
+ * from the field (plus `margin`) unless `explicit_bounds` is set. */
+typedef struct qmcrt_grid_params {
+  float cell[3];         /* cell size in m (RectGrid::interval_) */
+  float margin;          /* added around the field's bounding box, m */
+  int32_t explicit_bounds;
+  float origin[3];       /* used when explicit_bounds: RectGrid::pos_ */
+  float extent[3];       /* used when explicit_bounds: RectGrid::size_ */
+  int32_t fine_div;      /* >1: two-level grid, each coarse cell split into fine_div^3 */
+} qmcrt_grid_params;
+
+/* Sun (SunRay sunray.h:3-50). */
+typedef struct qmcrt_sun {
+  float dir[3]; /* incident direction, normalised inside (scene_instance_process.cu:8) */
+  float dni;    /* W/m^2 */
+  float csr;    /* circumsolar ratio of the Buie sunshape */
+} qmcrt_sun;
+
+/* What one trace does (replaces the per-heliostat loop of
+ * results_with_given_normal, Gtest.cu:10-63). */
+typedef struct qmcrt_trace_params {
+  uint64_t seed;           /* Philox key; every ray is a function of (seed, ray id) */
+  uint64_t rays;           /* total rays; must be a multiple of rays_per_point (Poisson) */
+  int32_t rays_per_point;  /* rays per micro-heliostat point (reference: 2048) */
+  int32_t point_mode;      /* QMCRT_POINTS_* */
+  float point_spacing;     /* Poisson: minimum spacing in m; GRID: pixel length in m */
+  float reflectivity;      /* rho (common_var.cpp:19 uses 0.88) */
+  uint32_t quirks;         /* QMCRT_QUIRK_* */
+  int32_t deposit;         /* QMCRT_DEPOSIT_* */
+  int32_t accumulate;      /* 0: zero the output maps first; 1: add into them */
+  int32_t kernel_variant;  /* 0: default (fastest); 1: plain global-atomic deposition; 2: no smem staging */
+  uint32_t item;           /* Philox stream (counter word 2): distinct items give independent ray sets
+                              (shards of one trace, items of a batch) */
+} qmcrt_trace_params;
+
+/* Device outputs of a trace.  Any pointer may be NULL. */
+typedef struct qmcrt_outputs {
+  uint32_t* d_counts;      /* [res_y*res_x] rays per pixel (exact integer) */
+  float* d_energy;         /* [res_y*res_x] sum of |sun . n_perturbed| * area-per-point (raw) */
+  float* d_flux;           /* [res_y*res_x] W/m^2 = energy * DNI * rho / (rays_per_point * pixel area) */
+  uint8_t* d_ray_flags;    /* [rays] QMCRT_RAY_* per ray */
+  int32_t* d_ray_pixel;    /* [rays] row*res_x + col, -1 if no receiver hit */
+} qmcrt_outputs;
+
+/* Scalars of a trace (filled only when requested; the call then synchronises). */
+typedef struct qmcrt_trace_stats {
+  uint64_t rays;
+  uint64_t shadowed;
+  uint64_t blocked;
+  uint64_t hit;
+  uint64_t offmap;
+  uint64_t rect_tests;      /* rectangle tests in both traversals */
+  uint64_t dda_cells;       /* cells visited in both traversals */
+  double total_power;       /* sum_h |n_h . sun| * DNI * A_h * rho, W (Gtest.cu:29,44) */
+  double intercepted_power; /* sum over the map of flux * pixel area, W */
+  double intercept_ratio;   /* intercepted / total (image_save.cpp:26-48) */
+} qmcrt_trace_stats;
+
+/* Table-mode inputs (device), the sampling structure of the reference kernel
+ * map_tracing (rectgrid_raytracing.cu:155-196): ray j of point m takes sun
+ * sample (start[m]+j) mod table_size and perturbation (start[m']+j) mod
+ * table_size (m' = m, or max(m-1,0) with QMCRT_QUIRK_PREV_PERTURB). */
+typedef struct qmcrt_table_inputs {
+  const float* d_sun_local;  /* [3T] unit vectors, y-up local frame (set_samplelights) */
+  const float* d_turb_local; /* [3T] unit vectors, y-up local frame (set_perturbation) */
+  int64_t table_size;        /* T (reference: 128*2048) */
+  const int32_t* d_start;    /* [points] start offsets (set_microhelio_groups) */
+  const float* d_point_xz;   /* [2*points] local (x, z) of each point, m, mirror-centred */
+  const int32_t* d_point_helio; /* [points] heliostat of each point */
+  int64_t points;
+  int32_t rays_per_point;
+} qmcrt_table_inputs;
+
+/* Grid summary. */
+typedef struct qmcrt_grid_info {
+  float origin[3];
+  float cell[3];
+  int32_t dims[3];
+  int64_t cells;
+  int64_t entries; /* CSR entries (heliostat registrations) */
+  int32_t fine_div;
+} qmcrt_grid_info;
+
+/* Radial-staggered field layout generator (scene front-end). */
+typedef struct qmcrt_layout_params {
+  int32_t n;               /* heliostats wanted */
+  float helio_w, helio_h;  /* mirror width, height (m) */
+  float thickness;         /* mirror thickness (m) */
+  float r_min, r_max;      /* ring radii (m) */
+  float az_center_deg;     /* centre of the field's azimuth span (0 = north), degrees */
+  float az_span_deg;       /* span; 360 = surround field */
+  float spacing;           /* minimum centre spacing (m); 0 = auto to fill r_max */
+  float jitter;            /* uniform jitter amplitude on x and z (m) */
+  float mount_height;      /* mirror centre height above ground (m) */
+  uint64_t seed;
+} qmcrt_layout_params;
+
+typedef struct qmcrt_scene qmcrt_scene;
+typedef struct qmcrt_tape qmcrt_tape;
+typedef struct qmcrt_batch qmcrt_batch;
+
+/* ------------------------------------------------------------------ info */
+const char* qmcrt_version(void);
+const char* qmcrt_status_string(qmcrt_status s);
+const char* qmcrt_last_error(void);
+
+/* --------------------------------------------------- host-side helpers
+ * Pure host code; these need no GPU. */
+
+/* Sun incident direction from elevation/azimuth (degrees, azimuth from north
+ * clockwise), the convention of main.cpp:71-73. */
+qmcrt_status qmcrt_sun_direction(float elevation_deg, float azimuth_deg, float dir_out[3]);
+
+/* Buie sunshape inverse-CDF table, built exactly as
+ * SceneProcessor::set_samplelights (scene_instance_process.cu:163-200) builds
+ * it: 1024 trapezoids on [0, 4.65] mrad plus the analytic aureole to 9.3 mrad.
+ * params_out = {k, gamma, core_area, total_area, B, C}. */
+qmcrt_status qmcrt_buie_table(float csr, float* cdf_x /*[1025]*/, float* cdf_y /*[1025]*/,
+                              float* slope /*[1024]*/, float params_out[6]);
+
+/* Radial-staggered layout: writes up to `capacity` heliostat centres. */
+qmcrt_status qmcrt_layout_radial_staggered(const qmcrt_layout_params* p, float* h_pos,
+                                           int32_t capacity, int32_t* n_out);
+
+/* Parse a reference .scn scene file (scene_file_proc.cpp:41-286) into
+ * caller-visible arrays.  Call once with h_pos == NULL to get the counts. */
+qmcrt_status qmcrt_scn_parse(const char* path, qmcrt_receiver* recv_out,
+                             qmcrt_grid_params* grid_out, float* h_pos, float* h_size,
+                             int32_t capacity, int32_t* n_out);
+
+/* -------------------------------------------------------------- scenes
+ * A scene owns the device copy of the field, receiver and grid.  Replaces
+ * SolarScene (solar_scene.h:19-50) plus SceneProcessor::set_*_content
+ * (scene_instance_process.h:5-26). */
+qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* recv,
+                                const qmcrt_grid_params* grid, qmcrt_scene** out);
+qmcrt_status qmcrt_scene_destroy(qmcrt_scene* scene);
+
+/* Upload a new field (same n) from host memory; h2d copies on `stream`. */
+qmcrt_status qmcrt_scene_set_field(qmcrt_scene* scene, const qmcrt_field* field, void* stream);
+
+/* Aim the heliostats for `sun` and rebuild the grid on the GPU.  Replaces
+ * set_helio_content + set_grid_content (scene_instance_process.cpp:4-35)
+ * and RectGrid::CGridHelioMatch (grid.cpp:47-83). */
+qmcrt_status qmcrt_scene_set_sun(qmcrt_scene* scene, const qmcrt_sun* sun, uint32_t quirks,
+                                 void* stream);
+
+qmcrt_status qmcrt_scene_grid_info(qmcrt_scene* scene, qmcrt_grid_info* info);
+
+/* Copy the grid CSR to host (cells+1 offsets, entries heliostat ids).  Syncs. */
+qmcrt_status qmcrt_scene_read_grid(qmcrt_scene* scene, int32_t* h_cell_start, int32_t* h_entries,
+                                   void* stream);
+
+/* Copy per-heliostat geometry (double): normals [3n] and vertices v0,v1,v3
+ * [9n] (RectangleHelio::Cget_vertex, heliostat.cuh:45-50).  Syncs. */
+qmcrt_status qmcrt_scene_read_geometry(qmcrt_scene* scene, double* h_normals, double* h_vertices,
+                                       void* stream);
+
+/* Micro-heliostat sample points for (seed, rays, rays_per_point, mode,
+ * spacing) (set_possion_microhelio_centers steps_for_raytracing.cu:105-158,
+ * set_microhelio_centers :67-103).  Cached in the scene.  points_out: count. */
+qmcrt_status qmcrt_scene_sample_points(qmcrt_scene* scene, const qmcrt_trace_params* params,
+                                       int64_t* points_out, void* stream);
+
+/* Copy the cached points: local (x, z) in m relative to the mirror centre
+ * ([2*points] floats; Poisson points lie on a 2^-16 m lattice from the mirror
+ * corner) and their heliostat ids.  Syncs. */
+qmcrt_status qmcrt_scene_read_points(qmcrt_scene* scene, float* h_point_xz, int32_t* h_point_helio,
+                                     void* stream);
+
+/* ------------------------------------------------------------- tracing */
+
+/* One full trace: aim, grid, points (cached), Philox sampling, shadow and
+ * block traversal, receiver deposition, flux scaling.  Replaces
+ * results_with_given_normal's loop over recthelio_ray_tracing
+ * (Gtest.cu:21-46, recthelio_tracing.cpp:46-80, ray_tracing.cu:3-32).
+ * If `stats` is not NULL the call synchronises `stream` and fills it. */
+qmcrt_status qmcrt_trace(qmcrt_scene* scene, const qmcrt_sun* sun, const qmcrt_trace_params* params,
+                         const qmcrt_outputs* out, qmcrt_trace_stats* stats, void* stream);
+
+/* Parity mode: the same traversal fed by caller-provided sample tables
+ * (the inputs of map_tracing, rectgrid_raytracing.cu:155-162).  Rays are
+ * numbered point-major (ray = point*rays_per_point + j). */
+qmcrt_status qmcrt_trace_tables(qmcrt_scene* scene, const qmcrt_sun* sun,
+                                const qmcrt_table_inputs* tables, const qmcrt_trace_params* params,
+                                const qmcrt_outputs* out, qmcrt_trace_stats* stats, void* stream);
+
+/* End-to-end call on host buffers: upload the field, trace, download the
+ * maps.  h_counts / h_flux may be NULL.  Synchronises. */
+qmcrt_status qmcrt_trace_host(qmcrt_scene* scene, const qmcrt_field* field, const qmcrt_sun* sun,
+                              const qmcrt_trace_params* params, uint32_t* h_counts, float* h_flux,
+                              qmcrt_trace_stats* stats, void* stream);
+
+/* ----------------------------------------------------------- smoothing
+ * Trimmed-mean smoothing over a (2r+1)^2 window clipped at the border,
+ * k = int(cnt * ratio) values dropped at each end (ImageSmoother::image_smooth,
+ * image_smooth.cu:60-115).  d_in and d_out must not overlap. */
+qmcrt_status qmcrt_smooth_trimmed_u32(const uint32_t* d_in, float* d_out, int32_t width,
+                                      int32_t height, int32_t radius, float ratio, int32_t method,
+                                      void* stream);
+qmcrt_status qmcrt_smooth_trimmed_f32(const float* d_in, float* d_out, int32_t width,
+                                      int32_t height, int32_t radius, float ratio, int32_t method,
+                                      void* stream);
+
+/* Device time of the stages of the last qmcrt_trace / qmcrt_trace_tables on
+ * this scene, from CUDA events recorded on the call's stream.  setup_ms is
+ * the aiming + grid build (negative when that trace reused the cached
+ * geometry).  Waits for the last trace to finish. */
+typedef struct qmcrt_timing {
+  float setup_ms;
+  float trace_kernel_ms;
+  float finalize_ms;
+} qmcrt_timing;
+qmcrt_status qmcrt_scene_timing(qmcrt_scene* scene, qmcrt_timing* timing);
+
+/* ------------------------------------------------------------ probes */
+
+/* FP32 FMA issue-rate probe for the roofline: `iters` dependent FMA chains
+ * per thread on every SM.  Writes a sink value (device) and returns the FLOP
+ * count of one launch in *flops. */
+qmcrt_status qmcrt_fp32_peak_probe(float* d_sink, int32_t iters, double* flops, void* stream);
+
+/* Philox4x32-10 block for a counter/key (test hook for the in-kernel RNG).
+ * Writes n blocks (4 words each) for counters ctr0 + i (word 0 incremented). */
+qmcrt_status qmcrt_philox_blocks(const uint32_t ctr0[4], const uint32_t key[2], int64_t n,
+                                 uint32_t* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMCRT_H_ */

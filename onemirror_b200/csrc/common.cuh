@@ -1,0 +1,78 @@
+// common.cuh — device/host helpers shared by the qmcrt kernels: small vector
+// algebra in float and double (written for this library), the Philox4x32-10
+// counter-based generator (Salmon et al., SC'11) and uniform conversions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define QMCRT_HD __host__ __device__ __forceinline__
+
+namespace qm {
+
+// ------------------------------------------------------------------ float3
+QMCRT_HD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+QMCRT_HD float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+QMCRT_HD float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+QMCRT_HD float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+QMCRT_HD float3 operator*(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+QMCRT_HD float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+QMCRT_HD float3 cross(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// ----------------------------------------------------------------- double3
+struct d3 {
+  double x, y, z;
+};
+QMCRT_HD d3 mk(double x, double y, double z) { return d3{x, y, z}; }
+QMCRT_HD d3 operator+(d3 a, d3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+QMCRT_HD d3 operator-(d3 a, d3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+QMCRT_HD d3 operator*(double s, d3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+QMCRT_HD double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+QMCRT_HD d3 cross(d3 a, d3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+QMCRT_HD float3 to_f(d3 a) { return f3((float)a.x, (float)a.y, (float)a.z); }
+QMCRT_HD d3 to_d(float3 a) { return mk(a.x, a.y, a.z); }
+
+// Frame applied to a local vector: out = d.x*u + d.y*n + d.z*v, the matrix of
+// local2world (global_function.cuh:47-49).
+struct frame64 {
+  d3 u, n, v;
+};
+QMCRT_HD d3 apply(const frame64& f, double x, double y, double z) {
+  return mk(x * f.u.x + y * f.n.x + z * f.v.x, x * f.u.y + y * f.n.y + z * f.v.y,
+            x * f.u.z + y * f.n.z + z * f.v.z);
+}
+
+// --------------------------------------------------------------- Philox
+// Philox4x32 with 10 rounds; multipliers and Weyl increments from the
+// published algorithm (Random123 paper, SC'11).
+QMCRT_HD uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+    uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+#else
+    uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
+    uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+    uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+#endif
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Uniform in (0,1) from the top 24 bits: exact in float and double.
+QMCRT_HD float u24f(uint32_t w) { return ((float)(w >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+
+constexpr uint32_t kTagTrace = 0x51A7u;
+constexpr uint32_t kTagPoisson = 0x9015u;
+constexpr uint32_t kPoissonKey0 = 0x5A17C0DEu;
+constexpr uint32_t kPoissonKey1 = 0x0B5E55EDu;
+constexpr float kEps = 1e-6f;  // global_constant.h:7
+
+}  // namespace qm

@@ -1,0 +1,118 @@
+// internal.hpp — host-side state behind the qmcrt C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/qmcrt.h"
+#include "common.cuh"
+
+namespace qm {
+
+// Thread-local last-error message; set_error returns its status for chaining.
+qmcrt_status set_error(qmcrt_status s, const std::string& msg);
+qmcrt_status cuda_error(cudaError_t e, const char* what);
+
+#define QM_CUDA(call)                                         \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return ::qm::cuda_error(e_, #call); \
+  } while (0)
+
+// Receiver geometry computed on the host in double (receiver.cpp:24-118).
+struct ReceiverGeom {
+  int type = 0;
+  double v0[3], v1[3], v3[3];  // flat: parallelogram corners (v2 = v1 + v3 - v0)
+  double focus[3];
+  double cyl[5];  // cylinder: cx, y0, cz, radius, height
+  int res_x = 0, res_y = 0;
+  double pixel_area = 0;
+};
+
+// Buie sunshape table (1025 + 1025 + 1024 floats) and its scalars.
+struct BuieTable {
+  float csr = -1.f;
+  std::vector<float> host;  // cdf_x | cdf_y | slope
+  float params[6];          // k, gamma, core, total, B, C
+};
+
+// Build the table exactly as set_samplelights does (float arithmetic).
+void buie_build(float csr, float* cdf_x, float* cdf_y, float* slope, float params[6]);
+
+// Receiver geometry from the C description.
+qmcrt_status receiver_setup(const qmcrt_receiver& r, ReceiverGeom* g);
+
+struct PointsKey {
+  uint64_t seed = 0, rays = 0;
+  int rpp = 0, mode = -1;
+  float spacing = 0;
+  bool operator==(const PointsKey& o) const {
+    return seed == o.seed && rays == o.rays && rpp == o.rpp && mode == o.mode && spacing == o.spacing;
+  }
+};
+
+struct SunKey {
+  float dir[3] = {0, 0, 0};
+  uint32_t quirks = 0xFFFFFFFFu;
+  uint64_t field_version = ~0ull;
+  bool operator==(const SunKey& o) const {
+    return dir[0] == o.dir[0] && dir[1] == o.dir[1] && dir[2] == o.dir[2] && quirks == o.quirks &&
+           field_version == o.field_version;
+  }
+};
+
+}  // namespace qm
+
+struct qmcrt_scene {
+  int device = 0;
+  int n = 0;
+  uint64_t field_version = 0;
+  bool has_aim = false, has_normal = false, has_tilt = false;
+  std::vector<float> h_pos, h_size;
+  qmcrt_receiver recv{};
+  qm::ReceiverGeom rg;
+  qmcrt_grid_params gp{};
+
+  // grid: bounds fixed per scene (orientation-independent sphere bounds)
+  float gpos[3], gcell[3];
+  int gdims[3];
+  int64_t cells = 0, entry_cap = 0;
+  int fine_div = 1;
+
+  // device field
+  float *d_pos = nullptr, *d_size = nullptr, *d_aim = nullptr, *d_normal_in = nullptr;
+  float *d_sigma = nullptr, *d_tilt = nullptr;
+  // per-sun geometry
+  double* d_normal = nullptr;   // [3n]
+  double* d_frame = nullptr;    // [9n] u, n, v
+  float4* d_rect = nullptr;     // [3n] A(v0)+id, E1, E2 (float)
+  int4* d_cellbox = nullptr;    // [2n] lo, hi cell indices per heliostat
+  int32_t* d_cell_count = nullptr;  // [cells]
+  int32_t* d_cell_start = nullptr;  // [cells+1]
+  int32_t* d_entries = nullptr;     // [entry_cap]
+  float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
+  qm::SunKey sun_key;
+
+  // points
+  qm::PointsKey points_key;
+  int64_t points = 0, points_cap = 0;
+  float2* d_point_xz = nullptr;
+  int32_t* d_point_helio = nullptr;
+  float* d_helio_weight = nullptr;  // [n] mirror area per point
+  int32_t* d_flag = nullptr;        // device error flag for setup kernels
+
+  // maps and statistics
+  uint32_t* d_counts = nullptr;
+  float* d_energy = nullptr;
+  unsigned long long* d_stats = nullptr;  // [16]
+
+  // sunshape
+  qm::BuieTable buie;
+  float* d_buie = nullptr;
+
+  // stage timing of the last trace: [0,1] setup, [2,3] trace kernel, [4] finalize end
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool setup_timed = false;
+  bool traced = false;
+};

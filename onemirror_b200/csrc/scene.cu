@@ -1,0 +1,745 @@
+// scene.cu — scene lifetime, heliostat aiming, GPU grid build and
+// micro-heliostat sample points.
+//
+// Replaces, on the GPU: set_helio_content + RectangleHelio::CRotate
+// (scene_instance_process.cpp:24-35, heliostat.cpp:16-58), the host CSR build
+// RectGrid::Cinit/CGridHelioMatch (grid.cpp:3-83) and the micro-point
+// generators set_microhelio_centers / set_possion_microhelio_centers
+// (steps_for_raytracing.cu:67-158).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.hpp"
+
+using namespace qm;
+
+namespace qm {
+
+// --------------------------------------------------------------- aiming
+struct AimArgs {
+  int n;
+  const float *pos, *size, *aim, *normal_in, *tilt;
+  double focus[3];
+  double sun[3];
+  uint32_t quirks;
+  double* normal;
+  double* frame;
+  float4* rect;
+  int4* cellbox;
+  int32_t* cell_count;
+  float gpos[3], gcell[3];
+  int gdims[3];
+  unsigned long long* stats;
+};
+
+__device__ __forceinline__ d3 nrm3(d3 a) {
+  double l = sqrt(dot(a, a));
+  return mk(a.x / l, a.y / l, a.z / l);
+}
+
+// local2world frame (global_function.cuh:14-52)
+__device__ __forceinline__ frame64 frame_of(d3 n, uint32_t quirks) {
+  frame64 f;
+  if (fabs(n.x) < 1e-6 && fabs(n.z) < 1e-6) {
+    double s = (n.y < 0 && !(quirks & QMCRT_QUIRK_ZENITH_FRAME)) ? -1.0 : 1.0;
+    f.u = mk(1, 0, 0);
+    f.n = mk(0, s, 0);
+    f.v = mk(0, 0, s);
+    return f;
+  }
+  f.n = n;
+  f.u = nrm3(mk(n.z, 0, -n.x));  // (0,1,0) x n
+  f.v = nrm3(cross(f.u, n));
+  return f;
+}
+
+__global__ void aim_kernel(AimArgs a) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  double pw = 0;
+  if (h < a.n) {
+    d3 p = mk(a.pos[3 * h], a.pos[3 * h + 1], a.pos[3 * h + 2]);
+    d3 n;
+    if (a.normal_in) {
+      n = nrm3(mk(a.normal_in[3 * h], a.normal_in[3 * h + 1], a.normal_in[3 * h + 2]));
+    } else {
+      d3 t = a.aim ? mk(a.aim[3 * h], a.aim[3 * h + 1], a.aim[3 * h + 2])
+                   : mk(a.focus[0], a.focus[1], a.focus[2]);
+      d3 r = nrm3(t - p);
+      n = nrm3(r - mk(a.sun[0], a.sun[1], a.sun[2]));  // heliostat.cpp:51-58
+    }
+    frame64 f = frame_of(n, a.quirks);
+    if (a.tilt) {
+      n = nrm3(n + a.tilt[2 * h] * f.u + a.tilt[2 * h + 1] * f.v);
+      f = frame_of(n, a.quirks);
+    }
+    a.normal[3 * h] = n.x;
+    a.normal[3 * h + 1] = n.y;
+    a.normal[3 * h + 2] = n.z;
+    double* fr = a.frame + 9 * h;
+    fr[0] = f.u.x; fr[1] = f.u.y; fr[2] = f.u.z;
+    fr[3] = f.n.x; fr[4] = f.n.y; fr[5] = f.n.z;
+    fr[6] = f.v.x; fr[7] = f.v.y; fr[8] = f.v.z;
+    double sx = a.size[3 * h], sy = a.size[3 * h + 1], sz = a.size[3 * h + 2];
+    // Cset_localvertex + Cset_worldvertex (heliostat.cpp:30-49): v0, v1, v3
+    d3 v0 = p + apply(f, -sx / 2, sy / 2, -sz / 2);
+    d3 v1 = p + apply(f, -sx / 2, sy / 2, sz / 2);
+    d3 v3 = p + apply(f, sx / 2, sy / 2, -sz / 2);
+    d3 e1 = v1 - v0, e2 = v3 - v0;
+    a.rect[3 * h] = make_float4((float)v0.x, (float)v0.y, (float)v0.z, __int_as_float(h));
+    a.rect[3 * h + 1] = make_float4((float)e1.x, (float)e1.y, (float)e1.z, 0.f);
+    a.rect[3 * h + 2] = make_float4((float)e2.x, (float)e2.y, (float)e2.z, 0.f);
+    // cells covered (CGridHelioMatch grid.cpp:47-61)
+    int lo[3], hi[3];
+    if (a.quirks & QMCRT_QUIRK_AABB_RADIUS) {
+      float fx = a.size[3 * h], fy = a.size[3 * h + 1], fz = a.size[3 * h + 2];
+      float radius = sqrtf(__fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)), __fmul_rn(fz, fz)))) / 2;
+      for (int i = 0; i < 3; ++i) {
+        float pc = a.pos[3 * h + i];
+        int l = (int)(__fsub_rn(__fsub_rn(pc, radius), a.gpos[i]) / a.gcell[i]);
+        int u = (int)(__fsub_rn(__fadd_rn(pc, radius), a.gpos[i]) / a.gcell[i]);
+        lo[i] = min(max(l, 0), a.gdims[i] - 1);
+        hi[i] = min(max(u, 0), a.gdims[i] - 1);
+      }
+    } else {
+      d3 v2 = v1 + e2;
+      double c[4][3] = {{v0.x, v0.y, v0.z}, {v1.x, v1.y, v1.z}, {v2.x, v2.y, v2.z}, {v3.x, v3.y, v3.z}};
+      for (int i = 0; i < 3; ++i) {
+        double mn = c[0][i], mx = c[0][i];
+        for (int k = 1; k < 4; ++k) {
+          mn = fmin(mn, c[k][i]);
+          mx = fmax(mx, c[k][i]);
+        }
+        int l = (int)floor((mn - (double)a.gpos[i]) / (double)a.gcell[i]);
+        int u = (int)floor((mx - (double)a.gpos[i]) / (double)a.gcell[i]);
+        lo[i] = min(max(l, 0), a.gdims[i] - 1);
+        hi[i] = min(max(u, 0), a.gdims[i] - 1);
+      }
+    }
+    a.cellbox[2 * h] = make_int4(lo[0], lo[1], lo[2], 0);
+    a.cellbox[2 * h + 1] = make_int4(hi[0], hi[1], hi[2], 0);
+    for (int x = lo[0]; x <= hi[0]; ++x)
+      for (int y = lo[1]; y <= hi[1]; ++y)
+        for (int z = lo[2]; z <= hi[2]; ++z)
+          atomicAdd(&a.cell_count[((int64_t)x * a.gdims[1] + y) * a.gdims[2] + z], 1);
+    // Gtest.cu:29: |n . sun| * A
+    pw = fabs(dot(n, mk(a.sun[0], a.sun[1], a.sun[2]))) * sx * sz;
+  }
+  for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
+  if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd((double*)&a.stats[8], pw);
+}
+
+// Exclusive scan of cell_count into cell_start (one CTA of 1024 threads,
+// each scanning a contiguous run), then zero cell_count for the fill cursor.
+__global__ void __launch_bounds__(1024) scan_kernel(int32_t* count, int32_t* start, int64_t cells,
+                                                    int64_t cap, int32_t* flag) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  int64_t per = (cells + 1023) / 1024;
+  int64_t b = t * per, e = min(cells, b + per);
+  int64_t s = 0;
+  for (int64_t i = b; i < e; ++i) s += count[i];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int64_t v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int64_t run = part[t] - s;
+  for (int64_t i = b; i < e; ++i) {
+    start[i] = (int32_t)min(run, cap);
+    run += count[i];
+    count[i] = 0;
+  }
+  if (t == 1023) {
+    start[cells] = (int32_t)min(part[1023], cap);
+    if (part[1023] > cap) atomicExch(flag, 1);
+  }
+}
+
+__global__ void fill_kernel(int n, const int4* cellbox, const int32_t* start, int32_t* cursor,
+                            int32_t* entries, int gy, int gz, int64_t cap) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n) return;
+  int4 lo = cellbox[2 * h], hi = cellbox[2 * h + 1];
+  for (int x = lo.x; x <= hi.x; ++x)
+    for (int y = lo.y; y <= hi.y; ++y)
+      for (int z = lo.z; z <= hi.z; ++z) {
+        int64_t c = ((int64_t)x * gy + y) * gz + z;
+        int slot = atomicAdd(&cursor[c], 1);
+        int64_t k = (int64_t)start[c] + slot;
+        if (k < start[c + 1] && k < cap) entries[k] = h;
+      }
+}
+
+// Sort each cell's list ascending (the reference's push_back order,
+// grid.cpp:36-44) and lay the rectangles out cell-major.
+__global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t* entries,
+                                   const float4* rect, float4* cell_rect) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  int b = start[c], e = start[c + 1];
+  for (int i = b + 1; i < e; ++i) {
+    int v = entries[i], j = i - 1;
+    while (j >= b && entries[j] > v) {
+      entries[j + 1] = entries[j];
+      --j;
+    }
+    entries[j + 1] = v;
+  }
+  for (int i = b; i < e; ++i) {
+    int h = entries[i];
+    cell_rect[3 * (int64_t)i] = rect[3 * h];
+    cell_rect[3 * (int64_t)i + 1] = rect[3 * h + 1];
+    cell_rect[3 * (int64_t)i + 2] = rect[3 * h + 2];
+  }
+}
+
+// ------------------------------------------------------------ points
+struct PoissonArgs {
+  int n;
+  const float* size;
+  int64_t q, rem;
+  int64_t Rq, R2, cq, nb;
+  uint2 key;
+  int64_t max_batches;
+  int2* point_q;
+  float2* point_xz;
+  int32_t* point_helio;
+  int32_t* flag;
+};
+
+// Sequential dart throwing on a 2^-16 m lattice with exact integer distance
+// tests: 32 candidates per batch (one per lane, Philox), accepted in lane
+// order against every earlier point.  One warp per heliostat, background grid
+// of cell r/sqrt(2) in shared memory (at most one point per cell).
+__global__ void __launch_bounds__(32) poisson_kernel(PoissonArgs a) {
+  extern __shared__ int32_t sgrid[];
+  const int h = blockIdx.x, lane = threadIdx.x;
+  const int64_t P = a.q + (h < a.rem ? 1 : 0);
+  const int64_t base = (int64_t)h * a.q + min((int64_t)h, a.rem);
+  const float sx = a.size[3 * h], sz = a.size[3 * h + 2];
+  const int64_t W = (int64_t)((double)sx * 65536.0), H = (int64_t)((double)sz * 65536.0);
+  const int64_t gx = (W + a.cq - 1) / a.cq, gz = (H + a.cq - 1) / a.cq;
+  for (int64_t i = lane; i < gx * gz; i += 32) sgrid[i] = -1;
+  __syncwarp();
+  int64_t got = 0;
+  for (int64_t b = 0; b < a.max_batches && got < P; ++b) {
+    uint64_t cid = (uint64_t)b * 32 + lane;
+    uint4 w = philox4x32_10(make_uint4((uint32_t)h, (uint32_t)cid, (uint32_t)(cid >> 32), kTagPoisson), a.key);
+    int64_t ix = (int64_t)(((uint64_t)w.x * (uint64_t)W) >> 32);
+    int64_t iz = (int64_t)(((uint64_t)w.y * (uint64_t)H) >> 32);
+    int64_t cx = ix / a.cq, cz = iz / a.cq;
+    bool ok = true;
+    for (int64_t dx = -a.nb; dx <= a.nb && ok; ++dx)
+      for (int64_t dz = -a.nb; dz <= a.nb && ok; ++dz) {
+        int64_t x = cx + dx, z = cz + dz;
+        if (x < 0 || z < 0 || x >= gx || z >= gz) continue;
+        int k = sgrid[x * gz + z];
+        if (k < 0) continue;
+        int2 pq = a.point_q[base + k];
+        int64_t ddx = pq.x - ix, ddz = pq.y - iz;
+        if (ddx * ddx + ddz * ddz < a.R2) ok = false;
+      }
+    for (int l = 0; l < 32 && got < P; ++l) {
+      unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (!((m >> l) & 1u)) continue;
+      int64_t lx = __shfl_sync(0xffffffffu, ix, l), lz = __shfl_sync(0xffffffffu, iz, l);
+      if (lane == l) {
+        sgrid[cx * gz + cz] = (int32_t)got;
+        a.point_q[base + got] = make_int2((int)ix, (int)iz);
+      }
+      if (lane > l && ok) {
+        int64_t ddx = lx - ix, ddz = lz - iz;
+        if (ddx * ddx + ddz * ddz < a.R2) ok = false;
+      }
+      ++got;
+    }
+    __syncwarp();
+  }
+  if (got < P) {
+    if (lane == 0) atomicExch(a.flag, 2);
+    return;
+  }
+  for (int64_t k = lane; k < P; k += 32) {
+    int2 pq = a.point_q[base + k];
+    float x = (float)pq.x * (1.0f / 65536.0f), z = (float)pq.y * (1.0f / 65536.0f);
+    a.point_xz[base + k] = make_float2(__fsub_rn(x, 0.5f * sx), __fsub_rn(z, 0.5f * sz));
+    a.point_helio[base + k] = h;
+  }
+}
+
+// Regular grid of cell centres (map_microhelio_centers, steps_for_raytracing.cu:4-22).
+__global__ void grid_points_kernel(int n, const float* size, float pl, const int64_t* base,
+                                   float2* xz, int32_t* helio) {
+  int h = blockIdx.x;
+  float sx = size[3 * h], sz = size[3 * h + 2];
+  int rows = (int)(sz / pl), cols = (int)(sx / pl);
+  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+    int r = i / cols, c = i % cols;
+    float x = __fsub_rn(__fadd_rn(__fmul_rn((float)c, pl), pl / 2), sx / 2);
+    float z = __fsub_rn(__fadd_rn(__fmul_rn((float)r, pl), pl / 2), sz / 2);
+    xz[base[h] + i] = make_float2(x, z);
+    helio[base[h] + i] = h;
+  }
+}
+
+__global__ void weight_kernel(int n, const float* size, int64_t q, int64_t rem, int mode, float pl,
+                              float* w) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n) return;
+  if (mode == QMCRT_POINTS_GRID) {
+    w[h] = pl * pl;  // Gtest.cu:40: S_sub = helio_pixel_length^2
+  } else {
+    int64_t P = q + (h < rem ? 1 : 0);
+    w[h] = (float)((double)size[3 * h] * (double)size[3 * h + 2] / (double)P);
+  }
+}
+
+// ------------------------------------------------------------ helpers
+template <class T>
+static qmcrt_status dev_alloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  QM_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
+  return QMCRT_OK;
+}
+template <class T>
+static void dev_free(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+static int64_t cells_in_box(const float gpos[3], const float gcell[3], const int gdims[3], const double lo[3],
+                            const double hi[3]) {
+  int64_t c = 1;
+  for (int i = 0; i < 3; ++i) {
+    int a = (int)std::floor((lo[i] - gpos[i]) / gcell[i]);
+    int b = (int)std::floor((hi[i] - gpos[i]) / gcell[i]);
+    a = std::min(std::max(a, 0), gdims[i] - 1);
+    b = std::min(std::max(b, 0), gdims[i] - 1);
+    c *= (b - a + 1);
+  }
+  return c;
+}
+
+static qmcrt_status check_field(const qmcrt_field* f) {
+  if (!f || f->n <= 0 || !f->pos || !f->size) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "field needs n > 0, pos and size");
+  for (int h = 0; h < f->n; ++h) {
+    for (int i = 0; i < 3; ++i)
+      if (!std::isfinite(f->pos[3 * h + i])) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "non-finite heliostat position");
+    if (!(f->size[3 * h] > 0) || !(f->size[3 * h + 2] > 0) || !(f->size[3 * h + 1] >= 0) ||
+        f->size[3 * h] > 1000.f || f->size[3 * h + 2] > 1000.f)
+      return set_error(QMCRT_ERR_INVALID_ARGUMENT, "heliostat size must be positive and below 1000 m");
+    float sg = f->slope_sigma ? f->slope_sigma[h] : f->sigma;
+    if (!(sg >= 0) || sg > 0.5f) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "slope error must be in [0, 0.5] rad");
+  }
+  return QMCRT_OK;
+}
+
+qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st) {
+  size_t n = (size_t)f->n;
+  QM_CUDA(cudaMemcpyAsync(s->d_pos, f->pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st));
+  QM_CUDA(cudaMemcpyAsync(s->d_size, f->size, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (f->aim) QM_CUDA(cudaMemcpyAsync(s->d_aim, f->aim, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (f->normal) QM_CUDA(cudaMemcpyAsync(s->d_normal_in, f->normal, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (f->tilt) QM_CUDA(cudaMemcpyAsync(s->d_tilt, f->tilt, 2 * n * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (f->slope_sigma) {
+    QM_CUDA(cudaMemcpyAsync(s->d_sigma, f->slope_sigma, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  } else {
+    std::vector<float> sg(n, f->sigma);
+    QM_CUDA(cudaMemcpyAsync(s->d_sigma, sg.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+    QM_CUDA(cudaStreamSynchronize(st));  // sg is a temporary
+  }
+  s->h_pos.assign(f->pos, f->pos + 3 * n);
+  s->h_size.assign(f->size, f->size + 3 * n);
+  s->field_version++;
+  s->points_key = PointsKey{};
+  return QMCRT_OK;
+}
+
+qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st) {
+  SunKey k;
+  std::memcpy(k.dir, sun->dir, sizeof(k.dir));
+  k.quirks = quirks & (QMCRT_QUIRK_AABB_RADIUS | QMCRT_QUIRK_ZENITH_FRAME);
+  k.field_version = s->field_version;
+  if (k == s->sun_key) return QMCRT_OK;
+  double sd[3] = {sun->dir[0], sun->dir[1], sun->dir[2]};
+  double l = std::sqrt(sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]);
+  if (!(l > 0) || !std::isfinite(l)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "sun direction is zero or not finite");
+  AimArgs a{};
+  a.n = s->n;
+  a.pos = s->d_pos;
+  a.size = s->d_size;
+  a.aim = s->has_aim ? s->d_aim : nullptr;
+  a.normal_in = s->has_normal ? s->d_normal_in : nullptr;
+  a.tilt = s->has_tilt ? s->d_tilt : nullptr;
+  std::memcpy(a.focus, s->rg.focus, sizeof(a.focus));
+  for (int i = 0; i < 3; ++i) a.sun[i] = sd[i] / l;
+  a.quirks = k.quirks;
+  a.normal = s->d_normal;
+  a.frame = s->d_frame;
+  a.rect = s->d_rect;
+  a.cellbox = s->d_cellbox;
+  a.cell_count = s->d_cell_count;
+  std::memcpy(a.gpos, s->gpos, sizeof(a.gpos));
+  std::memcpy(a.gcell, s->gcell, sizeof(a.gcell));
+  std::memcpy(a.gdims, s->gdims, sizeof(a.gdims));
+  a.stats = s->d_stats;
+  QM_CUDA(cudaEventRecord(s->ev[0], st));
+  QM_CUDA(cudaMemsetAsync(s->d_cell_count, 0, s->cells * sizeof(int32_t), st));
+  QM_CUDA(cudaMemsetAsync(s->d_stats + 8, 0, sizeof(unsigned long long), st));
+  aim_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(a);
+  QM_CUDA(cudaGetLastError());
+  scan_kernel<<<1, 1024, 0, st>>>(s->d_cell_count, s->d_cell_start, s->cells, s->entry_cap, s->d_flag);
+  QM_CUDA(cudaGetLastError());
+  fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, s->d_cellbox, s->d_cell_start, s->d_cell_count,
+                                                  s->d_entries, s->gdims[1], s->gdims[2], s->entry_cap);
+  QM_CUDA(cudaGetLastError());
+  cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, s->d_cell_start, s->d_entries,
+                                                                        s->d_rect, s->d_cell_rect);
+  QM_CUDA(cudaGetLastError());
+  QM_CUDA(cudaEventRecord(s->ev[1], st));
+  s->setup_timed = true;
+  s->sun_key = k;
+  return QMCRT_OK;
+}
+
+qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st) {
+  PointsKey k;
+  k.seed = p->seed;
+  k.rays = p->rays;
+  k.rpp = p->rays_per_point;
+  k.mode = p->point_mode;
+  k.spacing = p->point_spacing;
+  if (k == s->points_key) return QMCRT_OK;
+  if (p->rays_per_point <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "rays_per_point must be positive");
+  int64_t total = 0;
+  std::vector<int64_t> base;
+  if (p->point_mode == QMCRT_POINTS_GRID) {
+    if (!(p->point_spacing > 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid points need a pixel length");
+    base.resize(s->n);
+    for (int h = 0; h < s->n; ++h) {
+      base[h] = total;
+      int rows = (int)(s->h_size[3 * h + 2] / p->point_spacing), cols = (int)(s->h_size[3 * h] / p->point_spacing);
+      total += (int64_t)rows * cols;
+    }
+  } else if (p->point_mode == QMCRT_POINTS_POISSON) {
+    if (p->rays == 0 || p->rays % (uint64_t)p->rays_per_point != 0)
+      return set_error(QMCRT_ERR_INVALID_ARGUMENT, "rays must be a positive multiple of rays_per_point");
+    total = (int64_t)(p->rays / (uint64_t)p->rays_per_point);
+    if (total < s->n) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "fewer points than heliostats");
+    if (!(p->point_spacing > 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "Poisson points need a minimum spacing");
+  } else {
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown point mode");
+  }
+  if (total <= 0 || (uint64_t)total * (uint64_t)p->rays_per_point > 0xFFFFFFFFull)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray count must be in [1, 2^32)");
+  if (total > s->points_cap) {
+    dev_free(s->d_point_xz);
+    dev_free(s->d_point_helio);
+    qmcrt_status e = dev_alloc(&s->d_point_xz, total);
+    if (e) return e;
+    e = dev_alloc(&s->d_point_helio, total);
+    if (e) return e;
+    s->points_cap = total;
+  }
+  int64_t q = total / s->n, rem = total % s->n;
+  QM_CUDA(cudaMemsetAsync(s->d_flag, 0, sizeof(int32_t), st));
+  if (p->point_mode == QMCRT_POINTS_GRID) {
+    int64_t* d_base = nullptr;
+    qmcrt_status e = dev_alloc(&d_base, s->n);
+    if (e) return e;
+    QM_CUDA(cudaMemcpyAsync(d_base, base.data(), s->n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    grid_points_kernel<<<s->n, 256, 0, st>>>(s->n, s->d_size, p->point_spacing, d_base, s->d_point_xz, s->d_point_helio);
+    cudaError_t le = cudaGetLastError();
+    cudaStreamSynchronize(st);
+    cudaFree(d_base);
+    if (le != cudaSuccess) return cuda_error(le, "grid_points_kernel");
+  } else {
+    PoissonArgs a{};
+    a.n = s->n;
+    a.size = s->d_size;
+    a.q = q;
+    a.rem = rem;
+    a.Rq = (int64_t)((double)p->point_spacing * 65536.0);
+    if (a.Rq < 1) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "Poisson spacing below 2^-16 m");
+    a.R2 = a.Rq * a.Rq;
+    int64_t cq = (int64_t)std::sqrt((double)(a.R2 / 2));
+    while (cq * cq > a.R2 / 2) --cq;
+    while ((cq + 1) * (cq + 1) <= a.R2 / 2) ++cq;
+    a.cq = std::max<int64_t>(cq, 1);
+    a.nb = (a.Rq + a.cq - 1) / a.cq;
+    a.key = make_uint2((uint32_t)p->seed ^ kPoissonKey0, (uint32_t)(p->seed >> 32) ^ kPoissonKey1);
+    a.max_batches = (64 * (q + 1) + 1023) / 32 + 32;
+    int2* d_q = nullptr;
+    qmcrt_status e = dev_alloc(&d_q, total);
+    if (e) return e;
+    a.point_q = d_q;
+    a.point_xz = s->d_point_xz;
+    a.point_helio = s->d_point_helio;
+    a.flag = s->d_flag;
+    int64_t smem = 0;
+    for (int h = 0; h < s->n; ++h) {
+      int64_t W = (int64_t)((double)s->h_size[3 * h] * 65536.0), H = (int64_t)((double)s->h_size[3 * h + 2] * 65536.0);
+      int64_t g = ((W + a.cq - 1) / a.cq) * ((H + a.cq - 1) / a.cq);
+      smem = std::max(smem, g * (int64_t)sizeof(int32_t));
+    }
+    if (smem > 200 * 1024) {
+      cudaFree(d_q);
+      return set_error(QMCRT_ERR_INVALID_ARGUMENT, "Poisson spacing too small for the heliostat size (background grid over 200 KB)");
+    }
+    if (smem > 48 * 1024) QM_CUDA(cudaFuncSetAttribute(poisson_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    poisson_kernel<<<s->n, 32, (size_t)smem, st>>>(a);
+    cudaError_t le = cudaGetLastError();
+    int32_t flag = 0;
+    cudaError_t ce = cudaMemcpyAsync(&flag, s->d_flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    cudaError_t se = cudaStreamSynchronize(st);
+    cudaFree(d_q);
+    if (le != cudaSuccess) return cuda_error(le, "poisson_kernel");
+    if (ce != cudaSuccess) return cuda_error(ce, "poisson flag copy");
+    if (se != cudaSuccess) return cuda_error(se, "poisson sync");
+    if (flag == 2)
+      return set_error(QMCRT_ERR_SAMPLING, "Poisson-disk spacing too large for the requested points per heliostat");
+  }
+  weight_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, s->d_size, q, rem, p->point_mode, p->point_spacing,
+                                                     s->d_helio_weight);
+  QM_CUDA(cudaGetLastError());
+  s->points = total;
+  s->points_key = k;
+  return QMCRT_OK;
+}
+
+}  // namespace qm
+
+extern "C" {
+
+qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* recv, const qmcrt_grid_params* grid,
+                                qmcrt_scene** out) {
+  if (!out) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  qmcrt_status e = check_field(field);
+  if (e) return e;
+  if (!recv || !grid) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "receiver and grid are required");
+  for (int i = 0; i < 3; ++i)
+    if (!(grid->cell[i] > 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid cell sizes must be positive");
+  qmcrt_scene* s = new qmcrt_scene();
+  s->n = field->n;
+  s->recv = *recv;
+  s->gp = *grid;
+  e = receiver_setup(*recv, &s->rg);
+  if (e) { delete s; return e; }
+  s->has_aim = field->aim != nullptr;
+  s->has_normal = field->normal != nullptr;
+  s->has_tilt = field->tilt != nullptr;
+  // grid bounds: union of pos +- |size|/2 (any orientation) and of the
+  // reference's registration cube, plus margin (RectGrid::Cinit grid.cpp:3-8)
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  std::vector<double> rad(s->n);
+  for (int h = 0; h < s->n; ++h) {
+    double sx = field->size[3 * h], sy = field->size[3 * h + 1], sz = field->size[3 * h + 2];
+    double r = 0.5 * std::sqrt(sx * sx + sy * sy + sz * sz);
+    double rq = std::sqrt(std::sqrt(sx * sx + sy * sy + sz * sz)) / 2.0;
+    rad[h] = std::max(r, rq) + 1e-3;
+    for (int i = 0; i < 3; ++i) {
+      lo[i] = std::min(lo[i], field->pos[3 * h + i] - std::max(r, rq));
+      hi[i] = std::max(hi[i], field->pos[3 * h + i] + std::max(r, rq));
+    }
+  }
+  for (int i = 0; i < 3; ++i) {
+    s->gcell[i] = grid->cell[i];
+    if (grid->explicit_bounds) {
+      s->gpos[i] = grid->origin[i];
+      s->gdims[i] = std::max(1, (int)std::ceil((double)grid->extent[i] / grid->cell[i]));
+    } else {
+      float g = (float)(lo[i] - grid->margin);
+      s->gpos[i] = g;
+      s->gdims[i] = std::max(1, (int)std::ceil(((hi[i] + grid->margin) - (double)g) / grid->cell[i]));
+    }
+  }
+  s->cells = (int64_t)s->gdims[0] * s->gdims[1] * s->gdims[2];
+  if (s->cells > (int64_t)64 * 1024 * 1024) {
+    delete s;
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid has more than 2^26 cells; use larger cells");
+  }
+  int64_t cap = 0;
+  for (int h = 0; h < s->n; ++h) {
+    double l3[3], h3[3];
+    for (int i = 0; i < 3; ++i) {
+      l3[i] = field->pos[3 * h + i] - rad[h];
+      h3[i] = field->pos[3 * h + i] + rad[h];
+    }
+    cap += cells_in_box(s->gpos, s->gcell, s->gdims, l3, h3);
+  }
+  s->entry_cap = cap;
+  if (cap > 0x7FFFFFFF) { delete s; return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid registrations exceed 2^31"); }
+  s->fine_div = grid->fine_div > 1 ? grid->fine_div : 1;
+  size_t n = (size_t)s->n;
+  size_t res = (size_t)recv->res_x * recv->res_y;
+#define ALLOC(p, c)              \
+  do {                           \
+    e = dev_alloc(&(p), (c));    \
+    if (e) goto fail;            \
+  } while (0)
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    s->device = dev;
+  }
+  ALLOC(s->d_pos, 3 * n);
+  ALLOC(s->d_size, 3 * n);
+  if (s->has_aim) ALLOC(s->d_aim, 3 * n);
+  if (s->has_normal) ALLOC(s->d_normal_in, 3 * n);
+  if (s->has_tilt) ALLOC(s->d_tilt, 2 * n);
+  ALLOC(s->d_sigma, n);
+  ALLOC(s->d_normal, 3 * n);
+  ALLOC(s->d_frame, 9 * n);
+  ALLOC(s->d_rect, 3 * n);
+  ALLOC(s->d_cellbox, 2 * n);
+  ALLOC(s->d_cell_count, (size_t)s->cells);
+  ALLOC(s->d_cell_start, (size_t)s->cells + 1);
+  ALLOC(s->d_entries, (size_t)cap);
+  ALLOC(s->d_cell_rect, 3 * (size_t)cap);
+  ALLOC(s->d_helio_weight, n);
+  ALLOC(s->d_flag, 1);
+  ALLOC(s->d_counts, res);
+  ALLOC(s->d_energy, res);
+  ALLOC(s->d_stats, 16);
+  ALLOC(s->d_buie, 1025 + 1025 + 1024);
+#undef ALLOC
+  for (int i = 0; i < 5; ++i) {
+    cudaError_t ce = cudaEventCreate(&s->ev[i]);
+    if (ce != cudaSuccess) { e = cuda_error(ce, "cudaEventCreate"); goto fail; }
+  }
+  e = upload_field(s, field, 0);
+  if (e) goto fail;
+  {
+    cudaError_t ce = cudaMemset(s->d_flag, 0, sizeof(int32_t));
+    if (ce == cudaSuccess) ce = cudaMemset(s->d_stats, 0, 16 * sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+    if (ce != cudaSuccess) { e = cuda_error(ce, "scene init"); goto fail; }
+  }
+  *out = s;
+  return QMCRT_OK;
+fail:
+  qmcrt_scene_destroy(s);
+  return e;
+}
+
+qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
+  if (!s) return QMCRT_OK;
+  dev_free(s->d_pos); dev_free(s->d_size); dev_free(s->d_aim); dev_free(s->d_normal_in);
+  dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
+  dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
+  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
+  dev_free(s->d_stats); dev_free(s->d_buie);
+  for (int i = 0; i < 5; ++i)
+    if (s->ev[i]) cudaEventDestroy(s->ev[i]);
+  delete s;
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_scene_timing(qmcrt_scene* s, qmcrt_timing* t) {
+  if (!s || !t) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!s->traced) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "no trace recorded on this scene yet");
+  QM_CUDA(cudaEventSynchronize(s->ev[4]));
+  t->setup_ms = -1.f;
+  if (s->setup_timed) QM_CUDA(cudaEventElapsedTime(&t->setup_ms, s->ev[0], s->ev[1]));
+  QM_CUDA(cudaEventElapsedTime(&t->trace_kernel_ms, s->ev[2], s->ev[3]));
+  QM_CUDA(cudaEventElapsedTime(&t->finalize_ms, s->ev[3], s->ev[4]));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_scene_set_field(qmcrt_scene* s, const qmcrt_field* f, void* stream) {
+  if (!s) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  qmcrt_status e = check_field(f);
+  if (e) return e;
+  if (f->n != s->n) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "field size differs from the scene's");
+  if ((f->aim != nullptr) != s->has_aim || (f->normal != nullptr) != s->has_normal || (f->tilt != nullptr) != s->has_tilt)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "field must provide the same optional arrays as at creation");
+  for (int h = 0; h < s->n; ++h)
+    for (int i = 0; i < 3; ++i)
+      if (f->pos[3 * h + i] != s->h_pos[3 * h + i] || f->size[3 * h + i] != s->h_size[3 * h + i]) {
+        // positions/sizes define the grid bounds; they may move only within them
+        float r = 0.5f * std::sqrt(f->size[3 * h] * f->size[3 * h] + f->size[3 * h + 1] * f->size[3 * h + 1] +
+                                   f->size[3 * h + 2] * f->size[3 * h + 2]);
+        if (f->pos[3 * h + i] - r < s->gpos[i] || f->pos[3 * h + i] + r > s->gpos[i] + s->gdims[i] * s->gcell[i] ||
+            f->size[3 * h + i] > s->h_size[3 * h + i])
+          return set_error(QMCRT_ERR_INVALID_ARGUMENT, "a heliostat moved outside the scene's grid; create a new scene");
+      }
+  return upload_field(s, f, (cudaStream_t)stream);
+}
+
+qmcrt_status qmcrt_scene_set_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, void* stream) {
+  if (!s || !sun) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  return ensure_sun(s, sun, quirks, (cudaStream_t)stream);
+}
+
+qmcrt_status qmcrt_scene_grid_info(qmcrt_scene* s, qmcrt_grid_info* info) {
+  if (!s || !info) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::memcpy(info->origin, s->gpos, sizeof(info->origin));
+  std::memcpy(info->cell, s->gcell, sizeof(info->cell));
+  std::memcpy(info->dims, s->gdims, sizeof(info->dims));
+  info->cells = s->cells;
+  int32_t tot = 0;
+  if (s->d_cell_start) QM_CUDA(cudaMemcpy(&tot, s->d_cell_start + s->cells, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  info->entries = tot;
+  info->fine_div = s->fine_div;
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_scene_read_grid(qmcrt_scene* s, int32_t* h_start, int32_t* h_entries, void* stream) {
+  if (!s || !h_start) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  QM_CUDA(cudaMemcpyAsync(h_start, s->d_cell_start, (s->cells + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  if (h_entries && h_start[s->cells] > 0)
+    QM_CUDA(cudaMemcpyAsync(h_entries, s->d_entries, (size_t)h_start[s->cells] * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_scene_read_geometry(qmcrt_scene* s, double* h_normals, double* h_vertices, void* stream) {
+  if (!s) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h_normals) QM_CUDA(cudaMemcpyAsync(h_normals, s->d_normal, 3 * (size_t)s->n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (h_vertices) {
+    std::vector<double> fr(9 * (size_t)s->n);
+    QM_CUDA(cudaMemcpyAsync(fr.data(), s->d_frame, fr.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QM_CUDA(cudaStreamSynchronize(st));
+    for (int h = 0; h < s->n; ++h) {
+      const double* f = fr.data() + 9 * h;
+      double sx = s->h_size[3 * h], sy = s->h_size[3 * h + 1], sz = s->h_size[3 * h + 2];
+      const double loc[3][3] = {{-sx / 2, sy / 2, -sz / 2}, {-sx / 2, sy / 2, sz / 2}, {sx / 2, sy / 2, -sz / 2}};
+      for (int k = 0; k < 3; ++k)
+        for (int i = 0; i < 3; ++i)
+          h_vertices[9 * h + 3 * k + i] =
+              loc[k][0] * f[i] + loc[k][1] * f[3 + i] + loc[k][2] * f[6 + i] + s->h_pos[3 * h + i];
+    }
+  }
+  QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_scene_sample_points(qmcrt_scene* s, const qmcrt_trace_params* p, int64_t* points_out, void* stream) {
+  if (!s || !p) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  qmcrt_status e = ensure_points(s, p, (cudaStream_t)stream);
+  if (e) return e;
+  if (points_out) *points_out = s->points;
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_scene_read_points(qmcrt_scene* s, float* h_point_q, int32_t* h_point_helio, void* stream) {
+  if (!s) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  if (s->points <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "no points sampled yet");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h_point_q) QM_CUDA(cudaMemcpyAsync(h_point_q, s->d_point_xz, (size_t)s->points * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  if (h_point_helio) QM_CUDA(cudaMemcpyAsync(h_point_helio, s->d_point_helio, (size_t)s->points * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,302 @@
+// trace.cu — the tracing kernel and its C-ABI entry points.
+//
+// One thread per ray, rays numbered point-major so a warp's 32 rays leave
+// the same micro-heliostat point in nearly the same direction (coherent DDA
+// paths).  Per ray (map_tracing, rectgrid_raytracing.cu:155-196):
+//   1. sun sample from the Buie inverse CDF held in shared memory, Philox
+//      keyed by (seed, ray id) -> world direction through the sun frame;
+//   2. shadow test: 3D-DDA toward the sun over the uniform grid;
+//   3. slope-error normal (Gaussian theta, uniform phi), reflection;
+//   4. block test: 3D-DDA toward the reflected direction;
+//   5. receiver hit -> pixel -> count and energy deposit.
+// Precision: sampling and both traversals (the loops) run in FP32; the
+// per-ray frame products, reflection and receiver intersection run in FP64
+// so pixel indices agree with the FP64 oracle except where a hit lies within
+// ~1e-6 m of a pixel edge.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.hpp"
+#include "trace.cuh"
+
+using namespace qm;
+
+namespace qm {
+
+qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
+qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
+qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st);
+
+// ------------------------------------------------------------ finalize
+struct FinalizeArgs {
+  int64_t res;
+  const uint32_t* counts;
+  const float* energy;
+  uint32_t* out_counts;
+  float* out_energy;
+  float* out_flux;
+  float scale;
+  int accumulate;
+  unsigned long long* stats;
+};
+
+__global__ void finalize_kernel(FinalizeArgs a) {
+  double acc = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.res; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t c = a.counts[i];
+    float e = a.energy[i];
+    acc += e;
+    if (a.out_counts) a.out_counts[i] = (a.accumulate ? a.out_counts[i] : 0u) + c;
+    if (a.out_energy) a.out_energy[i] = (a.accumulate ? a.out_energy[i] : 0.f) + e;
+    if (a.out_flux) a.out_flux[i] = (a.accumulate ? a.out_flux[i] : 0.f) + e * a.scale;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc != 0) atomicAdd((double*)&a.stats[9], acc);
+}
+
+static int g_sm_count = 0;
+static int sm_count() {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+template <bool TABLES, bool RECORDS, bool STATS>
+static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<TABLES, RECORDS, STATS>,
+                                                                kTraceThreads, 0);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (int64_t)std::max(per_sm, 1) * sm_count();
+  int64_t need = ((int64_t)a.rays + kTraceThreads - 1) / kTraceThreads;
+  blocks = std::max<int64_t>(1, std::min(blocks, need));
+  trace_kernel<TABLES, RECORDS, STATS><<<(unsigned)blocks, kTraceThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool stats, cudaStream_t st) {
+  if (tables) {
+    if (records) return stats ? launch_trace<true, true, true>(a, st) : launch_trace<true, true, false>(a, st);
+    return stats ? launch_trace<true, false, true>(a, st) : launch_trace<true, false, false>(a, st);
+  }
+  if (records) return stats ? launch_trace<false, true, true>(a, st) : launch_trace<false, true, false>(a, st);
+  return stats ? launch_trace<false, false, true>(a, st) : launch_trace<false, false, false>(a, st);
+}
+
+static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
+  if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
+  if (s->buie.csr == csr) return QMCRT_OK;
+  s->buie.host.resize(1025 + 1025 + 1024);
+  float* h = s->buie.host.data();
+  buie_build(csr, h, h + 1025, h + 2050, s->buie.params);
+  QM_CUDA(cudaMemcpyAsync(s->d_buie, h, s->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  s->buie.csr = csr;
+  return QMCRT_OK;
+}
+
+static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a) {
+  double sd[3] = {sun->dir[0], sun->dir[1], sun->dir[2]};
+  double l = std::sqrt(sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]);
+  for (int i = 0; i < 3; ++i) sd[i] /= l;
+  // sun frame of local2world (global_function.cuh:14-52)
+  double u[3], n[3] = {sd[0], sd[1], sd[2]}, v[3];
+  if (std::fabs(n[0]) < 1e-6 && std::fabs(n[2]) < 1e-6) {
+    double sg = (n[1] < 0 && !(quirks & QMCRT_QUIRK_ZENITH_FRAME)) ? -1.0 : 1.0;
+    u[0] = 1; u[1] = 0; u[2] = 0;
+    n[0] = 0; n[1] = sg; n[2] = 0;
+    v[0] = 0; v[1] = 0; v[2] = sg;
+  } else {
+    double lu = std::sqrt(n[2] * n[2] + n[0] * n[0]);
+    u[0] = n[2] / lu; u[1] = 0; u[2] = -n[0] / lu;
+    v[0] = u[1] * n[2] - u[2] * n[1];
+    v[1] = u[2] * n[0] - u[0] * n[2];
+    v[2] = u[0] * n[1] - u[1] * n[0];
+    double lv = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int i = 0; i < 3; ++i) v[i] /= lv;
+  }
+  for (int i = 0; i < 3; ++i) {
+    a->su[i] = u[i];
+    a->sn[i] = n[i];
+    a->sv[i] = v[i];
+    a->sdir[i] = sd[i];
+  }
+  a->buie = s->d_buie;
+  a->b_total = s->buie.params[3];
+  a->b_core = s->buie.params[2];
+  a->b_B = s->buie.params[4];
+  a->b_C = s->buie.params[5];
+  a->b_inv = 1 / (s->buie.params[1] + 1);  // scene_instance_process.cu:135
+  a->frame = s->d_frame;
+  a->pos = s->d_pos;
+  a->size = s->d_size;
+  a->sigma = s->d_sigma;
+  a->weight = s->d_helio_weight;
+  a->crect = s->d_cell_rect;
+  a->cstart = s->d_cell_start;
+  for (int i = 0; i < 3; ++i) {
+    a->gpos[i] = s->gpos[i];
+    a->gcell[i] = s->gcell[i];
+    a->gdims[i] = s->gdims[i];
+  }
+  a->rtype = s->rg.type;
+  for (int i = 0; i < 3; ++i) {
+    a->rA[i] = s->rg.v0[i];
+    a->rE1[i] = s->rg.v1[i] - s->rg.v0[i];
+    a->rE2[i] = s->rg.v3[i] - s->rg.v0[i];
+  }
+  for (int i = 0; i < 5; ++i) a->cyl[i] = s->rg.cyl[i];
+  a->res_x = s->rg.res_x;
+  a->res_y = s->rg.res_y;
+  a->quirks = quirks;
+  a->counts = s->d_counts;
+  a->energy = s->d_energy;
+  a->stats = s->d_stats;
+}
+
+static qmcrt_status check_params(const qmcrt_trace_params* p) {
+  if (!p) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "params is NULL");
+  if (p->rays_per_point <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "rays_per_point must be positive");
+  if (!(p->reflectivity >= 0.f && p->reflectivity <= 1.f))
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "reflectivity must be in [0,1]");
+  if (p->quirks & ~QMCRT_QUIRKS_REFERENCE) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown quirk bits");
+  if (p->deposit != QMCRT_DEPOSIT_NEAREST) return set_error(QMCRT_ERR_NOT_SUPPORTED, "bilinear deposition is only used by the adjoint");
+  return QMCRT_OK;
+}
+
+static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace_params* p, TraceArgs& a,
+                                   bool tables, double weight_scale, const qmcrt_outputs* out,
+                                   qmcrt_trace_stats* stats, cudaStream_t st) {
+  int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
+  QM_CUDA(cudaMemsetAsync(s->d_counts, 0, res * sizeof(uint32_t), st));
+  QM_CUDA(cudaMemsetAsync(s->d_energy, 0, res * sizeof(float), st));
+  QM_CUDA(cudaMemsetAsync(s->d_stats, 0, 8 * sizeof(unsigned long long), st));
+  QM_CUDA(cudaMemsetAsync(s->d_stats + 9, 0, sizeof(unsigned long long), st));
+  bool records = out && (out->d_ray_flags || out->d_ray_pixel);
+  if (out) {
+    a.flags = out->d_ray_flags;
+    a.pixel = out->d_ray_pixel;
+  }
+  QM_CUDA(cudaEventRecord(s->ev[2], st));
+  QM_CUDA(dispatch(a, tables, records, stats != nullptr, st));
+  QM_CUDA(cudaEventRecord(s->ev[3], st));
+  double scale = (double)sun->dni * p->reflectivity * weight_scale / ((double)p->rays_per_point * s->rg.pixel_area);
+  FinalizeArgs f{};
+  f.res = res;
+  f.counts = s->d_counts;
+  f.energy = s->d_energy;
+  f.out_counts = out ? out->d_counts : nullptr;
+  f.out_energy = out ? out->d_energy : nullptr;
+  f.out_flux = out ? out->d_flux : nullptr;
+  f.scale = (float)scale;
+  f.accumulate = p->accumulate;
+  f.stats = s->d_stats;
+  int fb = (int)std::min<int64_t>((res + 255) / 256, 4 * sm_count());
+  finalize_kernel<<<fb, 256, 0, st>>>(f);
+  QM_CUDA(cudaGetLastError());
+  QM_CUDA(cudaEventRecord(s->ev[4], st));
+  s->traced = true;
+  if (stats) {
+    unsigned long long h[16];
+    int32_t flag = 0;
+    QM_CUDA(cudaMemcpyAsync(h, s->d_stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+    QM_CUDA(cudaMemcpyAsync(&flag, s->d_flag, sizeof(flag), cudaMemcpyDeviceToHost, st));
+    QM_CUDA(cudaStreamSynchronize(st));
+    if (flag == 1) return set_error(QMCRT_ERR_INTERNAL, "grid registrations exceeded the scene's capacity");
+    double tp, ie;
+    std::memcpy(&tp, &h[8], sizeof(double));
+    std::memcpy(&ie, &h[9], sizeof(double));
+    stats->rays = h[0];
+    stats->shadowed = h[1];
+    stats->blocked = h[2];
+    stats->hit = h[3];
+    stats->offmap = h[4];
+    stats->rect_tests = h[5];
+    stats->dda_cells = h[6];
+    stats->total_power = tp * sun->dni * p->reflectivity;
+    stats->intercepted_power = ie * sun->dni * p->reflectivity * weight_scale / p->rays_per_point;
+    stats->intercept_ratio = stats->total_power > 0 ? stats->intercepted_power / stats->total_power : 0.0;
+  }
+  return QMCRT_OK;
+}
+
+}  // namespace qm
+
+extern "C" {
+
+qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace_params* p, const qmcrt_outputs* out,
+                         qmcrt_trace_stats* stats, void* stream) {
+  if (!s || !sun) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  qmcrt_status e = check_params(p);
+  if (e) return e;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!(sun->dni >= 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "dni must be non-negative");
+  if ((e = ensure_buie(s, sun->csr, st))) return e;
+  s->setup_timed = false;
+  if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
+  if ((e = ensure_points(s, p, st))) return e;
+  TraceArgs a{};
+  fill_common(s, sun, p->quirks, &a);
+  a.rays = (uint32_t)(s->points * (int64_t)p->rays_per_point);
+  a.rpp = p->rays_per_point;
+  a.key = make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32));
+  a.item = p->item;
+  a.point_xz = s->d_point_xz;
+  a.point_helio = s->d_point_helio;
+  return run_and_finish(s, sun, p, a, false, 1.0, out, stats, st);
+}
+
+qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_table_inputs* t,
+                                const qmcrt_trace_params* p, const qmcrt_outputs* out, qmcrt_trace_stats* stats,
+                                void* stream) {
+  if (!s || !sun || !t) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  qmcrt_status e = check_params(p);
+  if (e) return e;
+  if (!t->d_sun_local || !t->d_turb_local || !t->d_start || !t->d_point_xz || !t->d_point_helio || t->table_size <= 0 ||
+      t->points <= 0 || t->rays_per_point <= 0 || t->rays_per_point != p->rays_per_point)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "incomplete table inputs");
+  if ((uint64_t)t->points * (uint64_t)t->rays_per_point > 0xFFFFFFFFull)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray count must be below 2^32");
+  cudaStream_t st = (cudaStream_t)stream;
+  s->setup_timed = false;
+  if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
+  TraceArgs a{};
+  fill_common(s, sun, p->quirks, &a);
+  a.rays = (uint32_t)(t->points * t->rays_per_point);
+  a.rpp = t->rays_per_point;
+  a.point_xz = (const float2*)t->d_point_xz;
+  a.point_helio = t->d_point_helio;
+  a.sun_local = t->d_sun_local;
+  a.turb_local = t->d_turb_local;
+  a.T = t->table_size;
+  a.start = t->d_start;
+  a.weight = nullptr;
+  // S_sub = point_spacing^2 (Gtest.cu:40)
+  double ws = (double)p->point_spacing * p->point_spacing;
+  return run_and_finish(s, sun, p, a, true, ws, out, stats, st);
+}
+
+qmcrt_status qmcrt_trace_host(qmcrt_scene* s, const qmcrt_field* field, const qmcrt_sun* sun,
+                              const qmcrt_trace_params* p, uint32_t* h_counts, float* h_flux,
+                              qmcrt_trace_stats* stats, void* stream) {
+  if (!s) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  qmcrt_status e;
+  if (field && (e = qmcrt_scene_set_field(s, field, stream))) return e;
+  qmcrt_outputs out{};
+  out.d_flux = s->d_energy;  // flux in place of the raw energy map
+  qmcrt_trace_params pp = *p;
+  pp.accumulate = 0;
+  if ((e = qmcrt_trace(s, sun, &pp, &out, stats, stream))) return e;
+  int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
+  if (h_counts) QM_CUDA(cudaMemcpyAsync(h_counts, s->d_counts, res * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (h_flux) QM_CUDA(cudaMemcpyAsync(h_flux, s->d_energy, res * sizeof(float), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,314 @@
+// trace.cuh — device side of the tracer: arguments, Buie sampling, the FP32
+// 3D-DDA any-hit traversal, the FP64 receiver intersection and the kernel.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/qmcrt.h"
+#include "common.cuh"
+
+namespace qm {
+
+constexpr int kTraceThreads = 256;
+
+struct TraceArgs {
+  // sun: frame of local2world for the sun direction, and the direction
+  double su[3], sn[3], sv[3], sdir[3];
+  // Buie table in global memory (cdf_x | cdf_y | slope) and its scalars
+  const float* buie;
+  float b_total, b_core, b_B, b_C, b_inv;
+  // field
+  const double* frame;  // [9n]
+  const float* pos;
+  const float* size;
+  const float* sigma;
+  const float* weight;  // [n] area per point; NULL -> 1
+  // grid
+  const float4* crect;
+  const int32_t* cstart;
+  float gpos[3], gcell[3];
+  int gdims[3];
+  // receiver
+  int rtype;
+  double rA[3], rE1[3], rE2[3];
+  double cyl[5];
+  int res_x, res_y;
+  // rays
+  uint32_t rays;
+  int rpp;
+  uint2 key;
+  uint32_t item;
+  uint32_t quirks;
+  const float2* point_xz;
+  const int32_t* point_helio;
+  // table mode
+  const float* sun_local;
+  const float* turb_local;
+  int64_t T;
+  const int32_t* start;
+  // outputs
+  uint32_t* counts;
+  float* energy;
+  uint8_t* flags;
+  int32_t* pixel;
+  unsigned long long* stats;
+};
+
+// max_less_index (scene_instance_process.cu:98-113) over the table in smem:
+// the largest i with cdf_y[i] <= value.
+__device__ __forceinline__ int max_less_index(const float* cdf_y, float value) {
+  int left = 0, right = 1024, mid;
+  while (left <= right) {
+    mid = (left + right) >> 1;
+    float c = cdf_y[mid];
+    if (value > c) left = mid + 1;
+    else if (value < c) right = mid - 1;
+    else return mid;
+  }
+  return right;
+}
+
+// Inverse CDF of the Buie sunshape (linear_interpolate, :115-137).  mrad.
+__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float* s_tab, float u) {
+  float uu = u * a.b_total;
+  if (uu < a.b_core) {
+    int id = max_less_index(s_tab + 1025, uu);
+    return (uu - s_tab[1025 + id]) * s_tab[2050 + id] + s_tab[id];
+  }
+  return powf((uu - a.b_core) * a.b_B + a.b_C, a.b_inv);
+}
+
+// One grid cell: any rectangle other than `own` hit at t > eps?  The
+// parallelogram test of rayParallelogramIntersect (global_function.cuh:78-105)
+// with the divisions by det folded into the comparisons.
+template <bool STATS>
+__device__ __forceinline__ bool cell_hit(const TraceArgs& a, int c, float3 o, float3 d, int own, bool selfhit,
+                                         uint32_t& ntest) {
+  int b = __ldg(a.cstart + c), e = __ldg(a.cstart + c + 1);
+  for (int k = b; k < e; ++k) {
+    float4 r0 = __ldg(a.crect + 3 * k);
+    if (__float_as_int(r0.w) == own && !selfhit) continue;
+    float4 r1 = __ldg(a.crect + 3 * k + 1);
+    float4 r2 = __ldg(a.crect + 3 * k + 2);
+    if (STATS) ++ntest;
+    float3 E1 = f3(r1.x, r1.y, r1.z), E2 = f3(r2.x, r2.y, r2.z);
+    float3 T = f3(o.x - r0.x, o.y - r0.y, o.z - r0.z);
+    float3 pv = cross(d, E2);
+    float det = dot(E1, pv);
+    if (fabsf(det) < kEps) continue;
+    float sg = det < 0.f ? -1.f : 1.f, ad = fabsf(det);
+    float un = dot(T, pv) * sg;
+    if (un < 0.f || un > ad) continue;
+    float3 qv = cross(T, E1);
+    float vn = dot(d, qv) * sg;
+    if (vn < 0.f || vn > ad) continue;
+    float tn = dot(E2, qv) * sg;
+    if (tn < kEps * ad) continue;
+    return true;
+  }
+  return false;
+}
+
+// |t / dir| with the reference's guard (absDivide, rectgrid_raytracing.cu:11-17)
+__device__ __forceinline__ float abs_div(float t, float d) {
+  return (d <= kEps && d >= -kEps) ? 2147483648.0f : fabsf(t / d);
+}
+
+// 3D-DDA any-hit (NotCollision, rectgrid_raytracing.cu:38-117).  The origin
+// cell is tested first unless QMCRT_QUIRK_SKIP_ORIGIN_CELL.
+template <bool STATS>
+__device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, uint32_t& ntest, uint32_t& ncell) {
+  const bool selfhit = a.quirks & QMCRT_QUIRK_SELF_HIT;
+  const int gx = a.gdims[0], gy = a.gdims[1], gz = a.gdims[2];
+  float rx = o.x - a.gpos[0], ry = o.y - a.gpos[1], rz = o.z - a.gpos[2];
+  int ix = min(max((int)floorf(rx / a.gcell[0]), 0), gx - 1);
+  int iy = min(max((int)floorf(ry / a.gcell[1]), 0), gy - 1);
+  int iz = min(max((int)floorf(rz / a.gcell[2]), 0), gz - 1);
+  int sx = d.x >= 0.f ? 1 : -1, sy = d.y >= 0.f ? 1 : -1, sz = d.z >= 0.f ? 1 : -1;
+  // calTMax (rectgrid_raytracing.cu:3-9)
+  float tx = abs_div(d.x >= 0.f ? (float)(ix + 1) * a.gcell[0] - rx : rx - (float)ix * a.gcell[0], d.x);
+  float ty = abs_div(d.y >= 0.f ? (float)(iy + 1) * a.gcell[1] - ry : ry - (float)iy * a.gcell[1], d.y);
+  float tz = abs_div(d.z >= 0.f ? (float)(iz + 1) * a.gcell[2] - rz : rz - (float)iz * a.gcell[2], d.z);
+  float dx = abs_div(a.gcell[0], d.x), dy = abs_div(a.gcell[1], d.y), dz = abs_div(a.gcell[2], d.z);
+  if (!(a.quirks & QMCRT_QUIRK_SKIP_ORIGIN_CELL)) {
+    if (STATS) ++ncell;
+    if (cell_hit<STATS>(a, (ix * gy + iy) * gz + iz, o, d, own, selfhit, ntest)) return true;
+  }
+  for (int guard = gx + gy + gz + 2; guard > 0; --guard) {
+    if (tx < ty) {
+      if (tx < tz) {
+        ix += sx;
+        if (ix >= gx || ix < 0) return false;
+        tx += dx;
+      } else {
+        iz += sz;
+        if (iz >= gz || iz < 0) return false;
+        tz += dz;
+      }
+    } else {
+      if (ty < tz) {
+        iy += sy;
+        if (iy >= gy || iy < 0) return false;
+        ty += dy;
+      } else {
+        iz += sz;
+        if (iz >= gz || iz < 0) return false;
+        tz += dz;
+      }
+    }
+    if (STATS) ++ncell;
+    if (cell_hit<STATS>(a, (ix * gy + iy) * gz + iz, o, d, own, selfhit, ntest)) return true;
+  }
+  return false;
+}
+
+// Receiver intersection in FP64; returns true on a hit and the pixel index
+// (-1 when the hit falls outside the map, QMCRT_QUIRK_PIXEL_EDGE only).
+__device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int& pix) {
+  double u, v;
+  if (a.rtype == QMCRT_RECEIVER_CYLINDER) {
+    double ox = o.x - a.cyl[0], oz = o.z - a.cyl[2], R = a.cyl[3], H = a.cyl[4];
+    double qa = d.x * d.x + d.z * d.z;
+    if (qa < 1e-18) return false;
+    double qb = ox * d.x + oz * d.z, qc = ox * ox + oz * oz - R * R;
+    double disc = qb * qb - qa * qc;
+    if (disc < 0) return false;
+    double sq = sqrt(disc);
+    double t = (-qb - sq) / qa;
+    double y = o.y + t * d.y - a.cyl[1];
+    if (t < 1e-6 || y < 0 || y > H) {
+      t = (-qb + sq) / qa;
+      y = o.y + t * d.y - a.cyl[1];
+      if (t < 1e-6 || y < 0 || y > H) return false;
+    }
+    double phi = atan2(oz + t * d.z, ox + t * d.x);
+    if (phi < 0) phi += 2.0 * 3.141592653589793;
+    u = y / H;
+    v = phi / (2.0 * 3.141592653589793);
+  } else {
+    d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
+    d3 pv = cross(d, E2);
+    double det = dot(E1, pv);
+    if (fabs(det) < 1e-6) return false;
+    double inv = 1.0 / det;
+    d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
+    u = dot(T, pv) * inv;
+    if (u < 0 || u > 1) return false;
+    d3 qv = cross(T, E1);
+    v = dot(d, qv) * inv;
+    if (v < 0 || v > 1) return false;
+    if (dot(E2, qv) * inv < 1e-6) return false;
+  }
+  int row = (int)(u * a.res_y), col = (int)(v * a.res_x);  // rectgrid_raytracing.cu:144
+  if (a.quirks & QMCRT_QUIRK_PIXEL_EDGE) {
+    if (row >= a.res_y || col >= a.res_x) {
+      pix = -1;
+      return true;
+    }
+  } else {
+    row = min(row, a.res_y - 1);
+    col = min(col, a.res_x - 1);
+  }
+  pix = row * a.res_x + col;
+  return true;
+}
+
+__device__ __forceinline__ d3 rnorm(d3 a) {
+  double r = rsqrt(dot(a, a));
+  return r * a;
+}
+
+template <bool TABLES, bool RECORDS, bool STATS>
+__global__ void __launch_bounds__(kTraceThreads) trace_kernel(const TraceArgs a) {
+  __shared__ float s_tab[1025 + 1025 + 1024];
+  if (!TABLES) {
+    for (int i = threadIdx.x; i < 3074; i += blockDim.x) s_tab[i] = __ldg(a.buie + i);
+    __syncthreads();
+  }
+  uint32_t n_sh = 0, n_bl = 0, n_hit = 0, n_off = 0, n_ray = 0, n_test = 0, n_cell = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride) {
+    const uint32_t ray = (uint32_t)r64;
+    const uint32_t g = ray / (uint32_t)a.rpp, j = ray - g * (uint32_t)a.rpp;
+    const int h = __ldg(a.point_helio + g);
+    const float2 xz = __ldg(a.point_xz + g);
+    const double* F = a.frame + 9 * h;
+    frame64 fr;
+    fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
+    fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
+    fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
+    const float hy = 0.5f * __ldg(a.size + 3 * h + 1);
+    d3 o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
+           apply(fr, (double)xz.x, (double)hy, (double)xz.y);
+    float3 sl, tl;
+    float w = 1.f;
+    if (TABLES) {
+      int64_t ia = ((int64_t)__ldg(a.start + g) + j) % a.T;
+      int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
+      int64_t ib = ((int64_t)__ldg(a.start + gp) + j) % a.T;
+      sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
+      tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
+    } else {
+      uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
+      float th = buie_theta_mrad(a, s_tab, u24f(r.x)) * 1e-3f;
+      float st, ct, sp, cp;
+      sincosf(th, &st, &ct);
+      sincospif(2.f * u24f(r.y), &sp, &cp);
+      sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
+      float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
+      float ths = __ldg(a.sigma + h) * z;
+      uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
+      sincosf(ths, &st, &ct);
+      sincospif(2.f * u24f(extra), &sp, &cp);
+      tl = f3(st * cp, ct, st * sp);
+      w = a.weight ? __ldg(a.weight + h) : 1.f;
+    }
+    // world sample (local2world(sample, sun_dir)), incident direction
+    d3 ws = mk(sl.x * a.su[0] + sl.y * a.sn[0] + sl.z * a.sv[0], sl.x * a.su[1] + sl.y * a.sn[1] + sl.z * a.sv[1],
+               sl.x * a.su[2] + sl.y * a.sn[2] + sl.z * a.sv[2]);
+    const float3 of = to_f(o);
+    uint8_t flag = 0;
+    int pix = -1;
+    if (dda_blocked<STATS>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, n_test, n_cell)) {
+      flag = QMCRT_RAY_SHADOWED;
+    } else {
+      d3 np = rnorm(apply(fr, (double)tl.x, (double)tl.y, (double)tl.z));
+      double di = dot(ws, np);
+      d3 rd = rnorm(ws - (2.0 * di) * np);  // reflect (i - 2 n (n.i)), normalise
+      if (dda_blocked<STATS>(a, of, to_f(rd), h, n_test, n_cell)) {
+        flag = QMCRT_RAY_BLOCKED;
+      } else if (receiver_hit(a, o, rd, pix)) {
+        flag = QMCRT_RAY_HIT;
+        if (pix < 0) {
+          flag |= QMCRT_RAY_OFFMAP;
+        } else {
+          // calEnergy (rectgrid_raytracing.cu:129-133), eta = 1
+          float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w;
+          atomicAdd(a.counts + pix, 1u);
+          atomicAdd(a.energy + pix, e);
+        }
+      }
+    }
+    if (RECORDS) {
+      if (a.flags) a.flags[ray] = flag;
+      if (a.pixel) a.pixel[ray] = pix;
+    }
+    if (STATS) {
+      ++n_ray;
+      n_sh += (flag & QMCRT_RAY_SHADOWED) != 0;
+      n_bl += (flag & QMCRT_RAY_BLOCKED) != 0;
+      n_hit += (flag & QMCRT_RAY_HIT) != 0;
+      n_off += (flag & QMCRT_RAY_OFFMAP) != 0;
+    }
+  }
+  if (STATS) {
+    unsigned long long v[7] = {n_ray, n_sh, n_bl, n_hit, n_off, n_test, n_cell};
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      unsigned long long x = v[k];
+      for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+      if ((threadIdx.x & 31) == 0 && x) atomicAdd(a.stats + k, x);
+    }
+  }
+}
+
+}  // namespace qm

@@ -1,0 +1,194 @@
+"""Python host API over the C-ABI, mirroring the reference's scene/solver surface.
+
+  SolarScene          -> SolarScene (solar_scene.h:19-50) + SceneProcessor
+  SolarScene.trace    -> results_with_given_normal's tracing loop (Gtest.cu:10-46)
+  SolarScene.trace_tables -> recthelio_ray_tracing / map_tracing on explicit
+                          sample tables (recthelio_tracing.cpp:46-80)
+  image_smooth        -> ImageSmoother::image_smooth (image_smooth.cuh:17-23)
+
+Device memory comes from torch (plumbing only); every computation runs in
+libqmcrt.so.  Errors raise capi.QmcrtError carrying the library's status.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class SolarScene:
+    def __init__(self, pos, size, receiver, grid, sigma=0.002, aim=None, normal=None, slope_sigma=None, tilt=None):
+        self.pos = np.ascontiguousarray(pos, np.float32)
+        self.size = np.ascontiguousarray(size, np.float32)
+        self.aim = None if aim is None else np.ascontiguousarray(aim, np.float32)
+        self.normal = None if normal is None else np.ascontiguousarray(normal, np.float32)
+        self.slope_sigma = None if slope_sigma is None else np.ascontiguousarray(slope_sigma, np.float32)
+        self.tilt = None if tilt is None else np.ascontiguousarray(tilt, np.float32)
+        self.sigma = float(sigma)
+        self.receiver = receiver
+        self.grid = grid
+        self.res = (receiver.res_y, receiver.res_x)
+        h = C.c_void_p()
+        capi.check(capi.lib().qmcrt_scene_create(C.byref(self.field()), C.byref(receiver), C.byref(grid), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_workload(cls, w):
+        return cls(w.pos, w.size, w.receiver, w.grid, sigma=w.sigma, aim=w.aim)
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+    def field(self):
+        f = capi.Field()
+        f.n = self.n
+        f.pos = capi.as_fp(self.pos)
+        f.size = capi.as_fp(self.size)
+        f.aim = capi.as_fp(self.aim)
+        f.normal = capi.as_fp(self.normal)
+        f.slope_sigma = capi.as_fp(self.slope_sigma)
+        f.sigma = self.sigma
+        f.tilt = capi.as_fp(self.tilt)
+        return f
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().qmcrt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_sun(self, sun, quirks=0):
+        capi.check(capi.lib().qmcrt_scene_set_sun(self.h, C.byref(sun), quirks, _stream()))
+
+    def grid_info(self):
+        gi = capi.GridInfo()
+        capi.check(capi.lib().qmcrt_scene_grid_info(self.h, C.byref(gi)))
+        return gi
+
+    def read_grid(self):
+        gi = self.grid_info()
+        start = np.zeros(gi.cells + 1, np.int32)
+        ent = np.zeros(max(gi.entries, 1), np.int32)
+        capi.check(capi.lib().qmcrt_scene_read_grid(self.h, capi.as_i32p(start), capi.as_i32p(ent), _stream()))
+        return start, ent[: start[-1]]
+
+    def read_geometry(self):
+        nrm = np.zeros((self.n, 3))
+        vert = np.zeros((self.n, 9))
+        capi.check(capi.lib().qmcrt_scene_read_geometry(self.h, nrm.ctypes.data_as(capi.dp),
+                                                        vert.ctypes.data_as(capi.dp), _stream()))
+        return nrm, vert
+
+    def sample_points(self, params):
+        n = C.c_int64()
+        capi.check(capi.lib().qmcrt_scene_sample_points(self.h, C.byref(params), C.byref(n), _stream()))
+        return n.value
+
+    def read_points(self):
+        n = self.sample_points_count
+        xz = np.zeros((n, 2), np.float32)
+        helio = np.zeros(n, np.int32)
+        capi.check(capi.lib().qmcrt_scene_read_points(self.h, capi.as_fp(xz), capi.as_i32p(helio), _stream()))
+        return xz, helio
+
+    def points(self, params):
+        self.sample_points_count = self.sample_points(params)
+        return self.read_points()
+
+    def _outputs(self, rays, records, maps=True):
+        dev = torch.device("cuda")
+        r = {}
+        o = capi.Outputs()
+        if maps:
+            r["counts"] = torch.zeros(self.res, dtype=torch.int32, device=dev)
+            r["energy"] = torch.zeros(self.res, dtype=torch.float32, device=dev)
+            r["flux"] = torch.zeros(self.res, dtype=torch.float32, device=dev)
+            o.d_counts, o.d_energy, o.d_flux = (r[k].data_ptr() for k in ("counts", "energy", "flux"))
+        if records:
+            r["flags"] = torch.zeros(rays, dtype=torch.uint8, device=dev)
+            r["pixel"] = torch.zeros(rays, dtype=torch.int32, device=dev)
+            o.d_ray_flags, o.d_ray_pixel = r["flags"].data_ptr(), r["pixel"].data_ptr()
+        return o, r
+
+    def trace(self, sun, params, records=False, stats=True, outputs=None):
+        """Full trace; returns device maps (and per-ray records) plus stats."""
+        rays = int(params.rays)
+        if params.point_mode == capi.POINTS_GRID:
+            rays = self.sample_points(params) * params.rays_per_point
+        self.sample_points_count = rays // params.rays_per_point
+        if outputs is None:
+            o, r = self._outputs(rays, records)
+        else:
+            o, r = outputs
+        st = capi.TraceStats() if stats else None
+        capi.check(capi.lib().qmcrt_trace(self.h, C.byref(sun), C.byref(params), C.byref(o),
+                                          C.byref(st) if stats else None, _stream()))
+        r["stats"] = st
+        return r
+
+    def trace_tables(self, sun, params, sun_local, turb_local, start, point_xz, point_helio, records=True,
+                     stats=True):
+        dev = torch.device("cuda")
+        t = {k: torch.as_tensor(np.ascontiguousarray(v), device=dev)
+             for k, v in (("sl", np.asarray(sun_local, np.float32)), ("tl", np.asarray(turb_local, np.float32)),
+                          ("st", np.asarray(start, np.int32)), ("xz", np.asarray(point_xz, np.float32)),
+                          ("ph", np.asarray(point_helio, np.int32)))}
+        ti = capi.TableInputs()
+        ti.d_sun_local, ti.d_turb_local = t["sl"].data_ptr(), t["tl"].data_ptr()
+        ti.table_size = t["sl"].shape[0]
+        ti.d_start, ti.d_point_xz, ti.d_point_helio = t["st"].data_ptr(), t["xz"].data_ptr(), t["ph"].data_ptr()
+        ti.points = t["st"].shape[0]
+        ti.rays_per_point = params.rays_per_point
+        rays = ti.points * ti.rays_per_point
+        o, r = self._outputs(rays, records)
+        st = capi.TraceStats() if stats else None
+        capi.check(capi.lib().qmcrt_trace_tables(self.h, C.byref(sun), C.byref(ti), C.byref(params), C.byref(o),
+                                                 C.byref(st) if stats else None, _stream()))
+        torch.cuda.current_stream().synchronize()
+        r["stats"] = st
+        return r
+
+    def timing(self):
+        t = capi.Timing()
+        capi.check(capi.lib().qmcrt_scene_timing(self.h, C.byref(t)))
+        return t
+
+    def trace_host(self, sun, params, stats=True):
+        """End-to-end call on host buffers (uploads the field, downloads maps)."""
+        counts = np.zeros(self.res, np.uint32)
+        flux = np.zeros(self.res, np.float32)
+        st = capi.TraceStats()
+        capi.check(capi.lib().qmcrt_trace_host(self.h, C.byref(self.field()), C.byref(sun), C.byref(params),
+                                               capi.as_u32p(counts), capi.as_fp(flux),
+                                               C.byref(st) if stats else None, _stream()))
+        return counts, flux, st
+
+
+def image_smooth(d_map, radius, ratio, method=capi.TRIM_SORTED):
+    """Trimmed-mean smoothing of a device map (uint32/int32 counts or float32)."""
+    assert d_map.is_cuda and d_map.is_contiguous() and d_map.dim() == 2
+    out = torch.empty(d_map.shape, dtype=torch.float32, device=d_map.device)
+    h, w = d_map.shape
+    if d_map.dtype in (torch.int32, torch.uint32):
+        f = capi.lib().qmcrt_smooth_trimmed_u32
+    elif d_map.dtype == torch.float32:
+        f = capi.lib().qmcrt_smooth_trimmed_f32
+    else:
+        raise TypeError("map must be int32/uint32 counts or float32")
+    capi.check(f(_ptr(d_map), _ptr(out), w, h, radius, C.c_float(ratio), method, _stream()))
+    return out

@@ -1,0 +1,178 @@
+"""Synthetic heliostat-field workloads with the shapes the tracer is measured on.
+
+No public dataset is involved: every field is generated by the library's
+radial-staggered layout generator from a fixed seed.  Sizes:
+
+  small  100 heliostats 2x2 m, tower 80 m, flat 5x5 m receiver at 128x128,
+         sun 45 deg elevation / 180 deg azimuth, CSR 0.1, slope 2 mrad,
+         16 Poisson points (0.3 m spacing) x 256 rays, 10 m cells.
+  mid    1000 heliostats 10x10 m out to 600 m, tower 150 m, flat 12x12 m
+         receiver at 256x256, aim offsets N(0, 0.5 m), sun 30 deg, CSR 0.05,
+         slope 2.5 mrad, 2^28 rays, 25 m cells.
+  large  10000 heliostats 11x11 m surround field out to 1300 m, tower 200 m,
+         cylinder R 8 m x H 18 m unrolled to 512x256, sun 20 deg, CSR 0.2,
+         slope 3 mrad, 2^31 rays, 12.5 m cells.
+"""
+import ctypes as C
+from dataclasses import dataclass, field as dfield
+
+import numpy as np
+
+from . import capi
+
+FIELD_SEED = 20261203
+
+
+@dataclass
+class Workload:
+    name: str
+    pos: np.ndarray
+    size: np.ndarray
+    sigma: float
+    receiver: capi.Receiver
+    grid: capi.GridParams
+    sun: capi.Sun
+    params: capi.TraceParams
+    aim: np.ndarray = None
+    smooth_radius: int = 2
+    smooth_ratio: float = 0.2
+    extra: dict = dfield(default_factory=dict)
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+    @property
+    def res(self):
+        return (self.receiver.res_y, self.receiver.res_x)
+
+    def field_struct(self):
+        """ctypes Field pointing into this workload's arrays (keep self alive)."""
+        f = capi.Field()
+        f.n = self.n
+        f.pos = capi.as_fp(self.pos)
+        f.size = capi.as_fp(self.size)
+        f.aim = capi.as_fp(self.aim) if self.aim is not None else None
+        f.normal = None
+        f.slope_sigma = None
+        f.sigma = self.sigma
+        f.tilt = None
+        return f
+
+
+def layout(n, w, h, r_min, r_max, az_center=0.0, az_span=120.0, spacing=0.0, jitter=0.0, mount=None, seed=FIELD_SEED):
+    p = capi.LayoutParams()
+    p.n = n
+    p.helio_w, p.helio_h = w, h
+    p.thickness = 0.05
+    p.r_min, p.r_max = r_min, r_max
+    p.az_center_deg, p.az_span_deg = az_center, az_span
+    p.spacing = spacing
+    p.jitter = jitter
+    p.mount_height = mount if mount is not None else 0.5 * h + 0.5
+    p.seed = seed
+    pos = np.zeros((n, 3), np.float32)
+    got = C.c_int32()
+    capi.check(capi.lib().qmcrt_layout_radial_staggered(C.byref(p), capi.as_fp(pos), n, C.byref(got)))
+    return pos
+
+
+def sun_dir(elev, azim):
+    d = (C.c_float * 3)()
+    capi.check(capi.lib().qmcrt_sun_direction(elev, azim, d))
+    return [d[0], d[1], d[2]]
+
+
+def make_sun(elev, azim, dni=1000.0, csr=0.1):
+    s = capi.Sun()
+    s.dir[:] = sun_dir(elev, azim)
+    s.dni = dni
+    s.csr = csr
+    return s
+
+
+def flat_receiver(tower, w, h, res_x, res_y, normal=(0.0, 0.0, -1.0)):
+    r = capi.Receiver()
+    r.type = capi.RECEIVER_FLAT
+    r.pos[:] = [0.0, tower, 0.0]
+    r.size[:] = [w, h, 0.0]
+    r.normal[:] = list(normal)
+    r.face = 0
+    r.res_x, r.res_y = res_x, res_y
+    return r
+
+
+def cylinder_receiver(tower, radius, height, res_x, res_y):
+    r = capi.Receiver()
+    r.type = capi.RECEIVER_CYLINDER
+    r.pos[:] = [0.0, tower - height / 2.0, 0.0]
+    r.size[:] = [radius, height, 0.0]
+    r.normal[:] = [0.0, 0.0, -1.0]
+    r.face = 0
+    r.res_x, r.res_y = res_x, res_y
+    return r
+
+
+def grid(cell, margin=1.0):
+    g = capi.GridParams()
+    g.cell[:] = [cell, cell, cell]
+    g.margin = margin
+    g.explicit_bounds = 0
+    g.fine_div = 1
+    return g
+
+
+def params(rays, rpp, spacing, seed=7, quirks=0, mode=capi.POINTS_POISSON):
+    p = capi.TraceParams()
+    p.seed = seed
+    p.rays = rays
+    p.rays_per_point = rpp
+    p.point_mode = mode
+    p.point_spacing = spacing
+    p.reflectivity = 0.88
+    p.quirks = quirks
+    p.deposit = capi.DEPOSIT_NEAREST
+    p.accumulate = 0
+    p.kernel_variant = 0
+    return p
+
+
+def small(rays=None, seed=7):
+    """100 heliostats, 16 points x 256 rays (409 600 rays)."""
+    n = 100
+    pos = layout(n, 2.0, 2.0, 40.0, 200.0, spacing=3.4, jitter=0.2, mount=1.6)
+    size = np.tile(np.array([[2.0, 0.05, 2.0]], np.float32), (n, 1))
+    rays = rays or n * 16 * 256
+    return Workload("small", pos, size, 0.002, flat_receiver(80.0, 5.0, 5.0, 128, 128), grid(10.0),
+                    make_sun(45.0, 180.0, 1000.0, 0.1), params(rays, 256, 0.3, seed))
+
+
+def mid(rays=1 << 28, seed=7):
+    """1000 heliostats 10x10 m to 600 m, 2^28 rays."""
+    n = 1000
+    pos = layout(n, 10.0, 10.0, 100.0, 600.0, jitter=0.0, mount=6.0)
+    size = np.tile(np.array([[10.0, 0.1, 10.0]], np.float32), (n, 1))
+    rec = flat_receiver(150.0, 12.0, 12.0, 256, 256)
+    rng = np.random.default_rng(FIELD_SEED + 1)
+    off = rng.normal(0.0, 0.5, (n, 2)).astype(np.float32)
+    # receiver plane basis: width along x, height along y (normal -z)
+    aim = np.zeros((n, 3), np.float32)
+    aim[:, 0] = off[:, 0]
+    aim[:, 1] = 150.0 + off[:, 1]
+    aim[:, 2] = 0.0
+    w = Workload("mid", pos, size, 0.0025, rec, grid(25.0), make_sun(30.0, 180.0, 1000.0, 0.05),
+                 params(rays, 256, 0.18, seed), aim=aim)
+    return w
+
+
+def large(rays=1 << 31, seed=7):
+    """10 000 heliostats 11x11 m surround field to 1300 m, cylinder receiver, 2^31 rays."""
+    n = 10000
+    pos = layout(n, 11.0, 11.0, 120.0, 1300.0, az_center=0.0, az_span=360.0, mount=6.5)
+    size = np.tile(np.array([[11.0, 0.1, 11.0]], np.float32), (n, 1))
+    rec = cylinder_receiver(200.0, 8.0, 18.0, 512, 256)
+    return Workload("large", pos, size, 0.003, rec, grid(12.5), make_sun(20.0, 180.0, 1000.0, 0.2),
+                    params(rays, 256, 0.22, seed))
+
+
+BUILDERS = {"small": small, "mid": mid, "large": large}

@@ -1,0 +1,353 @@
+"""CUDA path against the FP64 oracle, through the C-ABI.
+
+Bar (per ray, on identical sample streams): shadow/block/hit flags and pixel
+indices agree on >= 99.99% of rays, and every pixel disagreement is between
+adjacent pixels (a hit on a pixel edge).  Integer count maps agree exactly
+wherever the per-ray records agree; the float energy/flux maps agree to the
+relative tolerances written in each test.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from onemirror_b200 import capi, workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from onemirror_b200.scene import SolarScene, image_smooth  # noqa: E402
+
+AGREE = 0.9999
+
+
+def oracle_scene(w, sc, sun, quirks=0, use_gpu_grid=True):
+    gi = sc.grid_info()
+    csr = sc.read_grid() if use_gpu_grid else None
+    return O.Scene(w.pos, w.size, w.sigma, w.receiver, w.grid.cell[0], w.grid.margin, list(sun.dir), quirks=quirks,
+                   aim=w.aim, grid_csr=csr, grid_bounds=(list(gi.origin), list(gi.cell), list(gi.dims)))
+
+
+def compare_records(gf, gp, of, op, res_x):
+    gf, gp, of, op = (np.asarray(a) for a in (gf, gp, of, op))
+    same = (gf == of) & (gp == op)
+    frac = same.mean()
+    bad = np.nonzero(gp != op)[0]
+    both = bad[(gp[bad] >= 0) & (op[bad] >= 0)]
+    # pixel disagreements on rays both sides trace to the receiver must be
+    # neighbouring pixels: the hit lies on a pixel edge
+    dr = np.abs(gp[both] // res_x - op[both] // res_x)
+    dc = np.abs(gp[both] % res_x - op[both] % res_x)
+    assert np.all((dr <= 1) & (dc <= 1)), "non-adjacent pixel disagreement"
+    return frac, int((~same).sum())
+
+
+@pytest.fixture(scope="module")
+def small():
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    yield w, sc
+    sc.close()
+
+
+def test_philox_kernel_equals_oracle():
+    n = 4096
+    out = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    ctr = (C.c_uint32 * 4)(7, 0xFFFFFFF0, 3, 0x51A7)
+    key = (C.c_uint32 * 2)(0xDEADBEEF, 12345)
+    capi.check(capi.lib().qmcrt_philox_blocks(ctr, key, n, C.c_void_p(out.data_ptr()), None))
+    g = out.cpu().numpy().view(np.uint32)
+    for i in list(range(0, n, 97)) + [n - 1]:
+        ref = O.philox([(7 + i) & 0xFFFFFFFF, 0xFFFFFFF0, 3, 0x51A7], [0xDEADBEEF, 12345])
+        assert np.array_equal(g[i], ref)
+
+
+def test_philox_matches_curand():
+    """The in-kernel generator is cuRAND's Philox4_32_10 stream for the same key/counter."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "cuda"))
+    import build as cb
+    L = C.CDLL(cb.build())
+    L.curand_ref_philox.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_void_p]
+    n = 512
+    seed = 0x0123456789ABCDEF
+    for sub0, k in [(0, 0), (1 << 33, 5), (77, 1000)]:
+        out = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+        assert L.curand_ref_philox(seed, sub0, k, n, out.data_ptr()) == 0
+        g = out.cpu().numpy().view(np.uint32)
+        for i in range(0, n, 37):
+            s = sub0 + i
+            ref = O.philox([k, 0, s & 0xFFFFFFFF, s >> 32], [seed & 0xFFFFFFFF, seed >> 32])
+            assert np.array_equal(g[i], ref), (sub0, k, i)
+
+
+def test_poisson_points_bit_exact(small):
+    w, sc = small
+    xz, helio = sc.points(w.params)
+    oxz, oh = O.points_poisson(w.size, int(w.params.rays // w.params.rays_per_point), w.params.point_spacing,
+                               w.params.seed)
+    assert np.array_equal(helio, oh)
+    assert xz.tobytes() == oxz.tobytes()
+
+
+def test_poisson_points_bit_exact_large_mirrors():
+    w = W.mid(rays=1 << 22)
+    n = 40
+    pos, size = w.pos[:n].copy(), w.size[:n].copy()
+    sc = SolarScene(pos, size, w.receiver, w.grid, sigma=w.sigma)
+    p = W.params(n * 1000 * 64, 64, 0.18, seed=99)
+    xz, helio = sc.points(p)
+    oxz, oh = O.points_poisson(size, n * 1000, 0.18, 99)
+    assert np.array_equal(helio, oh) and xz.tobytes() == oxz.tobytes()
+    sc.close()
+
+
+def test_poisson_too_dense_reports_sampling_error():
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    p = W.params(w.n * 500 * 32, 32, 0.3)  # 500 points 0.3 m apart cannot fit on 2x2 m
+    with pytest.raises(capi.QmcrtError) as e:
+        sc.sample_points(p)
+    assert e.value.status == capi.ERR_SAMPLING
+    sc.close()
+
+
+def test_grid_points_match_reference_formula(small):
+    w, sc = small
+    p = W.params(0, 16, 0.25, mode=capi.POINTS_GRID)
+    xz, helio = sc.points(p)
+    oxz, oh = O.points_grid(w.size, 0.25)
+    assert np.array_equal(helio, oh) and xz.tobytes() == oxz.tobytes()
+
+
+@pytest.mark.parametrize("quirks", [0, capi.QUIRK_AABB_RADIUS])
+def test_geometry_and_grid_equal_oracle(small, quirks):
+    w, sc = small
+    sc.set_sun(w.sun, quirks)
+    nrm, vert = sc.read_geometry()
+    ref = oracle_scene(w, sc, w.sun, quirks, use_gpu_grid=False)
+    assert np.allclose(nrm, ref.normal, atol=1e-13)
+    assert np.allclose(vert, ref.vert, atol=1e-10)
+    start, ent = sc.read_grid()
+    assert np.array_equal(start, ref.cell_start)
+    assert np.array_equal(ent, ref.entries[: start[-1]])
+
+
+def run_pair(w, sc, sun, params, quirks=0):
+    params.quirks = quirks
+    g = sc.trace(sun, params, records=True)
+    torch.cuda.synchronize()
+    ref = oracle_scene(w, sc, sun, quirks)
+    xz, helio = sc.read_points()
+    weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
+    cfg = ref.cfg(sun.csr, params.seed, int(params.rays), params.rays_per_point, xz, helio, weight, quirks=quirks,
+                  item=params.item)
+    o = ref.trace_philox(cfg)
+    return g, o
+
+
+def check_pair(w, g, o, min_events=0):
+    frac, nbad = compare_records(g["flags"].cpu().numpy(), g["pixel"].cpu().numpy(), o["flags"], o["pixel"],
+                                 w.receiver.res_x)
+    assert frac >= AGREE, (frac, nbad)
+    st = g["stats"]
+    assert st.rays == o["stats"][0]
+    assert abs(int(st.shadowed) - o["stats"][1]) <= nbad and abs(int(st.blocked) - o["stats"][2]) <= nbad
+    assert st.shadowed + st.blocked >= min_events
+    gc = g["counts"].cpu().numpy().ravel().astype(np.int64)
+    oc = o["counts"].astype(np.int64)
+    assert gc.sum() == st.hit - st.offmap
+    assert np.abs(gc - oc).sum() <= 2 * nbad
+    if nbad == 0:
+        assert np.array_equal(gc, oc)
+    ge = g["energy"].cpu().numpy().ravel().astype(np.float64)
+    tol = 1e-5 * ge.max() + 2.0 * nbad * (o["energy"].max() / max(oc.max(), 1))
+    assert np.abs(ge - o["energy"]).max() <= tol
+    return frac, nbad
+
+
+def test_trace_small_records_equal_oracle(small):
+    w, sc = small
+    g, o = run_pair(w, sc, w.sun, w.params)
+    frac, nbad = check_pair(w, g, o)
+    st = g["stats"]
+    # the whole-map totals
+    assert abs(st.intercepted_power - (g["flux"].sum().item() * sc_pixel_area(w))) / st.intercepted_power < 1e-4
+    assert 0.5 < st.intercept_ratio <= 1.0
+
+
+def sc_pixel_area(w):
+    return (w.receiver.size[0] / w.receiver.res_x) * (w.receiver.size[1] / w.receiver.res_y)
+
+
+def test_trace_low_sun_shadow_and_block_equal_oracle(small):
+    w, sc = small
+    sun = W.make_sun(12.0, 200.0, 950.0, 0.1)
+    p = W.params(int(w.params.rays), 256, 0.3, seed=21)
+    g, o = run_pair(w, sc, sun, p)
+    check_pair(w, g, o, min_events=20000)
+
+
+def test_trace_reference_quirks_equal_oracle(small):
+    w, sc = small
+    sun = W.make_sun(14.0, 160.0, 1000.0, 0.2)
+    q = capi.QUIRK_SKIP_ORIGIN_CELL | capi.QUIRK_AABB_RADIUS | capi.QUIRK_PIXEL_EDGE
+    p = W.params(int(w.params.rays), 256, 0.3, seed=5)
+    g, o = run_pair(w, sc, sun, p, quirks=q)
+    check_pair(w, g, o)
+
+
+def test_trace_tables_mode_equals_oracle(small):
+    """Parity mode: explicit sun/perturbation tables, the map_tracing sampling structure."""
+    w, sc = small
+    sun = W.make_sun(18.0, 190.0, 1000.0, 0.1)
+    T = 8192
+    rng = np.random.default_rng(8)
+    th = rng.random(T) * 0.009
+    ph = rng.random(T) * 2 * np.pi
+    sun_local = np.stack([np.sin(th) * np.cos(ph), np.cos(th), np.sin(th) * np.sin(ph)], 1).astype(np.float32)
+    ts = rng.normal(0, 0.002, T)
+    tp = rng.random(T) * 2 * np.pi
+    turb_local = np.stack([np.sin(ts) * np.cos(tp), np.cos(ts), np.sin(ts) * np.sin(tp)], 1).astype(np.float32)
+    xz, helio = O.points_grid(w.size, 0.25)
+    start = rng.integers(0, T, len(helio)).astype(np.int32)
+    rpp = 64
+    for quirks in (0, capi.QUIRKS_REFERENCE & ~capi.QUIRK_ZENITH_FRAME):
+        p = W.params(0, rpp, 0.25, seed=1, quirks=quirks)
+        g = sc.trace_tables(sun, p, sun_local, turb_local, start, xz, helio)
+        ref = oracle_scene(w, sc, sun, quirks)
+        cfg = ref.cfg(sun.csr, 1, len(helio) * rpp, rpp, xz, helio, quirks=quirks)
+        o = ref.trace_tables(cfg, sun_local, turb_local, start)
+        frac, nbad = compare_records(g["flags"].cpu().numpy(), g["pixel"].cpu().numpy(), o["flags"], o["pixel"],
+                                     w.receiver.res_x)
+        assert frac >= AGREE, (quirks, frac, nbad)
+        # flux scaling of the reference driver: DNI * S_sub * rho / N_c / S_rec (Gtest.cu:40-46)
+        e = g["energy"].cpu().numpy().astype(np.float64)
+        f = g["flux"].cpu().numpy().astype(np.float64)
+        scale = 1000.0 * 0.25 ** 2 * 0.88 / rpp / sc_pixel_area(w)
+        assert np.allclose(f, e * scale, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("name", ["mid", "large"])
+def test_big_fields_on_ray_ranges(name):
+    """Mid (flat receiver) and large (cylinder) geometry: records of ray ranges spread over the field."""
+    w = W.BUILDERS[name](rays=1 << 24)
+    sc = SolarScene.from_workload(w)
+    g = sc.trace(w.sun, w.params, records=True)
+    torch.cuda.synchronize()
+    ref = oracle_scene(w, sc, w.sun)
+    xz, helio = sc.read_points()
+    weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
+    gf = g["flags"].cpu().numpy()
+    gp = g["pixel"].cpu().numpy()
+    R = int(w.params.rays)
+    total_bad, total = 0, 0
+    for b in np.linspace(0, R - (1 << 15), 12).astype(np.int64):
+        cfg = ref.cfg(w.sun.csr, w.params.seed, R, 256, xz, helio, weight, ray_begin=int(b), ray_end=int(b) + (1 << 15))
+        o = ref.trace_philox(cfg, maps=False)
+        frac, nbad = compare_records(gf[b:b + (1 << 15)], gp[b:b + (1 << 15)], o["flags"], o["pixel"],
+                                     w.receiver.res_x)
+        total_bad += nbad
+        total += 1 << 15
+    assert 1 - total_bad / total >= AGREE, (total_bad, total)
+    st = g["stats"]
+    assert g["counts"].sum().item() == st.hit - st.offmap
+    sc.close()
+
+
+def test_smoothing_u32_sorted_bit_exact():
+    rng = np.random.default_rng(4)
+    for (h, w_), r, ratio in [((128, 128), 2, 0.2), ((67, 201), 3, 0.1), ((1, 1), 2, 0.2), ((5, 300), 7, 0.45),
+                              ((64, 64), 0, 0.2), ((40, 33), 2, 0.0)]:
+        img = rng.integers(0, 5000, (h, w_)).astype(np.uint32)
+        img[rng.random(img.shape) < 0.3] = 0
+        d = torch.as_tensor(img.view(np.int32), device="cuda")
+        out = image_smooth(d, r, ratio, capi.TRIM_SORTED).cpu().numpy()
+        ref = O.smooth_u32(img, r, ratio, 0)
+        assert out.tobytes() == ref.tobytes(), (h, w_, r, ratio)
+
+
+def test_smoothing_heaps_bit_exact_float_and_counts():
+    rng = np.random.default_rng(5)
+    imgf = (rng.random((96, 130)) * 100).astype(np.float32)
+    imgf[rng.random(imgf.shape) < 0.4] = 0
+    for r, ratio in [(2, 0.2), (5, 0.02), (1, 0.3)]:
+        out = image_smooth(torch.as_tensor(imgf, device="cuda"), r, ratio, capi.TRIM_HEAPS).cpu().numpy()
+        assert out.tobytes() == O.smooth_f32(imgf, r, ratio, 1).tobytes()
+    imgu = rng.integers(0, 1000, (50, 70)).astype(np.uint32)
+    out = image_smooth(torch.as_tensor(imgu.view(np.int32), device="cuda"), 2, 0.2, capi.TRIM_HEAPS).cpu().numpy()
+    assert out.tobytes() == O.smooth_u32(imgu, 2, 0.2, 1).tobytes()
+    # float maps, sorted definition: FP32 sums against the FP64 oracle
+    out = image_smooth(torch.as_tensor(imgf, device="cuda"), 2, 0.2, capi.TRIM_SORTED).cpu().numpy()
+    assert np.allclose(out, O.smooth_f32(imgf, 2, 0.2, 0), rtol=1e-5, atol=1e-5)
+
+
+def test_smoothing_of_traced_counts_bit_exact(small):
+    w, sc = small
+    g = sc.trace(w.sun, w.params)
+    out = image_smooth(g["counts"], w.smooth_radius, w.smooth_ratio, capi.TRIM_SORTED).cpu().numpy()
+    ref = O.smooth_u32(g["counts"].cpu().numpy().view(np.uint32), w.smooth_radius, w.smooth_ratio, 0)
+    assert out.tobytes() == ref.tobytes()
+
+
+def test_smoothing_argument_errors():
+    d = torch.zeros((8, 8), dtype=torch.float32, device="cuda")
+    with pytest.raises(capi.QmcrtError):
+        capi.check(capi.lib().qmcrt_smooth_trimmed_f32(C.c_void_p(d.data_ptr()), C.c_void_p(d.data_ptr()), 8, 8, 2,
+                                                       C.c_float(0.2), 0, None))
+    with pytest.raises(capi.QmcrtError):
+        image_smooth(d, 9, 0.2)
+    with pytest.raises(capi.QmcrtError):
+        image_smooth(d, 2, 0.6)
+
+
+def test_full_size_properties_mid():
+    """2^28 rays: count-map sum equals hits, reruns reproduce counts exactly, disjoint items differ."""
+    w = W.mid()
+    sc = SolarScene.from_workload(w)
+    a = sc.trace(w.sun, w.params)
+    ca = a["counts"].clone()
+    b = sc.trace(w.sun, w.params)
+    st = a["stats"]
+    assert st.rays == 1 << 28
+    assert ca.sum().item() == st.hit - st.offmap
+    assert torch.equal(ca, b["counts"])
+    assert torch.allclose(a["energy"], b["energy"], rtol=1e-4, atol=1e-3)
+    w.params.item = 1
+    c = sc.trace(w.sun, w.params)
+    assert not torch.equal(ca, c["counts"])
+    rel = abs(c["stats"].intercepted_power - st.intercepted_power) / st.intercepted_power
+    assert rel < 1e-3  # two independent 2^28-ray estimates of the same power
+    sc.close()
+
+
+def test_host_entry_point_matches_device_path(small):
+    w, sc = small
+    counts, flux, st = sc.trace_host(w.sun, w.params)
+    g = sc.trace(w.sun, w.params)
+    assert np.array_equal(counts.view(np.int32), g["counts"].cpu().numpy())
+    assert np.allclose(flux, g["flux"].cpu().numpy(), rtol=1e-4, atol=1e-2)
+
+
+def test_trace_argument_errors(small):
+    w, sc = small
+    p = W.params(1001, 256, 0.3)
+    with pytest.raises(capi.QmcrtError) as e:
+        sc.trace(w.sun, p)
+    assert e.value.status == capi.ERR_INVALID_ARGUMENT
+    bad = W.make_sun(45, 180)
+    bad.csr = 0.0
+    with pytest.raises(capi.QmcrtError):
+        sc.trace(bad, w.params)
+    p = W.params(int(w.params.rays), 256, 0.3)
+    p.quirks = 1 << 20
+    with pytest.raises(capi.QmcrtError):
+        sc.trace(w.sun, p)
+    # the scene still works after rejected calls
+    g = sc.trace(w.sun, w.params)
+    assert g["stats"].rays == w.params.rays
