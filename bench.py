@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling runs; multiple of 256)")
     return ap.parse_args()
 
 
@@ -203,7 +204,7 @@ def b200_arm(a, rank, world, local):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    w = W.BUILDERS[a.workload]()
+    w = W.BUILDERS[a.workload](rays=a.rays) if a.rays else W.BUILDERS[a.workload]()
     sc = SolarScene.from_workload(w)
     p = w.params
     rays = int(p.rays)

@@ -353,10 +353,12 @@ qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st)
     QM_CUDA(cudaMemcpyAsync(s->d_sigma, sg.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
     QM_CUDA(cudaStreamSynchronize(st));  // sg is a temporary
   }
+  // sample points depend only on the mirror sizes (and the trace parameters)
+  bool sizes_changed = s->h_size.size() != 3 * n || std::memcmp(s->h_size.data(), f->size, 3 * n * sizeof(float)) != 0;
   s->h_pos.assign(f->pos, f->pos + 3 * n);
   s->h_size.assign(f->size, f->size + 3 * n);
   s->field_version++;
-  s->points_key = PointsKey{};
+  if (sizes_changed) s->points_key = PointsKey{};
   return QMCRT_OK;
 }
 

@@ -131,6 +131,7 @@ static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, T
   a->b_B = s->buie.params[4];
   a->b_C = s->buie.params[5];
   a->b_inv = 1 / (s->buie.params[1] + 1);  // scene_instance_process.cu:135
+  a->n_helio = s->n;
   a->frame = s->d_frame;
   a->pos = s->d_pos;
   a->size = s->d_size;

@@ -33,6 +33,7 @@ struct TraceArgs {
   double cyl[5];
   int res_x, res_y;
   // rays
+  int n_helio;
   uint32_t rays;
   int rpp;
   uint2 key;
@@ -230,6 +231,13 @@ __global__ void __launch_bounds__(kTraceThreads) trace_kernel(const TraceArgs a)
     const uint32_t ray = (uint32_t)r64;
     const uint32_t g = ray / (uint32_t)a.rpp, j = ray - g * (uint32_t)a.rpp;
     const int h = __ldg(a.point_helio + g);
+    if (TABLES && (h < 0 || h >= a.n_helio)) {  // caller-provided ids: skip, never index out of range
+      if (RECORDS) {
+        if (a.flags) a.flags[ray] = 0;
+        if (a.pixel) a.pixel[ray] = -1;
+      }
+      continue;
+    }
     const float2 xz = __ldg(a.point_xz + g);
     const double* F = a.frame + 9 * h;
     frame64 fr;
@@ -242,9 +250,10 @@ __global__ void __launch_bounds__(kTraceThreads) trace_kernel(const TraceArgs a)
     float3 sl, tl;
     float w = 1.f;
     if (TABLES) {
-      int64_t ia = ((int64_t)__ldg(a.start + g) + j) % a.T;
+      // (start + j) mod T, kept in [0, T) for any caller-provided start
+      int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
       int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
-      int64_t ib = ((int64_t)__ldg(a.start + gp) + j) % a.T;
+      int64_t ib = (((int64_t)__ldg(a.start + gp) + j) % a.T + a.T) % a.T;
       sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
       tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
     } else {

@@ -217,7 +217,9 @@ def test_trace_tables_mode_equals_oracle(small):
     xz, helio = O.points_grid(w.size, 0.25)
     start = rng.integers(0, T, len(helio)).astype(np.int32)
     rpp = 64
-    for quirks in (0, capi.QUIRKS_REFERENCE & ~capi.QUIRK_ZENITH_FRAME):
+    # every reference quirk except SELF_HIT, whose outcome is FP32 rounding
+    # noise of t around 0 on the ray's own mirror (test_self_hit_quirk_...)
+    for quirks in (0, capi.QUIRKS_REFERENCE & ~capi.QUIRK_ZENITH_FRAME & ~capi.QUIRK_SELF_HIT):
         p = W.params(0, rpp, 0.25, seed=1, quirks=quirks)
         g = sc.trace_tables(sun, p, sun_local, turb_local, start, xz, helio)
         ref = oracle_scene(w, sc, sun, quirks)
@@ -231,6 +233,26 @@ def test_trace_tables_mode_equals_oracle(small):
         f = g["flux"].cpu().numpy().astype(np.float64)
         scale = 1000.0 * 0.25 ** 2 * 0.88 / rpp / sc_pixel_area(w)
         assert np.allclose(f, e * scale, rtol=1e-6, atol=1e-6)
+
+
+def test_self_hit_quirk_only_adds_self_shadowing(small):
+    """QMCRT_QUIRK_SELF_HIT drops the own-heliostat exclusion, leaving only the
+    reference's t > 1e-6 test (global_function.cuh:101-102).  Rays start on
+    their own mirror, so whether that mirror 'shadows' them depends on the
+    rounding of t around 0: in FP32 a fraction of rays self-shadow, in the
+    FP64 oracle almost none do.  The quirk can only add shadowed rays."""
+    w, sc = small
+    p = W.params(int(w.params.rays), 256, 0.3, seed=3)
+    g0 = sc.trace(w.sun, p, records=True)
+    f0 = g0["flags"].clone()
+    p.quirks = capi.QUIRK_SELF_HIT
+    g1 = sc.trace(w.sun, p, records=True)
+    f1 = g1["flags"]
+    assert torch.all((f0 & 1) <= (f1 & 1))  # shadowed stays shadowed
+    diff = f0 != f1
+    assert diff.float().mean().item() > 0.0
+    # every changed ray ended earlier: newly shadowed, or newly blocked by its own mirror
+    assert torch.all((f1[diff] == 1) | ((f1[diff] == 2) & ((f0[diff] & 1) == 0)))
 
 
 @pytest.mark.parametrize("name", ["mid", "large"])

@@ -1,0 +1,113 @@
+"""The oracle against the REFERENCE's own code.
+
+tests/golden/ref_host_vectors.npz holds outputs of the reference's host-callable
+functions (global_function.cuh, scene_instance_process.cu, heap.cuh,
+heliostat.cpp) compiled from its sources by oracle/ref.mk and driven by
+tests/golden/gen_ref_vectors.py.  FP32 reference values against the FP64
+oracle: float-exact where the oracle replicates float arithmetic (Buie table,
+heaps), within FP32 rounding elsewhere.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from onemirror_b200 import capi
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+V = np.load(os.path.join(HERE, "golden", "ref_host_vectors.npz"))
+D3 = C.c_double * 3
+
+
+def test_local2world_matches_reference():
+    L = O.lib()
+    for d, n, r in zip(V["l2w_d"], V["l2w_n"], V["l2w_out"]):
+        o = D3()
+        # the reference normalises nothing here; the oracle takes the same unit-ish float normal
+        L.orc_local2world(D3(*map(float, d)), D3(*map(float, n)), capi.QUIRK_ZENITH_FRAME, o)
+        assert np.allclose(o[:], r, atol=2e-6 * (1 + np.abs(d).sum())), (d, n)
+
+
+def test_parallelogram_matches_reference_away_from_edges():
+    L = O.lib()
+    agree = 0
+    checked = 0
+    for i in range(len(V["rp_hit"])):
+        o, d = V["rp_o"][i].astype(np.float64), V["rp_d"][i].astype(np.float64)
+        A, B, Cc = (V[k][i].astype(np.float64) for k in ("rp_A", "rp_B", "rp_C"))
+        t, u, v = C.c_double(), C.c_double(), C.c_double()
+        h = L.orc_ray_parallelogram(D3(*o), D3(*d), D3(*A), D3(*B), D3(*Cc), C.byref(t), C.byref(u), C.byref(v))
+        # edge cases (u, v at 0 or 1, t at 0) can flip between FP32 and FP64
+        E1, E2 = B - A, Cc - A
+        M = np.stack([-d, E1, E2], 1)
+        try:
+            tt, uu, vv = np.linalg.solve(M, o - A)
+        except np.linalg.LinAlgError:
+            continue
+        margin = min(abs(uu), abs(1 - uu), abs(vv), abs(1 - vv), abs(tt))
+        if margin < 1e-4:
+            continue
+        checked += 1
+        agree += int(h == V["rp_hit"][i])
+        # FP32 error of the reference's t, u, v grows as the ray grazes the plane
+        cond = abs(np.dot(E1, np.cross(d, E2))) / (np.linalg.norm(E1) * np.linalg.norm(E2))
+        if h and V["rp_hit"][i]:
+            tol = 2e-6 * (1 + np.abs(o - A).max()) / max(cond, 1e-3)
+            assert np.allclose([t.value, u.value, v.value], V["rp_tuv"][i], rtol=tol, atol=tol)
+    assert checked > 1500 and agree == checked
+
+
+def test_angle2xyz_matches_reference():
+    th, ph = V["a2x_in"][:, 0].astype(np.float64), V["a2x_in"][:, 1].astype(np.float64)
+    ref = np.stack([np.sin(th) * np.cos(ph), np.cos(th), np.sin(th) * np.sin(ph)], 1)
+    assert np.allclose(ref, V["a2x_out"], atol=1e-6)
+
+
+@pytest.mark.parametrize("csr", [0.05, 0.1, 0.2, 0.3])
+def test_buie_table_bit_exact_with_reference(csr):
+    x, y, s, p = O.buie_table(csr)
+    key = "buie_%03d" % int(round(csr * 100))
+    assert x.tobytes() == V[key + "_x"].tobytes()
+    assert y.tobytes() == V[key + "_y"].tobytes()
+    assert s.tobytes() == V[key + "_slope"].tobytes()
+    assert p.tobytes() == V[key + "_params"].tobytes()
+
+
+def test_max_less_index_matches_reference():
+    x, y, s, p = O.buie_table(0.1)
+    L = O.lib()
+    for v, i in zip(V["mli_values"], V["mli_index"]):
+        assert L.orc_max_less_index(O._p(y, O.fp), float(v), 1024) == i
+
+
+def test_heap_trimmed_mean_bit_exact_with_reference_heaps():
+    for win, cnt, ratio, ref in zip(V["heap_win"], V["heap_cnt"], V["heap_ratio"], V["heap_out"]):
+        side = next(s for s in (3, 5, 7, 9, 11) if cnt % s == 0 and cnt // s in (s, s - 1, (s + 1) // 2))
+        img = win[:cnt].reshape(cnt // side, side)
+        r = max(img.shape)  # the window of every pixel is the whole image, row-major
+        out = O.smooth_f32(img, r, float(ratio), 1)
+        assert out[0, 0] == ref, (cnt, ratio)
+
+
+def test_heliostat_vertices_match_reference():
+    n = len(V["helio_pos"])
+    rec = capi.Receiver()
+    rec.type = 0
+    rec.pos[:] = [0, 80, 0]
+    rec.size[:] = [1, 1, 0]
+    rec.normal[:] = [0, 0, 1]
+    rec.res_x = rec.res_y = 4
+    for given in (True, False):
+        sun = V["helio_sun"].astype(np.float64)
+        sc = O.Scene(V["helio_pos"], V["helio_size"], 0.0, rec, 10.0, 1.0, list(sun),
+                     aim=None if given else np.tile(V["helio_focus"], (n, 1)),
+                     normal=V["helio_normal_in"] if given else None)
+        ref_v = V["helio_v_given" if given else "helio_v_aimed"].reshape(n, 4, 3)
+        ref_n = V["helio_n_given" if given else "helio_n_aimed"]
+        assert np.allclose(sc.normal, ref_n, atol=3e-7)
+        v = sc.vert.reshape(n, 3, 3)  # v0, v1, v3
+        assert np.allclose(v[:, 0], ref_v[:, 0], atol=5e-5)
+        assert np.allclose(v[:, 1], ref_v[:, 1], atol=5e-5)
+        assert np.allclose(v[:, 2], ref_v[:, 3], atol=5e-5)
