@@ -289,6 +289,30 @@ qmcrt_status qmcrt_scene_sample_points(qmcrt_scene* scene, const qmcrt_trace_par
 qmcrt_status qmcrt_scene_read_points(qmcrt_scene* scene, float* h_point_xz, int32_t* h_point_helio,
                                      void* stream);
 
+/* Poisson-disk sample points without allocating device memory.
+ *
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code running under another allocator's ownership (a host application that
+ * owns every device buffer), a real-time loop that may not allocate, or a
+ * plugin whose memory budget is fixed at load time.  The same points as
+ * qmcrt_scene_sample_points + qmcrt_scene_read_points for the same sizes,
+ * total_points, spacing and seed, written to caller-owned device outputs.
+ *
+ * Inputs: h_size [3n] host mirror sizes; outputs: d_point_xz [2*total_points]
+ * and d_point_helio [total_points], device.  Its working memory is one
+ * file-scope __device__ array that every GPU loading this library holds until
+ * the process exits: room for QMCRT_NOALLOC_MAX_POINTS points and
+ * QMCRT_NOALLOC_MAX_HELIOSTATS heliostats (about 8.2 MB); larger requests are
+ * rejected with QMCRT_ERR_INVALID_ARGUMENT.  The first call on a device looks
+ * up that array's device address; make that first call before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU
+ * (different streams or host threads at the same time) race; serialise them.
+ * Synchronises `stream` to read the sampler's status. */
+#define QMCRT_NOALLOC_MAX_POINTS 1048576
+#define QMCRT_NOALLOC_MAX_HELIOSTATS 16384
+qmcrt_status qmcrt_sample_points_noalloc(const float* h_size, int32_t n, int64_t total_points, float spacing,
+                                         uint64_t seed, float* d_point_xz, int32_t* d_point_helio, void* stream);
+
 /* ------------------------------------------------------------- tracing */
 
 /* One full trace: aim, grid, points (cached), Philox sampling, shadow and

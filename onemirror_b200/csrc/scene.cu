@@ -8,6 +8,7 @@
 // (steps_for_raytracing.cu:67-158).
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 
 #include "internal.hpp"
@@ -745,3 +746,100 @@ qmcrt_status qmcrt_scene_read_points(qmcrt_scene* s, float* h_point_q, int32_t* 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- points without allocation
+// Scratch for qmcrt_sample_points_noalloc: the lattice coordinates of accepted
+// points, a copy of the mirror sizes and the sampler's error flag.  It lives in
+// every context that loads this library, for the life of the process.
+namespace qm {
+
+struct NoAllocScratch {
+  int2 lattice[QMCRT_NOALLOC_MAX_POINTS];
+  float size[3 * QMCRT_NOALLOC_MAX_HELIOSTATS];
+  int32_t flag;
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+constexpr int kMaxDevices = 64;
+static NoAllocScratch* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch on the current device; looked up once per
+// device (host code cannot use the symbol itself as a device address).
+static qmcrt_status noalloc_scratch(NoAllocScratch** out) {
+  int dev = 0;
+  QM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return set_error(QMCRT_ERR_NOT_SUPPORTED, "device index above 63");
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    QM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = (NoAllocScratch*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return QMCRT_OK;
+}
+
+}  // namespace qm
+
+extern "C" qmcrt_status qmcrt_sample_points_noalloc(const float* h_size, int32_t n, int64_t total_points, float spacing,
+                                                    uint64_t seed, float* d_point_xz, int32_t* d_point_helio,
+                                                    void* stream) {
+  if (!h_size || !d_point_xz || !d_point_helio) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (n <= 0 || n > QMCRT_NOALLOC_MAX_HELIOSTATS)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "n must be in [1, QMCRT_NOALLOC_MAX_HELIOSTATS = 16384]");
+  if (total_points < n || total_points > QMCRT_NOALLOC_MAX_POINTS)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT,
+                     "total_points must be in [n, QMCRT_NOALLOC_MAX_POINTS = 1048576] for the allocation-free sampler");
+  if (!(spacing > 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "Poisson points need a minimum spacing");
+  for (int h = 0; h < n; ++h)
+    if (!(h_size[3 * h] > 0) || !(h_size[3 * h + 2] > 0) || h_size[3 * h] > 1000.f || h_size[3 * h + 2] > 1000.f)
+      return set_error(QMCRT_ERR_INVALID_ARGUMENT, "heliostat size must be positive and below 1000 m");
+  NoAllocScratch* scr = nullptr;
+  qmcrt_status e = noalloc_scratch(&scr);
+  if (e) return e;
+  cudaStream_t st = (cudaStream_t)stream;
+  PoissonArgs a{};
+  // addresses inside the device array, computed without dereferencing it on the host
+  char* base = reinterpret_cast<char*>(scr);
+  int2* lattice = reinterpret_cast<int2*>(base + offsetof(NoAllocScratch, lattice));
+  float* dsize = reinterpret_cast<float*>(base + offsetof(NoAllocScratch, size));
+  int32_t* dflag = reinterpret_cast<int32_t*>(base + offsetof(NoAllocScratch, flag));
+  a.n = n;
+  a.size = dsize;
+  a.q = total_points / n;
+  a.rem = total_points % n;
+  a.Rq = (int64_t)((double)spacing * 65536.0);
+  if (a.Rq < 1) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "Poisson spacing below 2^-16 m");
+  a.R2 = a.Rq * a.Rq;
+  int64_t cq = (int64_t)std::sqrt((double)(a.R2 / 2));
+  while (cq * cq > a.R2 / 2) --cq;
+  while ((cq + 1) * (cq + 1) <= a.R2 / 2) ++cq;
+  a.cq = std::max<int64_t>(cq, 1);
+  a.nb = (a.Rq + a.cq - 1) / a.cq;
+  a.key = make_uint2((uint32_t)seed ^ kPoissonKey0, (uint32_t)(seed >> 32) ^ kPoissonKey1);
+  a.max_batches = (64 * (a.q + 1) + 1023) / 32 + 32;
+  a.point_q = lattice;
+  a.point_xz = (float2*)d_point_xz;
+  a.point_helio = d_point_helio;
+  a.flag = dflag;
+  int64_t smem = 0;
+  for (int h = 0; h < n; ++h) {
+    int64_t W = (int64_t)((double)h_size[3 * h] * 65536.0), H = (int64_t)((double)h_size[3 * h + 2] * 65536.0);
+    smem = std::max(smem, ((W + a.cq - 1) / a.cq) * ((H + a.cq - 1) / a.cq) * (int64_t)sizeof(int32_t));
+  }
+  if (smem > 200 * 1024)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT,
+                     "Poisson spacing too small for the heliostat size (background grid over 200 KB)");
+  if (smem > 48 * 1024) QM_CUDA(cudaFuncSetAttribute(poisson_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the flag must start at zero; the lattice is written before it is read
+  QM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int32_t), st));
+  QM_CUDA(cudaMemcpyAsync(dsize, h_size, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+  poisson_kernel<<<n, 32, (size_t)smem, st>>>(a);
+  QM_CUDA(cudaGetLastError());
+  int32_t flag = 0;
+  QM_CUDA(cudaMemcpyAsync(&flag, dflag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  if (flag == 2)
+    return set_error(QMCRT_ERR_SAMPLING, "Poisson-disk spacing too large for the requested points per heliostat");
+  return QMCRT_OK;
+}
