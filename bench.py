@@ -196,6 +196,7 @@ def read_traffic(name):
 def b200_arm(a, rank, world, local):
     import torch
     from onemirror_b200 import capi, workloads as W
+    from onemirror_b200 import dist as D
     from onemirror_b200.scene import SolarScene, image_smooth
 
     torch.cuda.set_device(local)
@@ -234,14 +235,12 @@ def b200_arm(a, rank, world, local):
         r = sc.trace(sun, p, stats=want_stats, outputs=outs)
         sm = image_smooth(r["counts"], w.smooth_radius, w.smooth_ratio, capi.TRIM_SORTED)
         if world > 1:
-            import torch.distributed as dist
-            dist.all_reduce(r["counts"])
-            dist.all_reduce(r["energy"])
+            D.reduce_maps(r["counts"], r["energy"])  # the one exchange: sum of the ranks' maps
         return r, sm
 
     for k in range(a.warmup):
-        one(k, 1000 + k)
-    r, _ = one(a.warmup, 5000, want_stats=True)
+        one(k, D.shard_item(rank, 1000 + k))
+    r, _ = one(a.warmup, D.shard_item(rank, 5000), want_stats=True)
     gst = r["stats"]
     gpu_stats = [gst.rays, gst.shadowed, gst.blocked, gst.hit, gst.offmap, gst.rect_tests, gst.dda_cells]
     torch.cuda.synchronize()
@@ -260,7 +259,7 @@ def b200_arm(a, rank, world, local):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        one(a.warmup + 1 + k, rank * 65536 + 1 + k)
+        one(a.warmup + 1 + k, D.shard_item(rank, k))
         e1.record()
         t = sc.timing()
         kern_ms.append(t.trace_kernel_ms)
@@ -300,7 +299,7 @@ def b200_arm(a, rank, world, local):
                 t0 = time.perf_counter()
             sun = W.make_sun({"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload], base_az - 0.01 * (k + 1),
                              w.sun.dni, w.sun.csr)
-            p.item = 900000 + k
+            p.item = D.shard_item(rank, 9000 + k)
             capi.check(capi.lib().qmcrt_trace_host(sc.h, C.byref(f), C.byref(sun), C.byref(p),
                                                    counts.ctypes.data_as(capi.u32p), capi.as_fp(flux), None, stream))
         dt = time.perf_counter() - t0
