@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling runs; multiple of 256)")
+    ap.add_argument("--variant", type=int, default=0, help="trace kernel variant (qmcrt_trace_params.kernel_variant)")
     return ap.parse_args()
 
 
@@ -208,6 +209,7 @@ def b200_arm(a, rank, world, local):
     w = W.BUILDERS[a.workload](rays=a.rays) if a.rays else W.BUILDERS[a.workload]()
     sc = SolarScene.from_workload(w)
     p = w.params
+    p.kernel_variant = a.variant
     rays = int(p.rays)
     base_az = 180.0
 
@@ -316,11 +318,14 @@ def b200_arm(a, rank, world, local):
         cpu = {"value": ob["rays_per_s"], "unit": UNIT, "cores": ob["cores"], "kind": "port",
                "sample": "%d ray ranges x %d rays spread over the field (%d rays, %.1f s), FP64 oracle"
                          % (ob["ranges"], ob["rays_per_range"], ob["rays"], ob["seconds"])}
-        alg_stats = ob["stats"]
-        nbar_src = "oracle"
+        ref_stats = ob["stats"]
     else:
-        alg_stats = gpu_stats
-        nbar_src = "gpu"
+        ref_stats = None
+    # flops of the work the kernel performs: its own counted rectangle tests and
+    # cell visits (after vertical culling); the oracle's counts are those of
+    # the reference algorithm's traversal, reported beside them
+    alg_stats = gpu_stats
+    nbar_src = "gpu"
     fpr = flops_per_ray(alg_stats)
     kern_s = statistics.mean(kern_ms) * 1e-3
     achieved = rays * fpr / kern_s / 1e12
@@ -331,7 +336,9 @@ def b200_arm(a, rank, world, local):
             "peak_source": "measured live: FFMA chains (qmcrt_fp32_peak_probe), best of 5",
             "flops_per_ray": fpr, "nbar_source": nbar_src,
             "rect_tests_per_ray": alg_stats[5] / alg_stats[0], "dda_cells_per_ray": alg_stats[6] / alg_stats[0],
-            "gpu_rect_tests_per_ray": gpu_stats[5] / gpu_stats[0], "gpu_dda_cells_per_ray": gpu_stats[6] / gpu_stats[0],
+            "reference_rect_tests_per_ray": ref_stats[5] / ref_stats[0] if ref_stats else None,
+            "reference_dda_cells_per_ray": ref_stats[6] / ref_stats[0] if ref_stats else None,
+            "reference_flops_per_ray": flops_per_ray(ref_stats) if ref_stats else None,
             "hbm_peak_gbs_of_measured": peaks.get("hbm_gbs")}
     if traffic is not None:
         roof["hbm_achieved_gbs"] = traffic / kern_s / 1e9

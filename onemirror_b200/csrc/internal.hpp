@@ -33,8 +33,9 @@ struct ReceiverGeom {
 // Buie sunshape table (1025 + 1025 + 1024 floats) and its scalars.
 struct BuieTable {
   float csr = -1.f;
-  std::vector<float> host;  // cdf_x | cdf_y | slope
+  std::vector<float> host;  // cdf_x | cdf_y | slope | guide (int bits)
   float params[6];          // k, gamma, core, total, B, C
+  float inv_bucket = 0;     // guide buckets per unit of CDF
 };
 
 // Build the table exactly as set_samplelights does (float arithmetic).
@@ -92,6 +93,8 @@ struct qmcrt_scene {
   int32_t* d_cell_start = nullptr;  // [cells+1]
   int32_t* d_entries = nullptr;     // [entry_cap]
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
+  float2* d_cell_yr = nullptr;      // [cells] height range of each cell's rectangles
+  int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)
   qm::SunKey sun_key;
 
   // points

@@ -175,10 +175,18 @@ __global__ void fill_kernel(int n, const int4* cellbox, const int32_t* start, in
       }
 }
 
+// float -> int with the same order (for atomicMin/Max on floats)
+__device__ __forceinline__ int ordered(float f) {
+  int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+
 // Sort each cell's list ascending (the reference's push_back order,
-// grid.cpp:36-44) and lay the rectangles out cell-major.
+// grid.cpp:36-44), lay the rectangles out cell-major, and record the height
+// range [ylo, yhi] of the rectangles registered in each cell (for the
+// traversal's vertical culling) and of the whole field.
 __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t* entries,
-                                   const float4* rect, float4* cell_rect) {
+                                   const float4* rect, float4* cell_rect, float2* cell_yr, int* field_yr) {
   int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   int b = start[c], e = start[c + 1];
@@ -190,11 +198,21 @@ __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t*
     }
     entries[j + 1] = v;
   }
+  float ylo = 3.0e38f, yhi = -3.0e38f;
   for (int i = b; i < e; ++i) {
     int h = entries[i];
-    cell_rect[3 * (int64_t)i] = rect[3 * h];
-    cell_rect[3 * (int64_t)i + 1] = rect[3 * h + 1];
-    cell_rect[3 * (int64_t)i + 2] = rect[3 * h + 2];
+    float4 r0 = rect[3 * h], r1 = rect[3 * h + 1], r2 = rect[3 * h + 2];
+    cell_rect[3 * (int64_t)i] = r0;
+    cell_rect[3 * (int64_t)i + 1] = r1;
+    cell_rect[3 * (int64_t)i + 2] = r2;
+    float y0 = r0.y, y1 = r0.y + r1.y, y2 = r0.y + r2.y, y3 = r0.y + r1.y + r2.y;
+    ylo = fminf(ylo, fminf(fminf(y0, y1), fminf(y2, y3)));
+    yhi = fmaxf(yhi, fmaxf(fmaxf(y0, y1), fmaxf(y2, y3)));
+  }
+  cell_yr[c] = make_float2(ylo, yhi);
+  if (e > b) {
+    atomicMin(field_yr, ordered(ylo));
+    atomicMax(field_yr + 1, ordered(yhi));
   }
 }
 
@@ -401,8 +419,13 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
   fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, s->d_cellbox, s->d_cell_start, s->d_cell_count,
                                                   s->d_entries, s->gdims[1], s->gdims[2], s->entry_cap);
   QM_CUDA(cudaGetLastError());
+  {
+    static const int init_yr[2] = {0x7F7FFFFF, (int)(0xFF7FFFFFu ^ 0x7FFFFFFFu)};  // ordered(+FLT_MAX), ordered(-FLT_MAX)
+    QM_CUDA(cudaMemcpyAsync(s->d_field_yr, init_yr, sizeof(init_yr), cudaMemcpyHostToDevice, st));
+  }
   cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, s->d_cell_start, s->d_entries,
-                                                                        s->d_rect, s->d_cell_rect);
+                                                                        s->d_rect, s->d_cell_rect, s->d_cell_yr,
+                                                                        s->d_field_yr);
   QM_CUDA(cudaGetLastError());
   QM_CUDA(cudaEventRecord(s->ev[1], st));
   s->setup_timed = true;
@@ -605,12 +628,14 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_cell_start, (size_t)s->cells + 1);
   ALLOC(s->d_entries, (size_t)cap);
   ALLOC(s->d_cell_rect, 3 * (size_t)cap);
+  ALLOC(s->d_cell_yr, (size_t)s->cells);
+  ALLOC(s->d_field_yr, 2);
   ALLOC(s->d_helio_weight, n);
   ALLOC(s->d_flag, 1);
   ALLOC(s->d_counts, res);
   ALLOC(s->d_energy, res);
   ALLOC(s->d_stats, 16);
-  ALLOC(s->d_buie, 1025 + 1025 + 1024);
+  ALLOC(s->d_buie, 1025 + 1025 + 1024 + 1024);  // table + guide
 #undef ALLOC
   for (int i = 0; i < 5; ++i) {
     cudaError_t ce = cudaEventCreate(&s->ev[i]);
@@ -636,7 +661,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_pos); dev_free(s->d_size); dev_free(s->d_aim); dev_free(s->d_normal_in);
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
-  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_yr); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

@@ -66,34 +66,58 @@ static int sm_count() {
   return g_sm_count;
 }
 
-template <bool TABLES, bool RECORDS, bool STATS>
+template <bool TABLES, bool RECORDS, bool STATS, bool CULL, int MINB = 1>
 static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
+  auto k = trace_kernel<TABLES, RECORDS, STATS, CULL, MINB>;
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<TABLES, RECORDS, STATS>,
-                                                                kTraceThreads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTraceThreads, 0);
   if (e != cudaSuccess) return e;
   int64_t blocks = (int64_t)std::max(per_sm, 1) * sm_count();
   int64_t need = ((int64_t)a.rays + kTraceThreads - 1) / kTraceThreads;
   blocks = std::max<int64_t>(1, std::min(blocks, need));
-  trace_kernel<TABLES, RECORDS, STATS><<<(unsigned)blocks, kTraceThreads, 0, st>>>(a);
+  k<<<(unsigned)blocks, kTraceThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 
-static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool stats, cudaStream_t st) {
-  if (tables) {
-    if (records) return stats ? launch_trace<true, true, true>(a, st) : launch_trace<true, true, false>(a, st);
-    return stats ? launch_trace<true, false, true>(a, st) : launch_trace<true, false, false>(a, st);
-  }
-  if (records) return stats ? launch_trace<false, true, true>(a, st) : launch_trace<false, true, false>(a, st);
-  return stats ? launch_trace<false, false, true>(a, st) : launch_trace<false, false, false>(a, st);
+template <bool TABLES, bool RECORDS>
+static cudaError_t dispatch2(const TraceArgs& a, bool stats, bool cull, cudaStream_t st) {
+  if (stats) return cull ? launch_trace<TABLES, RECORDS, true, true>(a, st) : launch_trace<TABLES, RECORDS, true, false>(a, st);
+  return cull ? launch_trace<TABLES, RECORDS, false, true>(a, st) : launch_trace<TABLES, RECORDS, false, false>(a, st);
+}
+
+static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool stats, bool cull, int variant,
+                            cudaStream_t st) {
+  // the production path (no records, no statistics) is compiled for 4 resident
+  // CTAs per SM (64 registers); variant 3 keeps the unconstrained build
+  if (variant != 3 && !tables && !records && !stats && cull) return launch_trace<false, false, false, true, 4>(a, st);
+  if (tables) return records ? dispatch2<true, true>(a, stats, cull, st) : dispatch2<true, false>(a, stats, cull, st);
+  return records ? dispatch2<false, true>(a, stats, cull, st) : dispatch2<false, false>(a, stats, cull, st);
 }
 
 static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
   if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   if (s->buie.csr == csr) return QMCRT_OK;
-  s->buie.host.resize(1025 + 1025 + 1024);
+  s->buie.host.resize(1025 + 1025 + 1024 + kBuieBuckets);
   float* h = s->buie.host.data();
   buie_build(csr, h, h + 1025, h + 2050, s->buie.params);
+  // guide table: for each uniform bucket of [0, core), a lower bound of the
+  // interval index of every value the kernel maps to that bucket (one below
+  // the index at the bucket's lower edge, which absorbs float rounding of the
+  // bucket computation; CDF intervals are far wider than that rounding)
+  const float* cy = h + 1025;
+  float inv_bucket = (float)kBuieBuckets / s->buie.params[2];
+  for (int b = 0; b < kBuieBuckets; ++b) {
+    float edge = (float)b / inv_bucket;
+    int lo = 0, hi = 1024;
+    while (lo < hi) {  // largest i with cy[i] <= edge
+      int mid = (lo + hi + 1) >> 1;
+      if (cy[mid] <= edge) lo = mid;
+      else hi = mid - 1;
+    }
+    int g = std::max(lo - 1, 0);
+    std::memcpy(h + 3074 + b, &g, sizeof(int));
+  }
+  s->buie.inv_bucket = inv_bucket;
   QM_CUDA(cudaMemcpyAsync(s->d_buie, h, s->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   s->buie.csr = csr;
   return QMCRT_OK;
@@ -131,6 +155,7 @@ static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, T
   a->b_B = s->buie.params[4];
   a->b_C = s->buie.params[5];
   a->b_inv = 1 / (s->buie.params[1] + 1);  // scene_instance_process.cu:135
+  a->b_inv_bucket = s->buie.inv_bucket;
   a->n_helio = s->n;
   a->frame = s->d_frame;
   a->pos = s->d_pos;
@@ -139,6 +164,8 @@ static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, T
   a->weight = s->d_helio_weight;
   a->crect = s->d_cell_rect;
   a->cstart = s->d_cell_start;
+  a->cell_yr = s->d_cell_yr;
+  a->field_yr = s->d_field_yr;
   for (int i = 0; i < 3; ++i) {
     a->gpos[i] = s->gpos[i];
     a->gcell[i] = s->gcell[i];
@@ -183,7 +210,10 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
     a.pixel = out->d_ray_pixel;
   }
   QM_CUDA(cudaEventRecord(s->ev[2], st));
-  QM_CUDA(dispatch(a, tables, records, stats != nullptr, st));
+  // vertical culling needs every rectangle registered in every cell it
+  // touches and the origin cell tested: off under the two grid quirks
+  bool cull = p->kernel_variant != 2 && !(p->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS));
+  QM_CUDA(dispatch(a, tables, records, stats != nullptr, cull, p->kernel_variant, st));
   QM_CUDA(cudaEventRecord(s->ev[3], st));
   double scale = (double)sun->dni * p->reflectivity * weight_scale / ((double)p->rays_per_point * s->rg.pixel_area);
   FinalizeArgs f{};

@@ -9,13 +9,14 @@
 namespace qm {
 
 constexpr int kTraceThreads = 256;
+constexpr int kBuieBuckets = 1024;  // guide-table buckets over the core CDF
 
 struct TraceArgs {
   // sun: frame of local2world for the sun direction, and the direction
   double su[3], sn[3], sv[3], sdir[3];
-  // Buie table in global memory (cdf_x | cdf_y | slope) and its scalars
+  // Buie table in global memory (cdf_x | cdf_y | slope | guide as int) and its scalars
   const float* buie;
-  float b_total, b_core, b_B, b_C, b_inv;
+  float b_total, b_core, b_B, b_C, b_inv, b_inv_bucket;
   // field
   const double* frame;  // [9n]
   const float* pos;
@@ -25,6 +26,8 @@ struct TraceArgs {
   // grid
   const float4* crect;
   const int32_t* cstart;
+  const float2* cell_yr;  // [cells] height range of each cell's rectangles
+  const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3];
   int gdims[3];
   // receiver
@@ -69,13 +72,32 @@ __device__ __forceinline__ int max_less_index(const float* cdf_y, float value) {
 }
 
 // Inverse CDF of the Buie sunshape (linear_interpolate, :115-137).  mrad.
-__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float* s_tab, float u) {
+// The interval index equals max_less_index's (the largest i with
+// cdf_y[i] <= uu): a guide table over uniform buckets of [0, core) gives a
+// lower bound, then a short forward scan finishes.
+__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float* s_tab, const int* s_guide, float u) {
   float uu = u * a.b_total;
   if (uu < a.b_core) {
-    int id = max_less_index(s_tab + 1025, uu);
-    return (uu - s_tab[1025 + id]) * s_tab[2050 + id] + s_tab[id];
+    const float* cy = s_tab + 1025;
+    int b = min((int)(uu * a.b_inv_bucket), kBuieBuckets - 1);
+    int id = s_guide[b];
+    while (id < 1023 && cy[id + 1] <= uu) ++id;
+    return (uu - cy[id]) * s_tab[2050 + id] + s_tab[id];
   }
   return powf((uu - a.b_core) * a.b_B + a.b_C, a.b_inv);
+}
+
+// sin and cos of a small angle by their Taylor series (exact to float
+// rounding for |x| < 0.05: the first omitted terms are below 2e-11 relative);
+// sincosf otherwise.
+__device__ __forceinline__ void sincos_small(float x, float* s, float* c) {
+  if (fabsf(x) < 0.05f) {
+    float x2 = x * x;
+    *s = x * (1.f - x2 * (1.f / 6.f) * (1.f - x2 * (1.f / 20.f)));
+    *c = 1.f - x2 * 0.5f * (1.f - x2 * (1.f / 12.f));
+  } else {
+    sincosf(x, s, c);
+  }
 }
 
 // One grid cell: any rectangle other than `own` hit at t > eps?  The
@@ -114,10 +136,19 @@ __device__ __forceinline__ float abs_div(float t, float d) {
   return (d <= kEps && d >= -kEps) ? 2147483648.0f : fabsf(t / d);
 }
 
+__device__ __forceinline__ float from_ordered(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF); }
+
 // 3D-DDA any-hit (NotCollision, rectgrid_raytracing.cu:38-117).  The origin
 // cell is tested first unless QMCRT_QUIRK_SKIP_ORIGIN_CELL.
-template <bool STATS>
-__device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, uint32_t& ntest, uint32_t& ncell) {
+// CULL (corrected mode only): a cell whose rectangles all lie above or below
+// the ray's height over the cell's [t_in, t_out] is not tested, and the walk
+// ends once the ray has left the field's height range.  With every rectangle
+// registered in every cell it touches, a real hit is always found in the cell
+// holding the hit point, whose height range contains that point, so the
+// answer is unchanged.
+template <bool STATS, bool CULL>
+__device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, float fy0, float fy1, uint32_t& ntest,
+                            uint32_t& ncell) {
   const bool selfhit = a.quirks & QMCRT_QUIRK_SELF_HIT;
   const int gx = a.gdims[0], gy = a.gdims[1], gz = a.gdims[2];
   float rx = o.x - a.gpos[0], ry = o.y - a.gpos[1], rz = o.z - a.gpos[2];
@@ -130,34 +161,57 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, uin
   float ty = abs_div(d.y >= 0.f ? (float)(iy + 1) * a.gcell[1] - ry : ry - (float)iy * a.gcell[1], d.y);
   float tz = abs_div(d.z >= 0.f ? (float)(iz + 1) * a.gcell[2] - rz : rz - (float)iz * a.gcell[2], d.z);
   float dx = abs_div(a.gcell[0], d.x), dy = abs_div(a.gcell[1], d.y), dz = abs_div(a.gcell[2], d.z);
+  // true if the cell may hold a hit: the ray's height over [t0, t1], widened
+  // by a margin far above FP32 error, meets the cell's rectangle heights
+  auto may_hit = [&](int c, float t0, float t1) -> bool {
+    if (!CULL) return true;
+    float2 yr = __ldg(a.cell_yr + c);
+    float ya = o.y + t0 * d.y, yb = o.y + t1 * d.y;
+    float mg = 0.01f + 1e-5f * t1;
+    return !(fmaxf(ya, yb) + mg < yr.x || fminf(ya, yb) - mg > yr.y);
+  };
   if (!(a.quirks & QMCRT_QUIRK_SKIP_ORIGIN_CELL)) {
-    if (STATS) ++ncell;
-    if (cell_hit<STATS>(a, (ix * gy + iy) * gz + iz, o, d, own, selfhit, ntest)) return true;
+    int c = (ix * gy + iy) * gz + iz;
+    if (may_hit(c, 0.f, fminf(tx, fminf(ty, tz)))) {
+      if (STATS) ++ncell;
+      if (cell_hit<STATS>(a, c, o, d, own, selfhit, ntest)) return true;
+    }
   }
   for (int guard = gx + gy + gz + 2; guard > 0; --guard) {
+    float tin;
     if (tx < ty) {
       if (tx < tz) {
         ix += sx;
         if (ix >= gx || ix < 0) return false;
+        tin = tx;
         tx += dx;
       } else {
         iz += sz;
         if (iz >= gz || iz < 0) return false;
+        tin = tz;
         tz += dz;
       }
     } else {
       if (ty < tz) {
         iy += sy;
         if (iy >= gy || iy < 0) return false;
+        tin = ty;
         ty += dy;
       } else {
         iz += sz;
         if (iz >= gz || iz < 0) return false;
+        tin = tz;
         tz += dz;
       }
     }
+    if (CULL) {
+      float y = o.y + tin * d.y, mg = 0.01f + 1e-5f * tin;
+      if ((d.y > 0.f && y - mg > fy1) || (d.y < 0.f && y + mg < fy0)) return false;  // left the mirror layer
+    }
+    int c = (ix * gy + iy) * gz + iz;
+    if (!may_hit(c, tin, fminf(tx, fminf(ty, tz)))) continue;
     if (STATS) ++ncell;
-    if (cell_hit<STATS>(a, (ix * gy + iy) * gz + iz, o, d, own, selfhit, ntest)) return true;
+    if (cell_hit<STATS>(a, c, o, d, own, selfhit, ntest)) return true;
   }
   return false;
 }
@@ -218,11 +272,14 @@ __device__ __forceinline__ d3 rnorm(d3 a) {
   return r * a;
 }
 
-template <bool TABLES, bool RECORDS, bool STATS>
-__global__ void __launch_bounds__(kTraceThreads) trace_kernel(const TraceArgs a) {
+template <bool TABLES, bool RECORDS, bool STATS, bool CULL, int MINB = 1>
+__global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
   __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ int s_guide[kBuieBuckets];
+  const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   if (!TABLES) {
     for (int i = threadIdx.x; i < 3074; i += blockDim.x) s_tab[i] = __ldg(a.buie + i);
+    for (int i = threadIdx.x; i < kBuieBuckets; i += blockDim.x) s_guide[i] = __float_as_int(__ldg(a.buie + 3074 + i));
     __syncthreads();
   }
   uint32_t n_sh = 0, n_bl = 0, n_hit = 0, n_off = 0, n_ray = 0, n_test = 0, n_cell = 0;
@@ -258,15 +315,15 @@ __global__ void __launch_bounds__(kTraceThreads) trace_kernel(const TraceArgs a)
       tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
     } else {
       uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
-      float th = buie_theta_mrad(a, s_tab, u24f(r.x)) * 1e-3f;
+      float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
       float st, ct, sp, cp;
-      sincosf(th, &st, &ct);
+      sincos_small(th, &st, &ct);  // th <= 9.3 mrad
       sincospif(2.f * u24f(r.y), &sp, &cp);
       sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
       float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
       float ths = __ldg(a.sigma + h) * z;
       uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
-      sincosf(ths, &st, &ct);
+      sincos_small(ths, &st, &ct);
       sincospif(2.f * u24f(extra), &sp, &cp);
       tl = f3(st * cp, ct, st * sp);
       w = a.weight ? __ldg(a.weight + h) : 1.f;
@@ -277,13 +334,13 @@ __global__ void __launch_bounds__(kTraceThreads) trace_kernel(const TraceArgs a)
     const float3 of = to_f(o);
     uint8_t flag = 0;
     int pix = -1;
-    if (dda_blocked<STATS>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, n_test, n_cell)) {
+    if (dda_blocked<STATS, CULL>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, n_test, n_cell)) {
       flag = QMCRT_RAY_SHADOWED;
     } else {
       d3 np = rnorm(apply(fr, (double)tl.x, (double)tl.y, (double)tl.z));
       double di = dot(ws, np);
       d3 rd = rnorm(ws - (2.0 * di) * np);  // reflect (i - 2 n (n.i)), normalise
-      if (dda_blocked<STATS>(a, of, to_f(rd), h, n_test, n_cell)) {
+      if (dda_blocked<STATS, CULL>(a, of, to_f(rd), h, fy0, fy1, n_test, n_cell)) {
         flag = QMCRT_RAY_BLOCKED;
       } else if (receiver_hit(a, o, rd, pix)) {
         flag = QMCRT_RAY_HIT;
