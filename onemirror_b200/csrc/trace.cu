@@ -169,6 +169,7 @@ static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, T
   for (int i = 0; i < 3; ++i) {
     a->gpos[i] = s->gpos[i];
     a->gcell[i] = s->gcell[i];
+    a->ginv[i] = 1.0f / s->gcell[i];
     a->gdims[i] = s->gdims[i];
   }
   a->rtype = s->rg.type;
@@ -184,6 +185,14 @@ static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, T
   a->counts = s->d_counts;
   a->energy = s->d_energy;
   a->stats = s->d_stats;
+}
+
+// log2(v) when v is a power of two, else -1 (lets the kernel split ray ids with a shift)
+static int pow2_shift(int v) {
+  if (v <= 0 || (v & (v - 1))) return -1;
+  int s = 0;
+  while ((1 << s) < v) ++s;
+  return s;
 }
 
 static qmcrt_status check_params(const qmcrt_trace_params* p) {
@@ -274,6 +283,7 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   fill_common(s, sun, p->quirks, &a);
   a.rays = (uint32_t)(s->points * (int64_t)p->rays_per_point);
   a.rpp = p->rays_per_point;
+  a.rpp_shift = pow2_shift(a.rpp);
   a.key = make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32));
   a.item = p->item;
   a.point_xz = s->d_point_xz;
@@ -299,6 +309,7 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcr
   fill_common(s, sun, p->quirks, &a);
   a.rays = (uint32_t)(t->points * t->rays_per_point);
   a.rpp = t->rays_per_point;
+  a.rpp_shift = pow2_shift(a.rpp);
   a.point_xz = (const float2*)t->d_point_xz;
   a.point_helio = t->d_point_helio;
   a.sun_local = t->d_sun_local;

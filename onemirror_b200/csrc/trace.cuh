@@ -28,7 +28,7 @@ struct TraceArgs {
   const int32_t* cstart;
   const float2* cell_yr;  // [cells] height range of each cell's rectangles
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
-  float gpos[3], gcell[3];
+  float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
   int gdims[3];
   // receiver
   int rtype;
@@ -39,6 +39,7 @@ struct TraceArgs {
   int n_helio;
   uint32_t rays;
   int rpp;
+  int rpp_shift;  // log2(rpp) when rpp is a power of two, else -1
   uint2 key;
   uint32_t item;
   uint32_t quirks;
@@ -152,15 +153,20 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
   const bool selfhit = a.quirks & QMCRT_QUIRK_SELF_HIT;
   const int gx = a.gdims[0], gy = a.gdims[1], gz = a.gdims[2];
   float rx = o.x - a.gpos[0], ry = o.y - a.gpos[1], rz = o.z - a.gpos[2];
-  int ix = min(max((int)floorf(rx / a.gcell[0]), 0), gx - 1);
-  int iy = min(max((int)floorf(ry / a.gcell[1]), 0), gy - 1);
-  int iz = min(max((int)floorf(rz / a.gcell[2]), 0), gz - 1);
+  int ix = min(max((int)floorf(rx * a.ginv[0]), 0), gx - 1);
+  int iy = min(max((int)floorf(ry * a.ginv[1]), 0), gy - 1);
+  int iz = min(max((int)floorf(rz * a.ginv[2]), 0), gz - 1);
   int sx = d.x >= 0.f ? 1 : -1, sy = d.y >= 0.f ? 1 : -1, sz = d.z >= 0.f ? 1 : -1;
-  // calTMax (rectgrid_raytracing.cu:3-9)
-  float tx = abs_div(d.x >= 0.f ? (float)(ix + 1) * a.gcell[0] - rx : rx - (float)ix * a.gcell[0], d.x);
-  float ty = abs_div(d.y >= 0.f ? (float)(iy + 1) * a.gcell[1] - ry : ry - (float)iy * a.gcell[1], d.y);
-  float tz = abs_div(d.z >= 0.f ? (float)(iz + 1) * a.gcell[2] - rz : rz - (float)iz * a.gcell[2], d.z);
-  float dx = abs_div(a.gcell[0], d.x), dy = abs_div(a.gcell[1], d.y), dz = abs_div(a.gcell[2], d.z);
+  // calTMax and absDivide (rectgrid_raytracing.cu:3-17) with one reciprocal
+  // per axis in place of the divisions
+  const float big = 2147483648.0f;
+  const bool px = fabsf(d.x) > kEps, py = fabsf(d.y) > kEps, pz = fabsf(d.z) > kEps;
+  const float qx = px ? fabsf(__frcp_rn(d.x)) : 0.f, qy = py ? fabsf(__frcp_rn(d.y)) : 0.f,
+              qz = pz ? fabsf(__frcp_rn(d.z)) : 0.f;
+  float tx = px ? fabsf(d.x >= 0.f ? (float)(ix + 1) * a.gcell[0] - rx : rx - (float)ix * a.gcell[0]) * qx : big;
+  float ty = py ? fabsf(d.y >= 0.f ? (float)(iy + 1) * a.gcell[1] - ry : ry - (float)iy * a.gcell[1]) * qy : big;
+  float tz = pz ? fabsf(d.z >= 0.f ? (float)(iz + 1) * a.gcell[2] - rz : rz - (float)iz * a.gcell[2]) * qz : big;
+  float dx = px ? a.gcell[0] * qx : big, dy = py ? a.gcell[1] * qy : big, dz = pz ? a.gcell[2] * qz : big;
   // true if the cell may hold a hit: the ray's height over [t0, t1], widened
   // by a margin far above FP32 error, meets the cell's rectangle heights
   auto may_hit = [&](int c, float t0, float t1) -> bool {
@@ -286,7 +292,8 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride) {
     const uint32_t ray = (uint32_t)r64;
-    const uint32_t g = ray / (uint32_t)a.rpp, j = ray - g * (uint32_t)a.rpp;
+    const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
+    const uint32_t j = ray - g * (uint32_t)a.rpp;
     const int h = __ldg(a.point_helio + g);
     if (TABLES && (h < 0 || h >= a.n_helio)) {  // caller-provided ids: skip, never index out of range
       if (RECORDS) {
