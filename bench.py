@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling runs; multiple of 256)")
     ap.add_argument("--variant", type=int, default=0, help="trace kernel variant (qmcrt_trace_params.kernel_variant)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-versus-sequential section")
     return ap.parse_args()
 
 
@@ -167,6 +168,62 @@ def reference_arm(a, rank, world):
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def batch_section(reps=3):
+    """The batched form against sequential plain launches on the equinox day:
+    3 fields (300, 1000, 4000 heliostats) x 45 sun positions x 2^24 rays.
+    Batched: one captured CUDA graph (aiming, grids, one persistent trace
+    kernel, flux scaling) per pass.  Sequential: one qmcrt_trace per item
+    (its own aiming, grid, trace and scaling launches) plus a copy of the
+    item's flux map out of the scene.  Both timed with CUDA events."""
+    import torch
+    from onemirror_b200.scene import Batch, SolarScene
+    from onemirror_b200 import workloads as W
+    fields, suns, items, params = W.batched()
+    scenes = [SolarScene.from_workload(f) for f in fields]
+    b = Batch(scenes, items, params)
+    tuning = b.autotune()
+    b.capture()
+    b.launch()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        b.launch()
+    e1.record()
+    e1.synchronize()
+    batched_ms = e0.elapsed_time(e1) / reps
+    rays = len(items) * int(params.rays)
+    outs = [torch.empty((256, 256), dtype=torch.float32, device="cuda") for _ in items]
+    ps = []
+    for i in range(len(items)):
+        p = W.params(int(params.rays), params.rays_per_point, params.point_spacing, seed=params.seed)
+        p.item = i
+        ps.append(p)
+
+    def sequential():
+        for i, (si, sun) in enumerate(items):
+            r = scenes[si].trace(sun, ps[i], stats=False, outputs=seq_out[si])
+            outs[i].copy_(r["flux"])
+
+    seq_out = [scenes[k]._outputs(0, False) for k in range(len(scenes))]
+    sequential()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        sequential()
+    e1.record()
+    e1.synchronize()
+    seq_ms = e0.elapsed_time(e1) / reps
+    b.close()
+    for s in scenes:
+        s.close()
+    return {"items": len(items), "sun_positions": len(suns), "fields": [f.n for f in fields],
+            "rays_per_item": int(params.rays), "batched_ms": batched_ms, "sequential_ms": seq_ms,
+            "batched_rays_per_s": rays / (batched_ms * 1e-3), "sequential_rays_per_s": rays / (seq_ms * 1e-3),
+            "speedup_vs_sequential": seq_ms / batched_ms,
+            "tuning": {"chunk_rays": tuning.chunk_rays, "ctas_per_sm": tuning.ctas_per_sm, "tile": tuning.tile}}
 
 
 def workload_name(w):
@@ -312,6 +369,9 @@ def b200_arm(a, rank, world, local):
         e2e = {"value": rays * world * a.e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "call": "qmcrt_trace_host"}
 
+    batch = None
+    if rank == 0 and world == 1 and not a.no_batch and a.workload == "mid" and not a.rays:
+        batch = batch_section()
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         ob = oracle_sample(w, a.cpu_seconds)
@@ -355,6 +415,7 @@ def b200_arm(a, rank, world, local):
                                   "finalize": 1, "smooth": 1},
             "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
             "clocks": clocks,
+            "batched": batch,
             "stats": {"shadowed": gst.shadowed / gst.rays, "blocked": gst.blocked / gst.rays,
                       "hit": gst.hit / gst.rays, "intercept_ratio": gst.intercept_ratio}}
     if rank == 0:

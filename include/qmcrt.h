@@ -232,6 +232,15 @@ const char* qmcrt_last_error(void);
  * clockwise), the convention of main.cpp:71-73. */
 qmcrt_status qmcrt_sun_direction(float elevation_deg, float azimuth_deg, float dir_out[3]);
 
+/* Sun position for a site: solar declination (degrees) of day `day_of_year`
+ * by Cooper's formula, and elevation / azimuth (degrees, azimuth from north
+ * clockwise) for latitude, declination and hour angle (15 degrees per hour from
+ * solar noon, negative in the morning).  Stands in for the NREL SPA call of the
+ * reference driver (main.cpp:62-73). */
+float qmcrt_solar_declination(int32_t day_of_year);
+qmcrt_status qmcrt_solar_position(float latitude_deg, float declination_deg, float hour_angle_deg,
+                                  float* elevation_deg, float* azimuth_deg);
+
 /* Buie sunshape inverse-CDF table, built exactly as
  * SceneProcessor::set_samplelights (scene_instance_process.cu:163-200) builds
  * it: 1024 trapezoids on [0, 4.65] mrad plus the analytic aureole to 9.3 mrad.
@@ -334,6 +343,45 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* scene, const qmcrt_sun* sun,
  * maps.  h_counts / h_flux may be NULL.  Synchronises. */
 qmcrt_status qmcrt_trace_host(qmcrt_scene* scene, const qmcrt_field* field, const qmcrt_sun* sun,
                               const qmcrt_trace_params* params, uint32_t* h_counts, float* h_flux,
+                              qmcrt_trace_stats* stats, void* stream);
+
+/* ------------------------------------------------------------ batching
+ * No counterpart in the reference (it launches and synchronises once per
+ * heliostat per sun position, ray_tracing.cu:23-27).  Many (field, sun)
+ * items traced by ONE persistent kernel that takes ray chunks from a global
+ * work counter, the whole pass (aiming, grids, tracing, flux scaling)
+ * replayable as one captured CUDA graph.  Item i traces the same rays as
+ * qmcrt_trace with params.item = i, so its count map equals that trace's. */
+typedef struct qmcrt_batch_item {
+  int32_t scene;   /* index into the scenes array */
+  qmcrt_sun sun;
+} qmcrt_batch_item;
+
+typedef struct qmcrt_batch_tuning {
+  int32_t chunk_rays;   /* rays per work unit (multiple of 256) */
+  int32_t ctas_per_sm;  /* resident CTAs per SM of the persistent grid (1..4) */
+  int32_t tile;         /* 0, 32 or 48: side of the CTA-private shared-memory flux tile */
+  float ms;             /* autotune: device time of the trace pass with this tuning */
+} qmcrt_batch_tuning;
+
+/* Items must use corrected-mode traversal (no SKIP_ORIGIN_CELL / AABB_RADIUS
+ * quirks) and nearest deposition; every item traces params->rays rays. */
+qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, const qmcrt_batch_item* items,
+                                int32_t n_items, const qmcrt_trace_params* params, qmcrt_batch** out);
+qmcrt_status qmcrt_batch_destroy(qmcrt_batch* batch);
+/* Time candidate tunings on the first items and keep the fastest. Syncs. */
+qmcrt_status qmcrt_batch_autotune(qmcrt_batch* batch, qmcrt_batch_tuning* chosen, void* stream);
+qmcrt_status qmcrt_batch_set_tuning(qmcrt_batch* batch, const qmcrt_batch_tuning* tuning);
+/* Enqueue the whole pass on `stream` (no graph). */
+qmcrt_status qmcrt_batch_run(qmcrt_batch* batch, void* stream);
+/* Capture the pass into a CUDA graph (replaces any earlier graph). */
+qmcrt_status qmcrt_batch_capture(qmcrt_batch* batch);
+/* Replay the captured graph on `stream`. */
+qmcrt_status qmcrt_batch_launch(qmcrt_batch* batch, void* stream);
+/* Device pointers of an item's maps (valid until destroy). */
+qmcrt_status qmcrt_batch_maps(qmcrt_batch* batch, int32_t item, uint32_t** d_counts, float** d_flux);
+/* Copy an item's maps to host and fill its totals.  Syncs. */
+qmcrt_status qmcrt_batch_read(qmcrt_batch* batch, int32_t item, uint32_t* h_counts, float* h_flux,
                               qmcrt_trace_stats* stats, void* stream);
 
 /* ----------------------------------------------------------- smoothing

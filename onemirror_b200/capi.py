@@ -81,6 +81,14 @@ class GridInfo(C.Structure):
                 ("cells", C.c_int64), ("entries", C.c_int64), ("fine_div", C.c_int32)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("sun", Sun)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("chunk_rays", C.c_int32), ("ctas_per_sm", C.c_int32), ("tile", C.c_int32), ("ms", C.c_float)]
+
+
 class Timing(C.Structure):
     _fields_ = [("setup_ms", C.c_float), ("trace_kernel_ms", C.c_float), ("finalize_ms", C.c_float)]
 
@@ -98,6 +106,18 @@ PROTOTYPES = {
     "qmcrt_status_string": (C.c_char_p, [C.c_int]),
     "qmcrt_last_error": (C.c_char_p, []),
     "qmcrt_sun_direction": (C.c_int, [C.c_float, C.c_float, fp]),
+    "qmcrt_solar_declination": (C.c_float, [C.c_int32]),
+    "qmcrt_solar_position": (C.c_int, [C.c_float, C.c_float, C.c_float, fp, fp]),
+    "qmcrt_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(BatchItem), C.c_int32,
+                                     C.POINTER(TraceParams), C.POINTER(C.c_void_p)]),
+    "qmcrt_batch_destroy": (C.c_int, [C.c_void_p]),
+    "qmcrt_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning), C.c_void_p]),
+    "qmcrt_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+    "qmcrt_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qmcrt_batch_capture": (C.c_int, [C.c_void_p]),
+    "qmcrt_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qmcrt_batch_maps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "qmcrt_batch_read": (C.c_int, [C.c_void_p, C.c_int32, u32p, fp, C.POINTER(TraceStats), C.c_void_p]),
     "qmcrt_buie_table": (C.c_int, [C.c_float, fp, fp, fp, fp]),
     "qmcrt_layout_radial_staggered": (C.c_int, [C.POINTER(LayoutParams), fp, C.c_int32, i32p]),
     "qmcrt_scn_parse": (C.c_int, [C.c_char_p, C.POINTER(Receiver), C.POINTER(GridParams), fp, fp, C.c_int32, i32p]),

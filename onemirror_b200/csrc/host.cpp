@@ -212,6 +212,32 @@ qmcrt_status qmcrt_sun_direction(float elevation_deg, float azimuth_deg, float d
   return QMCRT_OK;
 }
 
+float qmcrt_solar_declination(int32_t day_of_year) {
+  // Cooper (1969): 23.45 deg * sin(360 deg * (284 + n) / 365)
+  return (float)(23.45 * std::sin(2.0 * M_PI * (284.0 + day_of_year) / 365.0));
+}
+
+qmcrt_status qmcrt_solar_position(float latitude_deg, float declination_deg, float hour_angle_deg,
+                                  float* elevation_deg, float* azimuth_deg) {
+  if (!elevation_deg || !azimuth_deg) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL output");
+  if (!(std::fabs(latitude_deg) <= 90.f) || !(std::fabs(declination_deg) <= 23.5f))
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "latitude or declination out of range");
+  const double d2r = M_PI / 180.0;
+  double phi = latitude_deg * d2r, dec = declination_deg * d2r, h = hour_angle_deg * d2r;
+  // spherical astronomy: sin(el) = sin(phi) sin(dec) + cos(phi) cos(dec) cos(h)
+  double se = std::sin(phi) * std::sin(dec) + std::cos(phi) * std::cos(dec) * std::cos(h);
+  se = std::max(-1.0, std::min(1.0, se));
+  double el = std::asin(se);
+  // azimuth from north, clockwise: east in the morning (h < 0), west after noon
+  double ca = (std::sin(dec) - se * std::sin(phi)) / std::max(1e-12, std::cos(el) * std::cos(phi));
+  ca = std::max(-1.0, std::min(1.0, ca));
+  double az = std::acos(ca);
+  if (h > 0) az = 2.0 * M_PI - az;
+  *elevation_deg = (float)(el / d2r);
+  *azimuth_deg = (float)(az / d2r);
+  return QMCRT_OK;
+}
+
 qmcrt_status qmcrt_buie_table(float csr, float* cdf_x, float* cdf_y, float* slope, float params_out[6]) {
   if (!cdf_x || !cdf_y || !slope || !params_out)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL output");

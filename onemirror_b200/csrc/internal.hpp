@@ -44,6 +44,23 @@ void buie_build(float csr, float* cdf_x, float* cdf_y, float* slope, float param
 // Receiver geometry from the C description.
 qmcrt_status receiver_setup(const qmcrt_receiver& r, ReceiverGeom* g);
 
+// Device geometry of a field for one sun position: aimed normals and frames,
+// rectangle records and the grid CSR.  A scene owns one; a batch owns one per
+// (field, sun) item.
+struct SunGeom {
+  double* normal = nullptr;      // [3n]
+  double* frame = nullptr;       // [9n] u, n, v
+  float4* rect = nullptr;        // [3n] A(v0)+id, E1, E2
+  int4* cellbox = nullptr;       // [2n]
+  int32_t* cell_count = nullptr; // [cells]
+  int32_t* cell_start = nullptr; // [cells+1]
+  int32_t* entries = nullptr;    // [entry_cap]
+  float4* cell_rect = nullptr;   // [3*entry_cap]
+  float2* cell_yr = nullptr;     // [cells]
+  int* field_yr = nullptr;       // [2]
+  double* power = nullptr;       // [1] sum |n . sun| * A
+};
+
 struct PointsKey {
   uint64_t seed = 0, rays = 0;
   int rpp = 0, mode = -1;
@@ -119,3 +136,15 @@ struct qmcrt_scene {
   bool setup_timed = false;
   bool traced = false;
 };
+
+namespace qm {
+// The scene's own per-sun buffers as a SunGeom.
+SunGeom scene_geom(qmcrt_scene* s);
+// Allocate / free a SunGeom sized for scene s.
+qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g);
+void free_sun_geom(SunGeom* g);
+// Enqueue aiming + grid build of scene s for the (normalised) sun direction into g.
+qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
+                             cudaStream_t st);
+qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
+}  // namespace qm

@@ -31,7 +31,7 @@ struct AimArgs {
   int32_t* cell_count;
   float gpos[3], gcell[3];
   int gdims[3];
-  unsigned long long* stats;
+  double* power;
 };
 
 __device__ __forceinline__ d3 nrm3(d3 a) {
@@ -127,15 +127,19 @@ __global__ void aim_kernel(AimArgs a) {
     pw = fabs(dot(n, mk(a.sun[0], a.sun[1], a.sun[2]))) * sx * sz;
   }
   for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
-  if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd((double*)&a.stats[8], pw);
+  if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd(a.power, pw);
 }
 
 // Exclusive scan of cell_count into cell_start (one CTA of 1024 threads,
 // each scanning a contiguous run), then zero cell_count for the fill cursor.
 __global__ void __launch_bounds__(1024) scan_kernel(int32_t* count, int32_t* start, int64_t cells,
-                                                    int64_t cap, int32_t* flag) {
+                                                    int64_t cap, int32_t* flag, int* field_yr) {
   __shared__ int64_t part[1024];
   const int t = threadIdx.x;
+  if (t == 0) {  // empty height range for cell_finish_kernel's atomicMin/Max
+    field_yr[0] = 0x7F7FFFFF;                        // ordered(+FLT_MAX)
+    field_yr[1] = (int)(0xFF7FFFFFu ^ 0x7FFFFFFFu);  // ordered(-FLT_MAX)
+  }
   int64_t per = (cells + 1023) / 1024;
   int64_t b = t * per, e = min(cells, b + per);
   int64_t s = 0;
@@ -390,6 +394,65 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
   double sd[3] = {sun->dir[0], sun->dir[1], sun->dir[2]};
   double l = std::sqrt(sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]);
   if (!(l > 0) || !std::isfinite(l)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "sun direction is zero or not finite");
+  for (int i = 0; i < 3; ++i) sd[i] /= l;
+  QM_CUDA(cudaEventRecord(s->ev[0], st));
+  qmcrt_status e = launch_sun_geom(s, scene_geom(s), sd, k.quirks, st);
+  if (e) return e;
+  QM_CUDA(cudaEventRecord(s->ev[1], st));
+  s->setup_timed = true;
+  s->sun_key = k;
+  return QMCRT_OK;
+}
+
+SunGeom scene_geom(qmcrt_scene* s) {
+  SunGeom g;
+  g.normal = s->d_normal;
+  g.frame = s->d_frame;
+  g.rect = s->d_rect;
+  g.cellbox = s->d_cellbox;
+  g.cell_count = s->d_cell_count;
+  g.cell_start = s->d_cell_start;
+  g.entries = s->d_entries;
+  g.cell_rect = s->d_cell_rect;
+  g.cell_yr = s->d_cell_yr;
+  g.field_yr = s->d_field_yr;
+  g.power = reinterpret_cast<double*>(s->d_stats + 8);
+  return g;
+}
+
+qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
+  size_t n = (size_t)s->n;
+  qmcrt_status e;
+#define GALLOC(p, c)                    \
+  if ((e = dev_alloc(&(p), (c)))) {     \
+    free_sun_geom(g);                   \
+    return e;                           \
+  }
+  GALLOC(g->normal, 3 * n);
+  GALLOC(g->frame, 9 * n);
+  GALLOC(g->rect, 3 * n);
+  GALLOC(g->cellbox, 2 * n);
+  GALLOC(g->cell_count, (size_t)s->cells);
+  GALLOC(g->cell_start, (size_t)s->cells + 1);
+  GALLOC(g->entries, (size_t)s->entry_cap);
+  GALLOC(g->cell_rect, 3 * (size_t)s->entry_cap);
+  GALLOC(g->cell_yr, (size_t)s->cells);
+  GALLOC(g->field_yr, 2);
+  GALLOC(g->power, 1);
+#undef GALLOC
+  return QMCRT_OK;
+}
+
+void free_sun_geom(SunGeom* g) {
+  dev_free(g->normal); dev_free(g->frame); dev_free(g->rect); dev_free(g->cellbox); dev_free(g->cell_count);
+  dev_free(g->cell_start); dev_free(g->entries); dev_free(g->cell_rect); dev_free(g->cell_yr); dev_free(g->field_yr);
+  dev_free(g->power);
+}
+
+// Aim every heliostat for the sun (normalised) and rebuild the grid into g:
+// stream-ordered kernels only, so the sequence can be captured in a graph.
+qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
+                             cudaStream_t st) {
   AimArgs a{};
   a.n = s->n;
   a.pos = s->d_pos;
@@ -398,38 +461,29 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
   a.normal_in = s->has_normal ? s->d_normal_in : nullptr;
   a.tilt = s->has_tilt ? s->d_tilt : nullptr;
   std::memcpy(a.focus, s->rg.focus, sizeof(a.focus));
-  for (int i = 0; i < 3; ++i) a.sun[i] = sd[i] / l;
-  a.quirks = k.quirks;
-  a.normal = s->d_normal;
-  a.frame = s->d_frame;
-  a.rect = s->d_rect;
-  a.cellbox = s->d_cellbox;
-  a.cell_count = s->d_cell_count;
+  for (int i = 0; i < 3; ++i) a.sun[i] = sun[i];
+  a.quirks = quirks & (QMCRT_QUIRK_AABB_RADIUS | QMCRT_QUIRK_ZENITH_FRAME);
+  a.normal = g.normal;
+  a.frame = g.frame;
+  a.rect = g.rect;
+  a.cellbox = g.cellbox;
+  a.cell_count = g.cell_count;
   std::memcpy(a.gpos, s->gpos, sizeof(a.gpos));
   std::memcpy(a.gcell, s->gcell, sizeof(a.gcell));
   std::memcpy(a.gdims, s->gdims, sizeof(a.gdims));
-  a.stats = s->d_stats;
-  QM_CUDA(cudaEventRecord(s->ev[0], st));
-  QM_CUDA(cudaMemsetAsync(s->d_cell_count, 0, s->cells * sizeof(int32_t), st));
-  QM_CUDA(cudaMemsetAsync(s->d_stats + 8, 0, sizeof(unsigned long long), st));
+  a.power = g.power;
+  QM_CUDA(cudaMemsetAsync(g.cell_count, 0, s->cells * sizeof(int32_t), st));
+  QM_CUDA(cudaMemsetAsync(g.power, 0, sizeof(double), st));
   aim_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(a);
   QM_CUDA(cudaGetLastError());
-  scan_kernel<<<1, 1024, 0, st>>>(s->d_cell_count, s->d_cell_start, s->cells, s->entry_cap, s->d_flag);
+  scan_kernel<<<1, 1024, 0, st>>>(g.cell_count, g.cell_start, s->cells, s->entry_cap, s->d_flag, g.field_yr);
   QM_CUDA(cudaGetLastError());
-  fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, s->d_cellbox, s->d_cell_start, s->d_cell_count,
-                                                  s->d_entries, s->gdims[1], s->gdims[2], s->entry_cap);
+  fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, g.cellbox, g.cell_start, g.cell_count, g.entries,
+                                                  s->gdims[1], s->gdims[2], s->entry_cap);
   QM_CUDA(cudaGetLastError());
-  {
-    static const int init_yr[2] = {0x7F7FFFFF, (int)(0xFF7FFFFFu ^ 0x7FFFFFFFu)};  // ordered(+FLT_MAX), ordered(-FLT_MAX)
-    QM_CUDA(cudaMemcpyAsync(s->d_field_yr, init_yr, sizeof(init_yr), cudaMemcpyHostToDevice, st));
-  }
-  cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, s->d_cell_start, s->d_entries,
-                                                                        s->d_rect, s->d_cell_rect, s->d_cell_yr,
-                                                                        s->d_field_yr);
+  cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
+                                                                        g.cell_rect, g.cell_yr, g.field_yr);
   QM_CUDA(cudaGetLastError());
-  QM_CUDA(cudaEventRecord(s->ev[1], st));
-  s->setup_timed = true;
-  s->sun_key = k;
   return QMCRT_OK;
 }
 

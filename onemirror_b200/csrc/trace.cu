@@ -94,18 +94,18 @@ static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool 
   return records ? dispatch2<false, true>(a, stats, cull, st) : dispatch2<false, false>(a, stats, cull, st);
 }
 
-static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
-  if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
-  if (s->buie.csr == csr) return QMCRT_OK;
-  s->buie.host.resize(1025 + 1025 + 1024 + kBuieBuckets);
-  float* h = s->buie.host.data();
-  buie_build(csr, h, h + 1025, h + 2050, s->buie.params);
+// Buie table plus its guide, in the layout the kernels stage into shared
+// memory: cdf_x | cdf_y | slope | guide (int bits).
+void buie_with_guide(float csr, BuieTable* t) {
+  t->host.resize(1025 + 1025 + 1024 + kBuieBuckets);
+  float* h = t->host.data();
+  buie_build(csr, h, h + 1025, h + 2050, t->params);
   // guide table: for each uniform bucket of [0, core), a lower bound of the
   // interval index of every value the kernel maps to that bucket (one below
   // the index at the bucket's lower edge, which absorbs float rounding of the
   // bucket computation; CDF intervals are far wider than that rounding)
   const float* cy = h + 1025;
-  float inv_bucket = (float)kBuieBuckets / s->buie.params[2];
+  float inv_bucket = (float)kBuieBuckets / t->params[2];
   for (int b = 0; b < kBuieBuckets; ++b) {
     float edge = (float)b / inv_bucket;
     int lo = 0, hi = 1024;
@@ -117,13 +117,20 @@ static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
     int g = std::max(lo - 1, 0);
     std::memcpy(h + 3074 + b, &g, sizeof(int));
   }
-  s->buie.inv_bucket = inv_bucket;
-  QM_CUDA(cudaMemcpyAsync(s->d_buie, h, s->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
-  s->buie.csr = csr;
+  t->inv_bucket = inv_bucket;
+  t->csr = csr;
+}
+
+static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
+  if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
+  if (s->buie.csr == csr) return QMCRT_OK;
+  buie_with_guide(csr, &s->buie);
+  QM_CUDA(cudaMemcpyAsync(s->d_buie, s->buie.host.data(), s->buie.host.size() * sizeof(float),
+                          cudaMemcpyHostToDevice, st));
   return QMCRT_OK;
 }
 
-static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a) {
+void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a) {
   double sd[3] = {sun->dir[0], sun->dir[1], sun->dir[2]};
   double l = std::sqrt(sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]);
   for (int i = 0; i < 3; ++i) sd[i] /= l;
@@ -157,15 +164,15 @@ static void fill_common(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, T
   a->b_inv = 1 / (s->buie.params[1] + 1);  // scene_instance_process.cu:135
   a->b_inv_bucket = s->buie.inv_bucket;
   a->n_helio = s->n;
-  a->frame = s->d_frame;
+  a->frame = geo.frame;
   a->pos = s->d_pos;
   a->size = s->d_size;
   a->sigma = s->d_sigma;
   a->weight = s->d_helio_weight;
-  a->crect = s->d_cell_rect;
-  a->cstart = s->d_cell_start;
-  a->cell_yr = s->d_cell_yr;
-  a->field_yr = s->d_field_yr;
+  a->crect = geo.cell_rect;
+  a->cstart = geo.cell_start;
+  a->cell_yr = geo.cell_yr;
+  a->field_yr = geo.field_yr;
   for (int i = 0; i < 3; ++i) {
     a->gpos[i] = s->gpos[i];
     a->gcell[i] = s->gcell[i];
@@ -280,7 +287,7 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
   if ((e = ensure_points(s, p, st))) return e;
   TraceArgs a{};
-  fill_common(s, sun, p->quirks, &a);
+  fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
   a.rays = (uint32_t)(s->points * (int64_t)p->rays_per_point);
   a.rpp = p->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);
@@ -306,7 +313,7 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcr
   s->setup_timed = false;
   if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
   TraceArgs a{};
-  fill_common(s, sun, p->quirks, &a);
+  fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
   a.rays = (uint32_t)(t->points * t->rays_per_point);
   a.rpp = t->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);

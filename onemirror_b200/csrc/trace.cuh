@@ -278,110 +278,137 @@ __device__ __forceinline__ d3 rnorm(d3 a) {
   return r * a;
 }
 
+struct RayCounters {
+  uint32_t ray = 0, sh = 0, bl = 0, hit = 0, off = 0, test = 0, cell = 0;
+};
+
+// Deposit into the global maps with plain atomics.
+struct GlobalDeposit {
+  uint32_t* counts;
+  float* energy;
+  __device__ __forceinline__ void operator()(int pix, float e) const {
+    atomicAdd(counts + pix, 1u);
+    atomicAdd(energy + pix, e);
+  }
+};
+
+// Load the Buie table and its guide into shared memory (all threads).
+__device__ __forceinline__ void load_buie(const float* buie, float* s_tab, int* s_guide) {
+  for (int i = threadIdx.x; i < 3074; i += blockDim.x) s_tab[i] = __ldg(buie + i);
+  for (int i = threadIdx.x; i < kBuieBuckets; i += blockDim.x) s_guide[i] = __float_as_int(__ldg(buie + 3074 + i));
+}
+
+// One ray: the body of map_tracing (rectgrid_raytracing.cu:164-195).
+template <bool TABLES, bool RECORDS, bool STATS, bool CULL, class Dep>
+__device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
+                                          float fy0, float fy1, RayCounters& c, const Dep& deposit) {
+  const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
+  const uint32_t j = ray - g * (uint32_t)a.rpp;
+  const int h = __ldg(a.point_helio + g);
+  if (TABLES && (h < 0 || h >= a.n_helio)) {  // caller-provided ids: skip, never index out of range
+    if (RECORDS) {
+      if (a.flags) a.flags[ray] = 0;
+      if (a.pixel) a.pixel[ray] = -1;
+    }
+    return;
+  }
+  const float2 xz = __ldg(a.point_xz + g);
+  const double* F = a.frame + 9 * h;
+  frame64 fr;
+  fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
+  fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
+  fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
+  const float hy = 0.5f * __ldg(a.size + 3 * h + 1);
+  d3 o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
+         apply(fr, (double)xz.x, (double)hy, (double)xz.y);
+  float3 sl, tl;
+  float w = 1.f;
+  if (TABLES) {
+    // (start + j) mod T, kept in [0, T) for any caller-provided start
+    int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
+    int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
+    int64_t ib = (((int64_t)__ldg(a.start + gp) + j) % a.T + a.T) % a.T;
+    sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
+    tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
+  } else {
+    uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
+    float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
+    float st, ct, sp, cp;
+    sincos_small(th, &st, &ct);  // th <= 9.3 mrad
+    sincospif(2.f * u24f(r.y), &sp, &cp);
+    sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
+    float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
+    float ths = __ldg(a.sigma + h) * z;
+    uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
+    sincos_small(ths, &st, &ct);
+    sincospif(2.f * u24f(extra), &sp, &cp);
+    tl = f3(st * cp, ct, st * sp);
+    w = a.weight ? __ldg(a.weight + h) : 1.f;
+  }
+  // world sample (local2world(sample, sun_dir)), incident direction
+  d3 ws = mk(sl.x * a.su[0] + sl.y * a.sn[0] + sl.z * a.sv[0], sl.x * a.su[1] + sl.y * a.sn[1] + sl.z * a.sv[1],
+             sl.x * a.su[2] + sl.y * a.sn[2] + sl.z * a.sv[2]);
+  const float3 of = to_f(o);
+  uint8_t flag = 0;
+  int pix = -1;
+  if (dda_blocked<STATS, CULL>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, c.test, c.cell)) {
+    flag = QMCRT_RAY_SHADOWED;
+  } else {
+    d3 np = rnorm(apply(fr, (double)tl.x, (double)tl.y, (double)tl.z));
+    double di = dot(ws, np);
+    d3 rd = rnorm(ws - (2.0 * di) * np);  // reflect (i - 2 n (n.i)), normalise
+    if (dda_blocked<STATS, CULL>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
+      flag = QMCRT_RAY_BLOCKED;
+    } else if (receiver_hit(a, o, rd, pix)) {
+      flag = QMCRT_RAY_HIT;
+      if (pix < 0) {
+        flag |= QMCRT_RAY_OFFMAP;
+      } else {
+        // calEnergy (rectgrid_raytracing.cu:129-133), eta = 1
+        deposit(pix, (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w);
+      }
+    }
+  }
+  if (RECORDS) {
+    if (a.flags) a.flags[ray] = flag;
+    if (a.pixel) a.pixel[ray] = pix;
+  }
+  if (STATS) {
+    ++c.ray;
+    c.sh += (flag & QMCRT_RAY_SHADOWED) != 0;
+    c.bl += (flag & QMCRT_RAY_BLOCKED) != 0;
+    c.hit += (flag & QMCRT_RAY_HIT) != 0;
+    c.off += (flag & QMCRT_RAY_OFFMAP) != 0;
+  }
+}
+
+// Warp-reduce the counters and add them to stats[0..6].
+__device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned long long* stats) {
+  unsigned long long v[7] = {c.ray, c.sh, c.bl, c.hit, c.off, c.test, c.cell};
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    unsigned long long x = v[k];
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(stats + k, x);
+  }
+}
+
+// The plain tracer: one grid-stride pass over the rays of one trace.
 template <bool TABLES, bool RECORDS, bool STATS, bool CULL, int MINB = 1>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
   __shared__ float s_tab[1025 + 1025 + 1024];
   __shared__ int s_guide[kBuieBuckets];
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   if (!TABLES) {
-    for (int i = threadIdx.x; i < 3074; i += blockDim.x) s_tab[i] = __ldg(a.buie + i);
-    for (int i = threadIdx.x; i < kBuieBuckets; i += blockDim.x) s_guide[i] = __float_as_int(__ldg(a.buie + 3074 + i));
+    load_buie(a.buie, s_tab, s_guide);
     __syncthreads();
   }
-  uint32_t n_sh = 0, n_bl = 0, n_hit = 0, n_off = 0, n_ray = 0, n_test = 0, n_cell = 0;
+  RayCounters c;
+  const GlobalDeposit dep{a.counts, a.energy};
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride) {
-    const uint32_t ray = (uint32_t)r64;
-    const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
-    const uint32_t j = ray - g * (uint32_t)a.rpp;
-    const int h = __ldg(a.point_helio + g);
-    if (TABLES && (h < 0 || h >= a.n_helio)) {  // caller-provided ids: skip, never index out of range
-      if (RECORDS) {
-        if (a.flags) a.flags[ray] = 0;
-        if (a.pixel) a.pixel[ray] = -1;
-      }
-      continue;
-    }
-    const float2 xz = __ldg(a.point_xz + g);
-    const double* F = a.frame + 9 * h;
-    frame64 fr;
-    fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
-    fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
-    fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
-    const float hy = 0.5f * __ldg(a.size + 3 * h + 1);
-    d3 o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
-           apply(fr, (double)xz.x, (double)hy, (double)xz.y);
-    float3 sl, tl;
-    float w = 1.f;
-    if (TABLES) {
-      // (start + j) mod T, kept in [0, T) for any caller-provided start
-      int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
-      int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
-      int64_t ib = (((int64_t)__ldg(a.start + gp) + j) % a.T + a.T) % a.T;
-      sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
-      tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
-    } else {
-      uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
-      float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
-      float st, ct, sp, cp;
-      sincos_small(th, &st, &ct);  // th <= 9.3 mrad
-      sincospif(2.f * u24f(r.y), &sp, &cp);
-      sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
-      float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
-      float ths = __ldg(a.sigma + h) * z;
-      uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
-      sincos_small(ths, &st, &ct);
-      sincospif(2.f * u24f(extra), &sp, &cp);
-      tl = f3(st * cp, ct, st * sp);
-      w = a.weight ? __ldg(a.weight + h) : 1.f;
-    }
-    // world sample (local2world(sample, sun_dir)), incident direction
-    d3 ws = mk(sl.x * a.su[0] + sl.y * a.sn[0] + sl.z * a.sv[0], sl.x * a.su[1] + sl.y * a.sn[1] + sl.z * a.sv[1],
-               sl.x * a.su[2] + sl.y * a.sn[2] + sl.z * a.sv[2]);
-    const float3 of = to_f(o);
-    uint8_t flag = 0;
-    int pix = -1;
-    if (dda_blocked<STATS, CULL>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, n_test, n_cell)) {
-      flag = QMCRT_RAY_SHADOWED;
-    } else {
-      d3 np = rnorm(apply(fr, (double)tl.x, (double)tl.y, (double)tl.z));
-      double di = dot(ws, np);
-      d3 rd = rnorm(ws - (2.0 * di) * np);  // reflect (i - 2 n (n.i)), normalise
-      if (dda_blocked<STATS, CULL>(a, of, to_f(rd), h, fy0, fy1, n_test, n_cell)) {
-        flag = QMCRT_RAY_BLOCKED;
-      } else if (receiver_hit(a, o, rd, pix)) {
-        flag = QMCRT_RAY_HIT;
-        if (pix < 0) {
-          flag |= QMCRT_RAY_OFFMAP;
-        } else {
-          // calEnergy (rectgrid_raytracing.cu:129-133), eta = 1
-          float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w;
-          atomicAdd(a.counts + pix, 1u);
-          atomicAdd(a.energy + pix, e);
-        }
-      }
-    }
-    if (RECORDS) {
-      if (a.flags) a.flags[ray] = flag;
-      if (a.pixel) a.pixel[ray] = pix;
-    }
-    if (STATS) {
-      ++n_ray;
-      n_sh += (flag & QMCRT_RAY_SHADOWED) != 0;
-      n_bl += (flag & QMCRT_RAY_BLOCKED) != 0;
-      n_hit += (flag & QMCRT_RAY_HIT) != 0;
-      n_off += (flag & QMCRT_RAY_OFFMAP) != 0;
-    }
-  }
-  if (STATS) {
-    unsigned long long v[7] = {n_ray, n_sh, n_bl, n_hit, n_off, n_test, n_cell};
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      unsigned long long x = v[k];
-      for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
-      if ((threadIdx.x & 31) == 0 && x) atomicAdd(a.stats + k, x);
-    }
-  }
+  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride)
+    trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep);
+  if (STATS) flush_counters(c, a.stats);
 }
 
 }  // namespace qm

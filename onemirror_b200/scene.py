@@ -179,6 +179,62 @@ class SolarScene:
         return counts, flux, st
 
 
+class Batch:
+    """Many (field, sun) items traced in one persistent launch (qmcrt_batch_*)."""
+
+    def __init__(self, scenes, items, params):
+        self.scenes = list(scenes)
+        self.n_items = len(items)
+        arr = (C.c_void_p * len(self.scenes))(*[s.h for s in self.scenes])
+        its = (capi.BatchItem * len(items))()
+        for k, (si, sun) in enumerate(items):
+            its[k].scene = si
+            its[k].sun = sun
+        self.items = list(items)
+        self.params = params
+        h = C.c_void_p()
+        capi.check(capi.lib().qmcrt_batch_create(arr, len(self.scenes), its, len(items), C.byref(params), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().qmcrt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self):
+        t = capi.BatchTuning()
+        capi.check(capi.lib().qmcrt_batch_autotune(self.h, C.byref(t), _stream()))
+        return t
+
+    def set_tuning(self, chunk_rays, ctas_per_sm, tile):
+        t = capi.BatchTuning(chunk_rays, ctas_per_sm, tile, 0.0)
+        capi.check(capi.lib().qmcrt_batch_set_tuning(self.h, C.byref(t)))
+
+    def run(self):
+        capi.check(capi.lib().qmcrt_batch_run(self.h, _stream()))
+
+    def capture(self):
+        capi.check(capi.lib().qmcrt_batch_capture(self.h))
+
+    def launch(self):
+        capi.check(capi.lib().qmcrt_batch_launch(self.h, _stream()))
+
+    def read(self, i):
+        sc = self.scenes[self.items[i][0]]
+        counts = np.zeros(sc.res, np.uint32)
+        flux = np.zeros(sc.res, np.float32)
+        st = capi.TraceStats()
+        capi.check(capi.lib().qmcrt_batch_read(self.h, i, capi.as_u32p(counts), capi.as_fp(flux), C.byref(st),
+                                               _stream()))
+        return counts, flux, st
+
+
 def image_smooth(d_map, radius, ratio, method=capi.TRIM_SORTED):
     """Trimmed-mean smoothing of a device map (uint32/int32 counts or float32)."""
     assert d_map.is_cuda and d_map.is_contiguous() and d_map.dim() == 2

@@ -175,4 +175,33 @@ def large(rays=1 << 31, seed=7):
                     params(rays, 256, 0.22, seed))
 
 
+def equinox_suns(latitude=37.0, step_min=15.0, min_elevation=5.0, dni=1000.0, csr=0.1):
+    """Sun positions over one equinox day (declination 0) every step_min
+    minutes of solar time, keeping elevations >= min_elevation."""
+    out = []
+    L = capi.lib()
+    el, az = C.c_float(), C.c_float()
+    for k in range(int(24 * 60 / step_min)):
+        hour = k * step_min / 60.0
+        capi.check(L.qmcrt_solar_position(latitude, 0.0, 15.0 * (hour - 12.0), C.byref(el), C.byref(az)))
+        if el.value >= min_elevation:
+            out.append((hour, el.value, az.value, make_sun(el.value, az.value, dni, csr)))
+    return out
+
+
+def batched(rays_per_item=1 << 24, seed=11):
+    """Three fields of 300, 1000 and 4000 heliostats (10x10 m, flat 12x12 m
+    receivers at 256x256 on 150 m towers) over every sun position of an
+    equinox day at 37 N (15-minute steps, elevation >= 5 deg)."""
+    fields = []
+    for n, rmax in ((300, 350.0), (1000, 600.0), (4000, 1100.0)):
+        pos = layout(n, 10.0, 10.0, 100.0 if n > 300 else 80.0, rmax, mount=6.0, seed=FIELD_SEED + n)
+        size = np.tile(np.array([[10.0, 0.1, 10.0]], np.float32), (n, 1))
+        fields.append(Workload("batch_%d" % n, pos, size, 0.0025, flat_receiver(150.0, 12.0, 12.0, 256, 256),
+                               grid(25.0), make_sun(45.0, 180.0), params(rays_per_item, 256, 0.4, seed)))
+    suns = equinox_suns()
+    items = [(f, s[3]) for f in range(len(fields)) for s in suns]
+    return fields, suns, items, params(rays_per_item, 256, 0.4, seed)
+
+
 BUILDERS = {"small": small, "mid": mid, "large": large}
