@@ -226,6 +226,41 @@ def batch_section(reps=3):
             "tuning": {"chunk_rays": tuning.chunk_rays, "ctas_per_sm": tuning.ctas_per_sm, "tile": tuning.tile}}
 
 
+def adjoint_section(reps=5):
+    """Adjoint cost on the differentiable field (2000 heliostats, 128x128,
+    2^26 rays): plain trace, adjoint forward (bilinear deposit + tape + loss)
+    and backward, CUDA events after warm-up."""
+    import torch
+    from onemirror_b200.scene import SolarScene
+    from onemirror_b200 import workloads as W
+    w = W.differentiable()
+    sc = SolarScene(w.pos, w.size, w.receiver, w.grid, sigma=w.sigma, aim=w.aim, tilt=w.extra["tilt"])
+    target = torch.as_tensor(w.extra["target"], device="cuda")
+    plain_p = W.params(int(w.params.rays), 256, 0.5, seed=w.params.seed)
+    outs = sc._outputs(0, False)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    tf, tb, tp = [], [], []
+    for it in range(reps + 2):
+        ev[0].record()
+        sc.trace(w.sun, plain_p, stats=False, outputs=outs)
+        ev[1].record()
+        tape, _, _ = sc.adjoint_forward(w.sun, w.params, target, want_loss=False, flux=False)
+        ev[2].record()
+        sc.adjoint_backward(tape)
+        ev[3].record()
+        ev[3].synchronize()
+        SolarScene.tape_free(tape)
+        if it >= 2:
+            tp.append(ev[0].elapsed_time(ev[1]))
+            tf.append(ev[1].elapsed_time(ev[2]))
+            tb.append(ev[2].elapsed_time(ev[3]))
+    sc.close()
+    f, b, p = statistics.median(tf), statistics.median(tb), statistics.median(tp)
+    return {"heliostats": w.n, "rays": int(w.params.rays), "params": 4 * w.n, "plain_trace_ms": p,
+            "adjoint_forward_ms": f, "adjoint_backward_ms": b, "backward_over_forward": b / f,
+            "adjoint_over_plain_forward": (f + b) / p}
+
+
 def workload_name(w):
     return {"small": "100 heliostats 2x2 m, flat 5x5 m receiver 128x128, 409600 rays",
             "mid": "1000 heliostats 10x10 m to 600 m, flat 12x12 m receiver 256x256, 2^28 rays",
@@ -369,9 +404,10 @@ def b200_arm(a, rank, world, local):
         e2e = {"value": rays * world * a.e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "call": "qmcrt_trace_host"}
 
-    batch = None
+    batch = adj = None
     if rank == 0 and world == 1 and not a.no_batch and a.workload == "mid" and not a.rays:
         batch = batch_section()
+        adj = adjoint_section()
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         ob = oracle_sample(w, a.cpu_seconds)
@@ -416,6 +452,7 @@ def b200_arm(a, rank, world, local):
             "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
             "clocks": clocks,
             "batched": batch,
+            "adjoint": adj,
             "stats": {"shadowed": gst.shadowed / gst.rays, "blocked": gst.blocked / gst.rays,
                       "hit": gst.hit / gst.rays, "intercept_ratio": gst.intercept_ratio}}
     if rank == 0:

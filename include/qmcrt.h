@@ -384,6 +384,28 @@ qmcrt_status qmcrt_batch_maps(qmcrt_batch* batch, int32_t item, uint32_t** d_cou
 qmcrt_status qmcrt_batch_read(qmcrt_batch* batch, int32_t item, uint32_t* h_counts, float* h_flux,
                               qmcrt_trace_stats* stats, void* stream);
 
+/* ------------------------------------------------------------- adjoint
+ * No counterpart in the reference.  Gradient of the flux-map loss
+ * L = sum_p (F_p - T_p)^2 (F in W/m^2, bilinear deposition) with respect to
+ * each heliostat's aim offset (along the receiver's width and height axes, m)
+ * and extra normal tilt (about the mirror's local u and v axes, rad), at the
+ * scene's current aim points and tilts.  Pathwise derivative under the same
+ * random numbers; shadow/block/receiver visibility held constant.
+ *
+ * qmcrt_adjoint_forward traces params->rays rays (params->deposit must be
+ * QMCRT_DEPOSIT_BILINEAR, flat receiver, corrected mode), keeps one
+ * visibility byte per ray for at most state_bytes_max rays (0 = all; rays past
+ * the cap recompute their visibility in the backward pass), writes the flux
+ * map to d_flux (may be NULL) and, if `loss` is not NULL, synchronises and
+ * returns L.  qmcrt_adjoint_backward writes d_grad_aim [2n] and d_grad_tilt
+ * [2n] (device). */
+qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* scene, const qmcrt_sun* sun, const qmcrt_trace_params* params,
+                                   const float* d_target, uint64_t state_bytes_max, float* d_flux, double* loss,
+                                   qmcrt_tape** tape, void* stream);
+qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* tape, float* d_grad_aim, float* d_grad_tilt, void* stream);
+qmcrt_status qmcrt_tape_loss(qmcrt_tape* tape, double* loss, void* stream);
+qmcrt_status qmcrt_tape_free(qmcrt_tape* tape);
+
 /* ----------------------------------------------------------- smoothing
  * Trimmed-mean smoothing over a (2r+1)^2 window clipped at the border,
  * k = int(cnt * ratio) values dropped at each end (ImageSmoother::image_smooth,

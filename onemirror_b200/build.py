@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libqmcrt.so")
 
-SOURCES = ["host.cpp", "scene.cu", "trace.cu", "batch.cu", "smooth.cu", "probe.cu"]
+SOURCES = ["host.cpp", "scene.cu", "trace.cu", "batch.cu", "adjoint.cu", "smooth.cu", "probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 CUDA_ONLY = ["-lineinfo", "--expt-relaxed-constexpr"]

@@ -1,0 +1,514 @@
+// adjoint.cu — gradients of a flux-map loss with respect to each heliostat's
+// 2D aim offset and 2D normal tilt.  No counterpart in the reference.
+//
+// Forward: the tracer with bilinear deposition of each ray's energy into the
+// four pixels around its receiver hit, writing one visibility byte per ray
+// (the tape).  Loss: L = sum_p (F_p - T_p)^2 for flux F and target T; the
+// adjoint map G_p = dL/dE_p = 2 (F_p - T_p) * scale (E = raw energy map).
+// Backward: per ray, the pathwise derivative of its deposit under the same
+// random numbers, visibility held constant: the chain
+//   theta -> mirror frame (u, n, v) -> origin, perturbed normal -> reflected
+//   direction -> receiver (u, v) -> bilinear weights, and -> energy |s . n'|,
+// with the frame's Jacobian per heliostat from FP64 dual numbers and the
+// per-ray chain in FP32 tangents.  Rays past the tape's capacity recompute
+// their visibility (two traversals) instead of reading it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.hpp"
+#include "trace.cuh"
+
+using namespace qm;
+
+namespace qm {
+void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a);
+qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
+void buie_with_guide(float csr, BuieTable* t);
+
+constexpr int kAdjThreads = 256;
+
+// ------------------------------------------------------------ dual numbers
+// value + derivatives with respect to the 4 parameters of one heliostat
+struct dual {
+  double v, d[4];
+};
+__device__ __forceinline__ dual dc(double v) { return dual{v, {0, 0, 0, 0}}; }
+__device__ __forceinline__ dual operator+(dual a, dual b) {
+  return dual{a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2], a.d[3] + b.d[3]}};
+}
+__device__ __forceinline__ dual operator-(dual a, dual b) {
+  return dual{a.v - b.v, {a.d[0] - b.d[0], a.d[1] - b.d[1], a.d[2] - b.d[2], a.d[3] - b.d[3]}};
+}
+__device__ __forceinline__ dual operator*(dual a, dual b) {
+  dual r;
+  r.v = a.v * b.v;
+  for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+__device__ __forceinline__ dual operator/(dual a, dual b) {
+  dual r;
+  r.v = a.v / b.v;
+  for (int k = 0; k < 4; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
+  return r;
+}
+__device__ __forceinline__ dual dsqrt(dual a) {
+  dual r;
+  r.v = sqrt(a.v);
+  for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] / (2.0 * r.v);
+  return r;
+}
+struct dvec {
+  dual x, y, z;
+};
+__device__ __forceinline__ dvec operator+(dvec a, dvec b) { return dvec{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ dvec operator-(dvec a, dvec b) { return dvec{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ dvec scale(dual s, dvec a) { return dvec{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ dual ddot(dvec a, dvec b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ dvec dcross(dvec a, dvec b) {
+  return dvec{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ dvec dnorm(dvec a) {
+  dual l = dsqrt(ddot(a, a));
+  return dvec{a.x / l, a.y / l, a.z / l};
+}
+
+struct JacArgs {
+  int n;
+  const float *pos, *aim, *normal_in, *tilt;
+  double focus[3], sun[3], ew[3], eh[3];
+  float* jac;  // [36 n]: d(u, n, v)/d(theta), row-major 9 x 4
+};
+
+// Jacobian of the mirror frame with respect to theta = (aim offset along the
+// receiver width, along its height, extra tilt about u, about v), evaluated at
+// theta = 0 with the aiming and tilt rule of the aim kernel (heliostat.cpp:51-58).
+__global__ void frame_jacobian_kernel(JacArgs a) {
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= a.n) return;
+  dvec n0;
+  if (a.normal_in) {
+    n0 = dnorm(dvec{dc(a.normal_in[3 * h]), dc(a.normal_in[3 * h + 1]), dc(a.normal_in[3 * h + 2])});
+  } else {
+    double t[3];
+    for (int i = 0; i < 3; ++i) t[i] = a.aim ? (double)a.aim[3 * h + i] : a.focus[i];
+    dvec aimp;
+    dual* ap[3] = {&aimp.x, &aimp.y, &aimp.z};
+    for (int i = 0; i < 3; ++i) *ap[i] = dual{t[i], {a.ew[i], a.eh[i], 0, 0}};
+    dvec p{dc(a.pos[3 * h]), dc(a.pos[3 * h + 1]), dc(a.pos[3 * h + 2])};
+    dvec r = dnorm(aimp - p);
+    n0 = dnorm(r - dvec{dc(a.sun[0]), dc(a.sun[1]), dc(a.sun[2])});
+  }
+  // frame of the untilted normal, then the tilt (tx + theta2, tz + theta3)
+  dvec u0 = dnorm(dvec{n0.z, dc(0), dc(0) - n0.x});
+  dvec v0 = dnorm(dcross(u0, n0));
+  dual tx = dual{a.tilt ? (double)a.tilt[2 * h] : 0.0, {0, 0, 1, 0}};
+  dual tz = dual{a.tilt ? (double)a.tilt[2 * h + 1] : 0.0, {0, 0, 0, 1}};
+  dvec n = dnorm(n0 + scale(tx, u0) + scale(tz, v0));
+  dvec u = dnorm(dvec{n.z, dc(0), dc(0) - n.x});
+  dvec v = dnorm(dcross(u, n));
+  const dvec fr[3] = {u, n, v};
+  float* J = a.jac + 36 * h;
+  for (int b = 0; b < 3; ++b) {
+    const dual* c[3] = {&fr[b].x, &fr[b].y, &fr[b].z};
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 4; ++k) J[(3 * b + i) * 4 + k] = (float)c[i]->d[k];
+  }
+}
+
+struct AdjArgs {
+  TraceArgs t;
+  double ew[3], eh[3];  // receiver width / height unit axes (flat receivers)
+  uint8_t* tape;        // one visibility byte per ray
+  uint64_t saved;       // rays with a byte in the tape
+  const float* G;       // adjoint map (backward)
+  const float* jac;     // frame Jacobians (backward)
+  float* grad_aim;      // [2n]
+  float* grad_tilt;     // [2n]
+};
+
+// Receiver hit with the continuous (u, v) (flat receivers): along E1 (rows)
+// and E2 (columns), each in [0, 1]; t along the ray.
+__device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, double* u, double* v) {
+  d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
+  d3 pv = cross(d, E2);
+  double det = dot(E1, pv);
+  if (fabs(det) < 1e-6) return false;
+  double inv = 1.0 / det;
+  d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
+  *u = dot(T, pv) * inv;
+  if (*u < 0 || *u > 1) return false;
+  d3 qv = cross(T, E1);
+  *v = dot(d, qv) * inv;
+  if (*v < 0 || *v > 1) return false;
+  return dot(E2, qv) * inv >= 1e-6;
+}
+
+// Visibility and hit geometry of one ray (shadow, reflection, block, receiver).
+template <bool CULL>
+__device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, float fy0, float fy1, d3* np, d3* rd,
+                                         double* u, double* v) {
+  uint32_t nt = 0, nc = 0;
+  const float3 of = to_f(R.o);
+  if (dda_blocked<false, CULL>(a, of, f3((float)-R.ws.x, (float)-R.ws.y, (float)-R.ws.z), R.h, fy0, fy1, nt, nc))
+    return false;
+  *np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
+  double di = dot(R.ws, *np);
+  *rd = rnorm(R.ws - (2.0 * di) * *np);
+  if (dda_blocked<false, CULL>(a, of, to_f(*rd), R.h, fy0, fy1, nt, nc)) return false;
+  return receiver_uv(a, R.o, *rd, u, v);
+}
+
+template <bool CULL>
+__global__ void __launch_bounds__(kAdjThreads) adjoint_forward_kernel(const AdjArgs A) {
+  __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ int s_guide[kBuieBuckets];
+  const TraceArgs& a = A.t;
+  load_buie(a.buie, s_tab, s_guide);
+  __syncthreads();
+  const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride) {
+    const uint32_t ray = (uint32_t)r64;
+    RaySetup R;
+    ray_setup<false>(a, s_tab, s_guide, ray, R);
+    d3 np, rd;
+    double u, v;
+    const bool hit = ray_hits<CULL>(a, R, fy0, fy1, &np, &rd, &u, &v);
+    if (r64 < A.saved) A.tape[r64] = hit ? 1 : 0;
+    if (!hit) continue;
+    float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * R.w;
+    float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
+    int i0 = (int)floorf(px), j0 = (int)floorf(py);
+    float fx = px - (float)i0, fy = py - (float)j0;
+    const float wgt[4] = {(1.f - fx) * (1.f - fy), fx * (1.f - fy), (1.f - fx) * fy, fx * fy};
+    for (int k = 0; k < 4; ++k) {
+      int ci = i0 + (k & 1), cj = j0 + (k >> 1);
+      if (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) continue;
+      atomicAdd(a.energy + cj * a.res_x + ci, e * wgt[k]);
+    }
+  }
+}
+
+struct LossArgs {
+  const float* energy;
+  const float* target;
+  float* flux;  // may be NULL
+  float* G;
+  float scale;
+  int64_t res;
+  double* loss;
+};
+
+__global__ void loss_kernel(LossArgs a) {
+  double acc = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.res; i += (int64_t)gridDim.x * blockDim.x) {
+    float f = a.energy[i] * a.scale;
+    if (a.flux) a.flux[i] = f;
+    float d = f - a.target[i];
+    acc += (double)d * d;
+    a.G[i] = 2.f * d * a.scale;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(a.loss, acc);
+}
+
+__device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(s * a.x + b.x, s * a.y + b.y, s * a.z + b.z); }
+
+template <bool CULL>
+__global__ void __launch_bounds__(kAdjThreads) adjoint_backward_kernel(const AdjArgs A) {
+  __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ int s_guide[kBuieBuckets];
+  const TraceArgs& a = A.t;
+  load_buie(a.buie, s_tab, s_guide);
+  __syncthreads();
+  const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
+  const float3 E1 = f3((float)a.rE1[0], (float)a.rE1[1], (float)a.rE1[2]);
+  const float3 E2 = f3((float)a.rE2[0], (float)a.rE2[1], (float)a.rE2[2]);
+  const float3 sd = f3((float)a.sdir[0], (float)a.sdir[1], (float)a.sdir[2]);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t end = ((uint64_t)a.rays + 31) / 32 * 32;  // whole warps keep the shuffles converged
+  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < end; r64 += stride) {
+    float gk[4] = {0.f, 0.f, 0.f, 0.f};
+    int h = -1;
+    if (r64 < a.rays) {
+      const uint32_t ray = (uint32_t)r64;
+      RaySetup R;
+      ray_setup<false>(a, s_tab, s_guide, ray, R);
+      h = R.h;
+      bool hit;
+      d3 np, rd;
+      double u = 0, v = 0;
+      if (r64 < A.saved) {
+        hit = A.tape[r64] != 0;
+        if (hit) {  // rebuild the hit geometry without the traversals
+          np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
+          rd = rnorm(R.ws - (2.0 * dot(R.ws, np)) * np);
+          hit = receiver_uv(a, R.o, rd, &u, &v);
+        }
+      } else {
+        hit = ray_hits<CULL>(a, R, fy0, fy1, &np, &rd, &u, &v);
+      }
+      if (hit) {
+        // bilinear corners and the adjoint map there
+        float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
+        int i0 = (int)floorf(px), j0 = (int)floorf(py);
+        float fx = px - (float)i0, fy = py - (float)j0;
+        float Gc[4];
+        for (int k = 0; k < 4; ++k) {
+          int ci = i0 + (k & 1), cj = j0 + (k >> 1);
+          Gc[k] = (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) ? 0.f : __ldg(A.G + cj * a.res_x + ci);
+        }
+        const float gW = (1.f - fx) * (1.f - fy) * Gc[0] + fx * (1.f - fy) * Gc[1] + (1.f - fx) * fy * Gc[2] + fx * fy * Gc[3];
+        const float gWx = (1.f - fy) * (Gc[1] - Gc[0]) + fy * (Gc[3] - Gc[2]);
+        const float gWy = (1.f - fx) * (Gc[2] - Gc[0]) + fx * (Gc[3] - Gc[1]);
+        // forward quantities in float
+        const float3 npf = to_f(np), rdf = to_f(rd), wsf = to_f(R.ws);
+        d3 npr = apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z);
+        const float lnp = (float)sqrt(dot(npr, npr));
+        d3 rr = R.ws - (2.0 * dot(R.ws, np)) * np;
+        const float lr = (float)sqrt(dot(rr, rr));
+        const float nws = dot(npf, wsf);
+        const float sdn = dot(sd, npf);
+        const float e = fabsf(sdn) * R.w, sg = sdn < 0.f ? -1.f : 1.f;
+        // t along the reflected ray to the receiver plane (for d(hit) = do + t dr)
+        const float3 cr = cross(E2, rdf);
+        const float den = dot(E1, cr);
+        d3 Tt = R.o - mk(a.rA[0], a.rA[1], a.rA[2]);
+        d3 qv = cross(Tt, mk(a.rE1[0], a.rE1[1], a.rE1[2]));
+        const float t = (float)(dot(mk(a.rE2[0], a.rE2[1], a.rE2[2]), qv) /
+                                dot(mk(a.rE1[0], a.rE1[1], a.rE1[2]), cross(rd, mk(a.rE2[0], a.rE2[1], a.rE2[2]))));
+        const float* J = A.jac + 36 * h;
+        const float x = R.xz.x, z = R.xz.y, hy = R.hy;
+        for (int k = 0; k < 4; ++k) {
+          const float3 du = f3(__ldg(J + 0 * 4 + k), __ldg(J + 1 * 4 + k), __ldg(J + 2 * 4 + k));
+          const float3 dn = f3(__ldg(J + 3 * 4 + k), __ldg(J + 4 * 4 + k), __ldg(J + 5 * 4 + k));
+          const float3 dv = f3(__ldg(J + 6 * 4 + k), __ldg(J + 7 * 4 + k), __ldg(J + 8 * 4 + k));
+          const float3 dO = fma3(x, du, fma3(hy, dn, z * dv));
+          float3 dN = fma3(R.tl.x, du, fma3(R.tl.y, dn, R.tl.z * dv));
+          dN = (1.f / lnp) * (dN - dot(npf, dN) * npf);  // d(normalize)
+          float3 dR = -2.f * (dot(dN, wsf) * npf + nws * dN);
+          dR = (1.f / lr) * (dR - dot(rdf, dR) * rdf);
+          const float3 b = dO + t * dR;  // d(hit point) = du E1 + dv E2 along the plane
+          const float duk = dot(b, cr) / den;
+          const float dvk = dot(E1, cross(b, rdf)) / den;
+          const float dpx = (float)a.res_x * dvk, dpy = (float)a.res_y * duk;
+          const float dek = sg * dot(sd, dN) * R.w;
+          gk[k] = dek * gW + e * (gWx * dpx + gWy * dpy);
+        }
+      }
+    }
+    // one atomic per warp and parameter when the warp's rays share a heliostat
+    const unsigned full = 0xffffffffu;
+    const int h0 = __shfl_sync(full, h, 0);
+    const bool uniform = __all_sync(full, h == h0 || h < 0);
+    if (uniform && h0 >= 0) {
+      for (int k = 0; k < 4; ++k)
+        for (int o = 16; o > 0; o >>= 1) gk[k] += __shfl_down_sync(full, gk[k], o);
+      if ((threadIdx.x & 31) == 0) {
+        atomicAdd(A.grad_aim + 2 * h0, gk[0]);
+        atomicAdd(A.grad_aim + 2 * h0 + 1, gk[1]);
+        atomicAdd(A.grad_tilt + 2 * h0, gk[2]);
+        atomicAdd(A.grad_tilt + 2 * h0 + 1, gk[3]);
+      }
+    } else if (h >= 0) {
+      atomicAdd(A.grad_aim + 2 * h, gk[0]);
+      atomicAdd(A.grad_aim + 2 * h + 1, gk[1]);
+      atomicAdd(A.grad_tilt + 2 * h, gk[2]);
+      atomicAdd(A.grad_tilt + 2 * h + 1, gk[3]);
+    }
+  }
+}
+
+static int adj_blocks(uint64_t rays) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * 4, (rays + kAdjThreads - 1) / kAdjThreads));
+}
+
+}  // namespace qm
+
+struct qmcrt_tape {
+  qmcrt_scene* scene = nullptr;
+  qmcrt_sun sun{};
+  qmcrt_trace_params params{};
+  qm::AdjArgs args{};
+  qm::BuieTable buie;
+  float* d_buie = nullptr;
+  uint8_t* d_tape = nullptr;
+  float* d_G = nullptr;
+  float* d_jac = nullptr;
+  double* d_loss = nullptr;
+  float* d_energy = nullptr;
+  bool cull = true;
+};
+
+namespace qm {
+static qmcrt_status tape_geometry(qmcrt_tape* t, cudaStream_t st) {
+  qmcrt_scene* s = t->scene;
+  qmcrt_status e;
+  if ((e = ensure_sun(s, &t->sun, t->params.quirks, st))) return e;
+  if ((e = ensure_points(s, &t->params, st))) return e;
+  return QMCRT_OK;
+}
+}  // namespace qm
+
+extern "C" {
+
+qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace_params* p,
+                                   const float* d_target, uint64_t state_bytes_max, float* d_flux, double* loss,
+                                   qmcrt_tape** tape, void* stream) {
+  if (!s || !sun || !p || !d_target || !tape) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  *tape = nullptr;
+  if (s->rg.type != QMCRT_RECEIVER_FLAT) return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint needs a flat receiver");
+  if (p->deposit != QMCRT_DEPOSIT_BILINEAR) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "the adjoint deposits bilinearly");
+  if (p->point_mode != QMCRT_POINTS_POISSON || p->rays == 0 || p->rays > 0xFFFFFFFFull)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "the adjoint needs Poisson points and 0 < rays < 2^32");
+  if (p->quirks & ~QMCRT_QUIRK_ZENITH_FRAME)
+    return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint traces in corrected mode");
+  if (!(sun->csr > 0.f && sun->csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
+  cudaStream_t st = (cudaStream_t)stream;
+  qmcrt_tape* t = new qmcrt_tape();
+  t->scene = s;
+  t->sun = *sun;
+  t->params = *p;
+  qmcrt_status e;
+  int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
+  uint64_t saved = state_bytes_max == 0 ? p->rays : std::min<uint64_t>(p->rays, state_bytes_max);
+  cudaError_t ce = cudaMalloc(&t->d_tape, std::max<uint64_t>(saved, 1));
+  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_G, res * sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_jac, 36 * (size_t)s->n * sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_loss, sizeof(double));
+  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_energy, res * sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_buie, (1025 + 1025 + 1024 + kBuieBuckets) * sizeof(float));
+  if (ce != cudaSuccess) {
+    qmcrt_tape_free(t);
+    return cuda_error(ce, "adjoint tape allocation");
+  }
+  if ((e = tape_geometry(t, st))) {
+    qmcrt_tape_free(t);
+    return e;
+  }
+  buie_with_guide(sun->csr, &t->buie);
+  AdjArgs& A = t->args;
+  fill_trace_args(s, scene_geom(s), sun, p->quirks, &A.t);
+  A.t.buie = t->d_buie;
+  A.t.b_total = t->buie.params[3];
+  A.t.b_core = t->buie.params[2];
+  A.t.b_B = t->buie.params[4];
+  A.t.b_C = t->buie.params[5];
+  A.t.b_inv = 1 / (t->buie.params[1] + 1);
+  A.t.b_inv_bucket = t->buie.inv_bucket;
+  A.t.rays = (uint32_t)p->rays;
+  A.t.rpp = p->rays_per_point;
+  A.t.rpp_shift = (A.t.rpp & (A.t.rpp - 1)) ? -1 : __builtin_ctz((unsigned)A.t.rpp);
+  A.t.key = make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32));
+  A.t.item = p->item;
+  A.t.point_xz = s->d_point_xz;
+  A.t.point_helio = s->d_point_helio;
+  A.t.energy = t->d_energy;
+  double l1 = 0, l2 = 0;
+  for (int i = 0; i < 3; ++i) {
+    A.ew[i] = s->rg.v3[i] - s->rg.v0[i];
+    A.eh[i] = s->rg.v1[i] - s->rg.v0[i];
+    l1 += A.ew[i] * A.ew[i];
+    l2 += A.eh[i] * A.eh[i];
+  }
+  for (int i = 0; i < 3; ++i) {
+    A.ew[i] /= std::sqrt(l1);
+    A.eh[i] /= std::sqrt(l2);
+  }
+  A.tape = t->d_tape;
+  A.saved = saved;
+  A.G = t->d_G;
+  A.jac = t->d_jac;
+  const int blocks = adj_blocks(p->rays);
+  QM_CUDA(cudaMemcpyAsync(t->d_buie, t->buie.host.data(), t->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
+  QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
+  adjoint_forward_kernel<true><<<blocks, kAdjThreads, 0, st>>>(A);
+  QM_CUDA(cudaGetLastError());
+  LossArgs la{t->d_energy, d_target, d_flux, t->d_G,
+              (float)((double)sun->dni * p->reflectivity / ((double)p->rays_per_point * s->rg.pixel_area)), res,
+              t->d_loss};
+  loss_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
+  QM_CUDA(cudaGetLastError());
+  if (loss) {
+    QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    QM_CUDA(cudaStreamSynchronize(st));
+  }
+  *tape = t;
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_grad_tilt, void* stream) {
+  if (!t || !d_grad_aim || !d_grad_tilt) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  qmcrt_scene* s = t->scene;
+  qmcrt_status e;
+  if ((e = tape_geometry(t, st))) return e;  // re-aims only if the scene moved on to another sun
+  AdjArgs A = t->args;
+  fill_trace_args(s, scene_geom(s), &t->sun, t->params.quirks, &A.t);
+  A.t.buie = t->d_buie;
+  A.t.b_total = t->buie.params[3];
+  A.t.b_core = t->buie.params[2];
+  A.t.b_B = t->buie.params[4];
+  A.t.b_C = t->buie.params[5];
+  A.t.b_inv = 1 / (t->buie.params[1] + 1);
+  A.t.b_inv_bucket = t->buie.inv_bucket;
+  A.t.rays = t->args.t.rays;
+  A.t.rpp = t->args.t.rpp;
+  A.t.rpp_shift = t->args.t.rpp_shift;
+  A.t.key = t->args.t.key;
+  A.t.item = t->args.t.item;
+  A.t.point_xz = s->d_point_xz;
+  A.t.point_helio = s->d_point_helio;
+  A.t.energy = t->d_energy;
+  A.grad_aim = d_grad_aim;
+  A.grad_tilt = d_grad_tilt;
+  JacArgs j{};
+  j.n = s->n;
+  j.pos = s->d_pos;
+  j.aim = s->has_aim ? s->d_aim : nullptr;
+  j.normal_in = s->has_normal ? s->d_normal_in : nullptr;
+  j.tilt = s->has_tilt ? s->d_tilt : nullptr;
+  for (int i = 0; i < 3; ++i) {
+    j.focus[i] = s->rg.focus[i];
+    j.ew[i] = A.ew[i];
+    j.eh[i] = A.eh[i];
+  }
+  double l = std::sqrt((double)t->sun.dir[0] * t->sun.dir[0] + (double)t->sun.dir[1] * t->sun.dir[1] +
+                       (double)t->sun.dir[2] * t->sun.dir[2]);
+  for (int i = 0; i < 3; ++i) j.sun[i] = t->sun.dir[i] / l;
+  j.jac = t->d_jac;
+  QM_CUDA(cudaMemsetAsync(d_grad_aim, 0, 2 * (size_t)s->n * sizeof(float), st));
+  QM_CUDA(cudaMemsetAsync(d_grad_tilt, 0, 2 * (size_t)s->n * sizeof(float), st));
+  frame_jacobian_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(j);
+  QM_CUDA(cudaGetLastError());
+  adjoint_backward_kernel<true><<<adj_blocks(A.t.rays), kAdjThreads, 0, st>>>(A);
+  QM_CUDA(cudaGetLastError());
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_tape_loss(qmcrt_tape* t, double* loss, void* stream) {
+  if (!t || !loss) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_tape_free(qmcrt_tape* t) {
+  if (!t) return QMCRT_OK;
+  cudaFree(t->d_tape);
+  cudaFree(t->d_G);
+  cudaFree(t->d_jac);
+  cudaFree(t->d_loss);
+  cudaFree(t->d_energy);
+  cudaFree(t->d_buie);
+  delete t;
+  return QMCRT_OK;
+}
+
+}  // extern "C"

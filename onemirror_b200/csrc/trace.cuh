@@ -298,56 +298,92 @@ __device__ __forceinline__ void load_buie(const float* buie, float* s_tab, int* 
   for (int i = threadIdx.x; i < kBuieBuckets; i += blockDim.x) s_guide[i] = __float_as_int(__ldg(buie + 3074 + i));
 }
 
+// Everything a ray needs before its traversals: heliostat, local point,
+// mirror frame, origin, the sun sample (local and world) and the local
+// perturbation of the normal.
+struct RaySetup {
+  int h;
+  float2 xz;
+  float hy;
+  frame64 fr;
+  d3 o;
+  float3 sl, tl;
+  d3 ws;
+  float w;
+};
+
+// Sun sample and slope-error perturbation of ray `ray` from Philox (seed,
+// ray id): theta from the Buie inverse CDF, phi uniform; slope theta
+// Gaussian (Box-Muller), phi uniform (set_samplelights, set_perturbation).
+__device__ __forceinline__ void philox_samples(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
+                                               float sigma, float3* sl, float3* tl) {
+  uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
+  float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
+  float st, ct, sp, cp;
+  sincos_small(th, &st, &ct);  // th <= 9.3 mrad
+  sincospif(2.f * u24f(r.y), &sp, &cp);
+  *sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
+  float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
+  float ths = sigma * z;
+  uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
+  sincos_small(ths, &st, &ct);
+  sincospif(2.f * u24f(extra), &sp, &cp);
+  *tl = f3(st * cp, ct, st * sp);
+}
+
+// Returns false for a ray to skip (table mode with an out-of-range heliostat id).
+template <bool TABLES>
+__device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
+                                          RaySetup& R) {
+  const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
+  const uint32_t j = ray - g * (uint32_t)a.rpp;
+  const int h = __ldg(a.point_helio + g);
+  if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
+  R.h = h;
+  R.xz = __ldg(a.point_xz + g);
+  const double* F = a.frame + 9 * h;
+  R.fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
+  R.fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
+  R.fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
+  R.hy = 0.5f * __ldg(a.size + 3 * h + 1);
+  R.o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
+        apply(R.fr, (double)R.xz.x, (double)R.hy, (double)R.xz.y);
+  R.w = 1.f;
+  if (TABLES) {
+    // (start + j) mod T, kept in [0, T) for any caller-provided start
+    int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
+    int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
+    int64_t ib = (((int64_t)__ldg(a.start + gp) + j) % a.T + a.T) % a.T;
+    R.sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
+    R.tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
+  } else {
+    philox_samples(a, s_tab, s_guide, ray, __ldg(a.sigma + h), &R.sl, &R.tl);
+    R.w = a.weight ? __ldg(a.weight + h) : 1.f;
+  }
+  // world sample (local2world(sample, sun_dir)), incident direction
+  const float3 sl = R.sl;
+  R.ws = mk(sl.x * a.su[0] + sl.y * a.sn[0] + sl.z * a.sv[0], sl.x * a.su[1] + sl.y * a.sn[1] + sl.z * a.sv[1],
+            sl.x * a.su[2] + sl.y * a.sn[2] + sl.z * a.sv[2]);
+  return true;
+}
+
 // One ray: the body of map_tracing (rectgrid_raytracing.cu:164-195).
 template <bool TABLES, bool RECORDS, bool STATS, bool CULL, class Dep>
 __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit) {
-  const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
-  const uint32_t j = ray - g * (uint32_t)a.rpp;
-  const int h = __ldg(a.point_helio + g);
-  if (TABLES && (h < 0 || h >= a.n_helio)) {  // caller-provided ids: skip, never index out of range
+  RaySetup R;
+  if (!ray_setup<TABLES>(a, s_tab, s_guide, ray, R)) {
     if (RECORDS) {
       if (a.flags) a.flags[ray] = 0;
       if (a.pixel) a.pixel[ray] = -1;
     }
     return;
   }
-  const float2 xz = __ldg(a.point_xz + g);
-  const double* F = a.frame + 9 * h;
-  frame64 fr;
-  fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
-  fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
-  fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
-  const float hy = 0.5f * __ldg(a.size + 3 * h + 1);
-  d3 o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
-         apply(fr, (double)xz.x, (double)hy, (double)xz.y);
-  float3 sl, tl;
-  float w = 1.f;
-  if (TABLES) {
-    // (start + j) mod T, kept in [0, T) for any caller-provided start
-    int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
-    int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
-    int64_t ib = (((int64_t)__ldg(a.start + gp) + j) % a.T + a.T) % a.T;
-    sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
-    tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
-  } else {
-    uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
-    float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
-    float st, ct, sp, cp;
-    sincos_small(th, &st, &ct);  // th <= 9.3 mrad
-    sincospif(2.f * u24f(r.y), &sp, &cp);
-    sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
-    float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
-    float ths = __ldg(a.sigma + h) * z;
-    uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
-    sincos_small(ths, &st, &ct);
-    sincospif(2.f * u24f(extra), &sp, &cp);
-    tl = f3(st * cp, ct, st * sp);
-    w = a.weight ? __ldg(a.weight + h) : 1.f;
-  }
-  // world sample (local2world(sample, sun_dir)), incident direction
-  d3 ws = mk(sl.x * a.su[0] + sl.y * a.sn[0] + sl.z * a.sv[0], sl.x * a.su[1] + sl.y * a.sn[1] + sl.z * a.sv[1],
-             sl.x * a.su[2] + sl.y * a.sn[2] + sl.z * a.sv[2]);
+  const int h = R.h;
+  const frame64& fr = R.fr;
+  const d3 o = R.o, ws = R.ws;
+  const float3 tl = R.tl;
+  const float w = R.w;
   const float3 of = to_f(o);
   uint8_t flag = 0;
   int pix = -1;

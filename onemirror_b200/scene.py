@@ -66,6 +66,10 @@ class SolarScene:
             capi.lib().qmcrt_scene_destroy(self.h)
             self.h = None
 
+    def update_field(self):
+        """Upload the (modified) host arrays pos/size/aim/normal/tilt/slope_sigma."""
+        capi.check(capi.lib().qmcrt_scene_set_field(self.h, C.byref(self.field()), _stream()))
+
     def __del__(self):
         try:
             self.close()
@@ -162,6 +166,27 @@ class SolarScene:
         torch.cuda.current_stream().synchronize()
         r["stats"] = st
         return r
+
+    def adjoint_forward(self, sun, params, target, state_bytes_max=0, want_loss=True, flux=True):
+        """Bilinear forward pass + loss against `target` (device [res] W/m^2).
+        Returns (tape, loss or None, flux map or None)."""
+        tape = C.c_void_p()
+        loss = C.c_double()
+        fl = torch.zeros(self.res, dtype=torch.float32, device="cuda") if flux else None
+        capi.check(capi.lib().qmcrt_adjoint_forward(self.h, C.byref(sun), C.byref(params), _ptr(target),
+                                                    state_bytes_max, _ptr(fl), C.byref(loss) if want_loss else None,
+                                                    C.byref(tape), _stream()))
+        return tape, (loss.value if want_loss else None), fl
+
+    def adjoint_backward(self, tape):
+        ga = torch.empty((self.n, 2), dtype=torch.float32, device="cuda")
+        gt = torch.empty((self.n, 2), dtype=torch.float32, device="cuda")
+        capi.check(capi.lib().qmcrt_adjoint_backward(tape, _ptr(ga), _ptr(gt), _stream()))
+        return ga, gt
+
+    @staticmethod
+    def tape_free(tape):
+        capi.lib().qmcrt_tape_free(tape)
 
     def timing(self):
         t = capi.Timing()

@@ -204,4 +204,33 @@ def batched(rays_per_item=1 << 24, seed=11):
     return fields, suns, items, params(rays_per_item, 256, 0.4, seed)
 
 
+def differentiable(n=2000, rays=1 << 26, seed=13):
+    """2000 heliostats 10x10 m, flat 12x12 m receiver at 128x128 on a 150 m
+    tower, sun at 40 deg; explicit aim points (the receiver centre) and zero
+    tilts are the parameters; target: a uniform 800 kW/m^2 disk of radius 4 m
+    whose centre is offset by a seeded N(0, 0.5 m) in the receiver plane."""
+    pos = layout(n, 10.0, 10.0, 100.0, 800.0, mount=6.0, seed=FIELD_SEED + 7)
+    size = np.tile(np.array([[10.0, 0.1, 10.0]], np.float32), (n, 1))
+    rec = flat_receiver(150.0, 12.0, 12.0, 128, 128)
+    aim = np.tile(np.array([[0.0, 150.0, 0.0]], np.float32), (n, 1))
+    p = params(rays, 256, 0.5, seed)
+    p.deposit = capi.DEPOSIT_BILINEAR
+    w = Workload("differentiable", pos, size, 0.0025, rec, grid(25.0), make_sun(40.0, 180.0, 1000.0, 0.1), p, aim=aim)
+    w.extra["tilt"] = np.zeros((n, 2), np.float32)
+    w.extra["target"] = target_disk(rec, 800e3, 4.0, np.random.default_rng(FIELD_SEED + 9).normal(0, 0.5, 2))
+    return w
+
+
+def target_disk(rec, level, radius, centre_offset):
+    """Target flux map [res_y, res_x]: `level` W/m^2 inside a disk of `radius` m
+    centred at the receiver centre + centre_offset (width, height), 0 outside."""
+    ny, nx = rec.res_y, rec.res_x
+    # pixel centres in receiver-plane coordinates: column along the width, row along the height
+    xs = (np.arange(nx) + 0.5) / nx * rec.size[0] - rec.size[0] / 2
+    ys = (np.arange(ny) + 0.5) / ny * rec.size[1] - rec.size[1] / 2
+    X, Y = np.meshgrid(xs, ys)
+    inside = (X - centre_offset[0]) ** 2 + (Y - centre_offset[1]) ** 2 <= radius ** 2
+    return np.where(inside, level, 0.0).astype(np.float32)
+
+
 BUILDERS = {"small": small, "mid": mid, "large": large}

@@ -844,3 +844,170 @@ void orc_smooth_u32(const uint32_t* in, float* out, int w, int h, int radius, fl
     free(buf);
   }
 }
+
+/* ------------------------------------------------------------ adjoint */
+/* Heliostat frame for parameters th = (aim offset along ew, along eh, extra
+ * tilt about u0, about v0), following orc_scene_aim. */
+static void adj_frame(const orc_scene* s, int h, const double sun[3], const float* aim, const float* normal_in,
+                      const float* tilt0, const double ew[3], const double eh[3], const double th[4], double f[9]) {
+  double p[3] = {s->pos[3 * h], s->pos[3 * h + 1], s->pos[3 * h + 2]};
+  double n[3];
+  if (normal_in) {
+    n[0] = normal_in[3 * h]; n[1] = normal_in[3 * h + 1]; n[2] = normal_in[3 * h + 2];
+    normalize3(n);
+  } else {
+    double a[3], r[3];
+    for (int i = 0; i < 3; ++i) a[i] = (aim ? (double)aim[3 * h + i] : s->recv_focus[i]) + th[0] * ew[i] + th[1] * eh[i];
+    sub3(a, p, r);
+    normalize3(r);
+    sub3(r, sun, n);
+    normalize3(n);
+  }
+  double tx = (tilt0 ? (double)tilt0[2 * h] : 0.0) + th[2], tz = (tilt0 ? (double)tilt0[2 * h + 1] : 0.0) + th[3];
+  if (tilt0 || th[2] != 0.0 || th[3] != 0.0) {
+    double f0[9];
+    frame_of(n, 0, f0);
+    for (int i = 0; i < 3; ++i) n[i] = n[i] + tx * f0[i] + tz * f0[6 + i];
+    normalize3(n);
+  }
+  frame_of(n, 0, f);
+}
+
+/* origin, perturbed normal and reflected direction of a ray for frame f */
+static void adj_ray(const orc_scene* s, int h, const double f[9], const float xz[2], const double ws[3],
+                    const double tl[3], double o[3], double np[3], double r[3]) {
+  double lp[3] = {(double)xz[0], (double)s->size[3 * h + 1] / 2.0, (double)xz[1]};
+  apply_frame(f, lp, o);
+  o[0] += s->pos[3 * h]; o[1] += s->pos[3 * h + 1]; o[2] += s->pos[3 * h + 2];
+  apply_frame(f, tl, np);
+  normalize3(np);
+  double di = dot3(ws, np);
+  for (int i = 0; i < 3; ++i) r[i] = ws[i] - 2 * di * np[i];
+  normalize3(r);
+}
+
+/* receiver-plane coordinates (u along v1-v0, v along v3-v0), no bounds */
+static void adj_plane_uv(const orc_scene* s, const double o[3], const double d[3], double* u, double* v) {
+  double E1[3], E2[3], T[3], pv[3], qv[3];
+  sub3(s->recv_v + 3, s->recv_v, E1);
+  sub3(s->recv_v + 9, s->recv_v, E2);
+  cross3(d, E2, pv);
+  double inv = 1.0 / dot3(E1, pv);
+  sub3(o, s->recv_v, T);
+  *u = dot3(T, pv) * inv;
+  cross3(T, E1, qv);
+  *v = dot3(d, qv) * inv;
+}
+
+/* sum over the bilinear corners of map[c] * W_c (corners off the map add 0) */
+static double adj_bilinear(const orc_scene* s, double u, double v, const double* map, double* w4, int* c4) {
+  double px = v * s->res_x - 0.5, py = u * s->res_y - 0.5;
+  double i0 = floor(px), j0 = floor(py), fx = px - i0, fy = py - j0;
+  double w[4] = {(1 - fx) * (1 - fy), fx * (1 - fy), (1 - fx) * fy, fx * fy};
+  double acc = 0;
+  for (int k = 0; k < 4; ++k) {
+    int ci = (int)i0 + (k & 1), cj = (int)j0 + (k >> 1);
+    int ok = ci >= 0 && cj >= 0 && ci < s->res_x && cj < s->res_y;
+    if (w4) { w4[k] = w[k]; c4[k] = ok ? cj * s->res_x + ci : -1; }
+    if (ok && map) acc += map[cj * s->res_x + ci] * w[k];
+  }
+  return acc;
+}
+
+void orc_adjoint(const orc_scene* s, const orc_trace_cfg* c, const float* aim, const float* normal_in,
+                 const float* tilt0, const double ew[3], const double eh[3], const double* target, double scale,
+                 double fd_h, double* energy, double* loss, double* grad) {
+  double sd[3], sf[9];
+  sun_frame(c, sd, sf);
+  int nt = 1;
+#ifdef _OPENMP
+  nt = c->threads > 0 ? c->threads : omp_get_max_threads();
+#endif
+  int64_t res = (int64_t)s->res_x * s->res_y;
+  int64_t rays = c->ray_end > 0 ? c->ray_end : c->rays;
+  uint8_t* vis = (uint8_t*)calloc((size_t)rays, 1);
+  double* te = (double*)calloc((size_t)nt * res, sizeof(double));
+  /* forward: visibility with the scene's geometry, bilinear deposit */
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+#endif
+  for (int64_t ray = 0; ray < rays; ++ray) {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    int64_t m = ray / c->rays_per_point;
+    int h = c->point_helio[m];
+    double sl[3], tl[3], ws[3], dir[3], o[3], np[3], r[3];
+    orc_ray_samples(c, (double)s->sigma[h], (uint64_t)ray, sl, tl);
+    apply_frame(sf, sl, ws);
+    adj_ray(s, h, s->frame + 9 * h, c->point_xz + 2 * m, ws, tl, o, np, r);
+    dir[0] = -ws[0]; dir[1] = -ws[1]; dir[2] = -ws[2];
+    if (orc_dda_blocked(s, o, dir, h, 0, NULL)) continue;
+    if (orc_dda_blocked(s, o, r, h, 0, NULL)) continue;
+    double t, u, v;
+    if (!orc_ray_parallelogram(o, r, s->recv_v, s->recv_v + 3, s->recv_v + 9, &t, &u, &v)) continue;
+    vis[ray] = 1;
+    double e = fabs(dot3(sd, np)) * (c->helio_weight ? c->helio_weight[h] : 1.0);
+    double w4[4];
+    int c4[4];
+    adj_bilinear(s, u, v, NULL, w4, c4);
+    for (int k = 0; k < 4; ++k)
+      if (c4[k] >= 0) te[(int64_t)tid * res + c4[k]] += e * w4[k];
+  }
+  for (int64_t i = 0; i < res; ++i) {
+    double acc = 0;
+    for (int t = 0; t < nt; ++t) acc += te[(int64_t)t * res + i];
+    energy[i] = acc;
+  }
+  double L = 0;
+  double* G = (double*)malloc((size_t)res * sizeof(double));
+  for (int64_t i = 0; i < res; ++i) {
+    double d = scale * energy[i] - target[i];
+    L += d * d;
+    G[i] = 2.0 * d * scale;
+  }
+  *loss = L;
+  /* backward: per-ray central differences of sum_c G_c e W_c */
+  double* tg = (double*)calloc((size_t)nt * 4 * s->n, sizeof(double));
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+#endif
+  for (int64_t ray = 0; ray < rays; ++ray) {
+    if (!vis[ray]) continue;
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    int64_t m = ray / c->rays_per_point;
+    int h = c->point_helio[m];
+    double w = c->helio_weight ? c->helio_weight[h] : 1.0;
+    double sl[3], tl[3], ws[3];
+    orc_ray_samples(c, (double)s->sigma[h], (uint64_t)ray, sl, tl);
+    apply_frame(sf, sl, ws);
+    for (int k = 0; k < 4; ++k) {
+      double val[2];
+      /* tilts move the hit ~1000x more per unit than aim offsets: a smaller
+       * step keeps the difference away from the bilinear weights' kinks */
+      const double step = k < 2 ? fd_h : fd_h * 1e-3;
+      for (int sgn = 0; sgn < 2; ++sgn) {
+        double th[4] = {0, 0, 0, 0}, f[9], o[3], np[3], r[3], u, v;
+        th[k] = sgn ? -step : step;
+        adj_frame(s, h, sd, aim, normal_in, tilt0, ew, eh, th, f);
+        adj_ray(s, h, f, c->point_xz + 2 * m, ws, tl, o, np, r);
+        adj_plane_uv(s, o, r, &u, &v);
+        val[sgn] = fabs(dot3(sd, np)) * w * adj_bilinear(s, u, v, G, NULL, NULL);
+      }
+      tg[((int64_t)tid * s->n + h) * 4 + k] += (val[0] - val[1]) / (2.0 * step);
+    }
+  }
+  for (int64_t i = 0; i < 4 * (int64_t)s->n; ++i) {
+    double acc = 0;
+    for (int t = 0; t < nt; ++t) acc += tg[(int64_t)t * 4 * s->n + i];
+    grad[i] = acc;
+  }
+  free(tg);
+  free(G);
+  free(te);
+  free(vis);
+}

@@ -171,6 +171,19 @@ void orc_trace_tables(const orc_scene* s, const orc_trace_cfg* c, const float* s
 void orc_ray_samples(const orc_trace_cfg* c, double sigma, uint64_t ray, double sun_local[3],
                      double turb_local[3]);
 
+/* FP64 adjoint of the bilinear-deposition loss L = sum_p (scale*E_p - T_p)^2.
+ * Forward: visibility with the scene's current geometry, bilinear deposit of
+ * |sun . n'| * w at the receiver hit.  Gradient with respect to theta_h =
+ * (aim offset along ew, along eh, extra tilt about u, about v) of every
+ * heliostat: for each visible ray, central differences (step fd_h) of that
+ * ray's value sum_c G_c e W_c, where G = dL/dE, with its random numbers and
+ * visibility fixed -- the pathwise derivative, computed without the analytic
+ * chain.  aim / normal_in / tilt0 as in orc_scene_aim.  energy [res],
+ * grad [4n] (aim_w, aim_h, tilt_u, tilt_v per heliostat). */
+void orc_adjoint(const orc_scene* s, const orc_trace_cfg* c, const float* aim, const float* normal_in,
+                 const float* tilt0, const double ew[3], const double eh[3], const double* target, double scale,
+                 double fd_h, double* energy, double* loss, double* grad);
+
 /* Trimmed mean (trimmed_mean image_smooth.cu:10-58, heap.cuh:9-212).
  * method 0: sorted order statistics; 1: the reference's two-heap stream. */
 void orc_smooth_u32(const uint32_t* in, float* out, int w, int h, int radius, float ratio,

@@ -82,6 +82,8 @@ def lib():
         L.orc_trace_tables.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcTraceCfg), fp, fp, C.c_int64, i32p,
                                        C.c_int64, C.POINTER(OrcTraceOut)]
         L.orc_ray_samples.argtypes = [C.POINTER(OrcTraceCfg), C.c_double, C.c_uint64, dp, dp]
+        L.orc_adjoint.argtypes = [C.POINTER(OrcScene), C.POINTER(OrcTraceCfg), fp, fp, fp, dp, dp, dp, C.c_double,
+                                  C.c_double, dp, dp, dp]
         L.orc_smooth_u32.argtypes = [u32p, fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int]
         L.orc_smooth_f32.argtypes = [fp, fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int]
         _lib = L
@@ -256,6 +258,23 @@ class Scene:
                                st.shape[0], C.byref(o))
         r["stats"] = list(o.stats)
         return r
+
+    def adjoint(self, cfg, target, scale, fd_h=1e-7):
+        """FP64 loss, bilinear energy map and per-heliostat gradients [n, 4]
+        (aim along the receiver width, along its height, tilt u, tilt v)."""
+        rv = np.array(self.s.recv_v[:]).reshape(4, 3)
+        ew = rv[3] - rv[0]
+        eh = rv[1] - rv[0]
+        ew = np.ascontiguousarray(ew / np.linalg.norm(ew))
+        eh = np.ascontiguousarray(eh / np.linalg.norm(eh))
+        tgt = np.ascontiguousarray(target, np.float64).ravel()
+        energy = np.zeros(self.res[0] * self.res[1])
+        grad = np.zeros((self.s.n, 4))
+        loss = C.c_double()
+        lib().orc_adjoint(C.byref(self.s), C.byref(cfg), _p(self.aim, fp), _p(self.normal_in, fp), _p(self.tilt, fp),
+                          _p(ew, dp), _p(eh, dp), _p(tgt, dp), scale, fd_h, _p(energy, dp), C.byref(loss),
+                          _p(grad, dp))
+        return loss.value, energy.reshape(self.res), grad
 
     def dda(self, o, d, own, brute=False):
         ov = (C.c_double * 3)(*o)
