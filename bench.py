@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling runs; multiple of 256)")
     ap.add_argument("--variant", type=int, default=0, help="trace kernel variant (qmcrt_trace_params.kernel_variant)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-versus-sequential section")
+    ap.add_argument("--cell", type=float, default=0.0, help="override the grid cell size (m; the coarse cell of a two-level grid)")
+    ap.add_argument("--fine-div", type=int, default=-1, help="override the two-level grid split (1 = one level)")
     return ap.parse_args()
 
 
@@ -57,7 +59,9 @@ def dist_env():
 def oracle_sample(w, seconds, threads=0):
     """Time the FP64 oracle on ray ranges spread over the whole field."""
     from oracle import oracle as O
-    sc = O.Scene(w.pos, w.size, w.sigma, w.receiver, w.grid.cell[0], w.grid.margin, list(w.sun.dir), aim=w.aim)
+    # the oracle walks one uniform grid with the fine cell size
+    cell = w.grid.cell[0] / max(w.grid.fine_div, 1)
+    sc = O.Scene(w.pos, w.size, w.sigma, w.receiver, cell, w.grid.margin, list(w.sun.dir), aim=w.aim)
     rpp = w.params.rays_per_point
     total = int(w.params.rays)
     xz, helio = O.points_poisson(w.size, total // rpp, w.params.point_spacing, w.params.seed)
@@ -267,6 +271,12 @@ def workload_name(w):
             "large": "10000 heliostats 11x11 m to 1300 m, cylinder 8x18 m 512x256, 2^31 rays"}[w.name]
 
 
+def grid_name(g):
+    if g.fine_div > 1:
+        return "two-level: %g m coarse / %g m fine cells" % (g.cell[0], g.cell[0] / g.fine_div)
+    return "%g m cells" % g.cell[0]
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -299,6 +309,10 @@ def b200_arm(a, rank, world, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     w = W.BUILDERS[a.workload](rays=a.rays) if a.rays else W.BUILDERS[a.workload]()
+    if a.cell > 0:
+        w.grid.cell[:] = [a.cell] * 3
+    if a.fine_div >= 0:
+        w.grid.fine_div = a.fine_div
     sc = SolarScene.from_workload(w)
     p = w.params
     p.kernel_variant = a.variant
@@ -438,17 +452,21 @@ def b200_arm(a, rank, world, local):
             "hbm_peak_gbs_of_measured": peaks.get("hbm_gbs")}
     if traffic is not None:
         roof["hbm_achieved_gbs"] = traffic / kern_s / 1e9
+    per_step = {"aim": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "trace": 1, "finalize": 1, "smooth": 1}
+    if w.grid.fine_div > 1:
+        per_step["grid_coarse"] = 1
+    launches = sum(per_step.values())
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_name(w), "rays_per_step_per_gpu": rays, "heliostats": w.n,
                        "parallelism": "ray shards per GPU + NCCL all-reduce of maps" if world > 1 else "1 GPU",
                        "l2": "flushed between timed steps (256 MB write)",
+                       "grid": grid_name(w.grid),
                        "step": "aim + grid build + trace + flux scaling + trimmed-mean smoothing"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": 7 * a.steps,
-            "launches_per_step": {"aim": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "trace": 1,
-                                  "finalize": 1, "smooth": 1},
+            "gpu_launches": launches * a.steps,
+            "launches_per_step": per_step,
             "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
             "clocks": clocks,
             "batched": batch,

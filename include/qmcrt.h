@@ -57,8 +57,9 @@ enum {
   /* The ray's own heliostat is not excluded; only t > 1e-6 rejects the
    * self-hit (global_function.cuh:101-102). */
   QMCRT_QUIRK_SELF_HIT = 1u << 2,
-  /* Table mode: the perturbation of point m uses the start offset of point
-   * max(m-1, 0) (rectgrid_raytracing.cu:183-184). */
+  /* Table mode: the perturbation of a heliostat's point l uses the start
+   * offset of its point max(l-1, 0) (rectgrid_raytracing.cu:183-184; the
+   * reference launches map_tracing per heliostat, so l restarts at each one). */
   QMCRT_QUIRK_PREV_PERTURB = 1u << 3,
   /* local2world returns its input unchanged whenever the aligned normal is
    * parallel to y, also for -y (global_function.cuh:29-30). */
@@ -77,6 +78,14 @@ enum { QMCRT_POINTS_POISSON = 0, QMCRT_POINTS_GRID = 1 };
 
 /* Flux deposition: nearest pixel (reference) or bilinear (adjoint). */
 enum { QMCRT_DEPOSIT_NEAREST = 0, QMCRT_DEPOSIT_BILINEAR = 1 };
+
+/* Atmospheric attenuation eta(d) of a ray's energy over its slant range d (m)
+ * from the mirror to the receiver hit (eta_aAlpha, rectgrid_raytracing.cu:120-127). */
+enum {
+  QMCRT_ATTEN_NONE = 0,    /* eta = 1: what the reference computes */
+  QMCRT_ATTEN_POLY_EXP = 1 /* the formula the reference carries disabled: d <= 1000 m:
+                              0.99331 - 1.176e-4 d + 1.97e-8 d^2, else exp(-1.106e-4 d) */
+};
 
 /* Trimmed-mean definitions (image_smooth.cu:10-58). */
 enum {
@@ -120,14 +129,19 @@ typedef struct qmcrt_receiver {
 } qmcrt_receiver;
 
 /* Uniform grid over the field (RectGrid grid.h:25-48).  The bounds are taken
- * from the field (plus `margin`) unless `explicit_bounds` is set. */
+ * from the field (plus `margin`) unless `explicit_bounds` is set.
+ * Two-level grid (fine_div = 2, 4 or 8): `cell` is the coarse cell; the
+ * heliostats are registered in fine cells of cell / fine_div, and each coarse
+ * cell keeps the height range of its fine cells so that the traversal can
+ * step through a coarse cell without visiting its fine cells.  The grid
+ * reported by qmcrt_scene_grid_info is the fine one. */
 typedef struct qmcrt_grid_params {
-  float cell[3];         /* cell size in m (RectGrid::interval_) */
+  float cell[3];         /* cell size in m (RectGrid::interval_); the coarse cell when fine_div > 1 */
   float margin;          /* added around the field's bounding box, m */
   int32_t explicit_bounds;
   float origin[3];       /* used when explicit_bounds: RectGrid::pos_ */
   float extent[3];       /* used when explicit_bounds: RectGrid::size_ */
-  int32_t fine_div;      /* >1: two-level grid, each coarse cell split into fine_div^3 */
+  int32_t fine_div;      /* 0 or 1: one level; 2, 4 or 8: two-level grid, each coarse cell split into fine_div^3 */
 } qmcrt_grid_params;
 
 /* Sun (SunRay sunray.h:3-50). */
@@ -149,9 +163,12 @@ typedef struct qmcrt_trace_params {
   uint32_t quirks;         /* QMCRT_QUIRK_* */
   int32_t deposit;         /* QMCRT_DEPOSIT_* */
   int32_t accumulate;      /* 0: zero the output maps first; 1: add into them */
-  int32_t kernel_variant;  /* 0: default (fastest); 1: plain global-atomic deposition; 2: no smem staging */
+  int32_t kernel_variant;  /* 0 or 1: default (fastest); 2: no vertical culling (every cell on the path
+                              tested); 3: the production kernel without its 4-CTA register cap;
+                              4: a two-level grid walked on its fine level only */
   uint32_t item;           /* Philox stream (counter word 2): distinct items give independent ray sets
                               (shards of one trace, items of a batch) */
+  int32_t attenuation;     /* QMCRT_ATTEN_*: atmospheric transmittance of the mirror-to-receiver leg */
 } qmcrt_trace_params;
 
 /* Device outputs of a trace.  Any pointer may be NULL. */
@@ -192,11 +209,11 @@ typedef struct qmcrt_table_inputs {
   int32_t rays_per_point;
 } qmcrt_table_inputs;
 
-/* Grid summary. */
+/* Grid summary (of the fine grid when the grid has two levels). */
 typedef struct qmcrt_grid_info {
   float origin[3];
   float cell[3];
-  int32_t dims[3];
+  int32_t dims[3];    /* a multiple of fine_div on every axis */
   int64_t cells;
   int64_t entries; /* CSR entries (heliostat registrations) */
   int32_t fine_div;
@@ -257,6 +274,23 @@ qmcrt_status qmcrt_layout_radial_staggered(const qmcrt_layout_params* p, float* 
 qmcrt_status qmcrt_scn_parse(const char* path, qmcrt_receiver* recv_out,
                              qmcrt_grid_params* grid_out, float* h_pos, float* h_size,
                              int32_t capacity, int32_t* n_out);
+
+/* Result files, host buffers, the reference's text formats
+ * (ImageSaver::savetxt, image_save.cpp:5-48).  The map is [height][width] as
+ * the tracer writes it; both writers go from its last row to its first (the
+ * receiver's top edge first) and treat values below 1e-6 as zero.
+ * append != 0 appends, as the reference does (it opens with ios::app).
+ *
+ * Flux map (image_save.cpp:5-24): one line per row, every value followed by
+ * ','; zero as "0", others in fixed notation with `precision` decimals. */
+qmcrt_status qmcrt_write_flux_csv(const char* path, const float* h_map, int32_t width, int32_t height,
+                                  int32_t precision, int32_t append);
+
+/* Intercept ratio (image_save.cpp:26-48): the float sum of the map's values
+ * (in the file's order) divided by total_energy, written with 6 significant
+ * digits and a newline.  path may be NULL to get *ratio_out only. */
+qmcrt_status qmcrt_write_intercept_ratio(const char* path, const float* h_map, int32_t width, int32_t height,
+                                         float total_energy, int32_t append, float* ratio_out);
 
 /* -------------------------------------------------------------- scenes
  * A scene owns the device copy of the field, receiver and grid.  Replaces

@@ -24,6 +24,7 @@ QUIRKS_REFERENCE = 0x3F
 RECEIVER_FLAT, RECEIVER_CYLINDER = 0, 1
 POINTS_POISSON, POINTS_GRID = 0, 1
 DEPOSIT_NEAREST, DEPOSIT_BILINEAR = 0, 1
+ATTEN_NONE, ATTEN_POLY_EXP = 0, 1
 TRIM_SORTED, TRIM_HEAPS = 0, 1
 RAY_SHADOWED, RAY_BLOCKED, RAY_HIT, RAY_OFFMAP = 1, 2, 4, 8
 
@@ -56,7 +57,7 @@ class TraceParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("rays", C.c_uint64), ("rays_per_point", C.c_int32),
                 ("point_mode", C.c_int32), ("point_spacing", C.c_float), ("reflectivity", C.c_float),
                 ("quirks", C.c_uint32), ("deposit", C.c_int32), ("accumulate", C.c_int32),
-                ("kernel_variant", C.c_int32), ("item", C.c_uint32)]
+                ("kernel_variant", C.c_int32), ("item", C.c_uint32), ("attenuation", C.c_int32)]
 
 
 class Outputs(C.Structure):
@@ -121,6 +122,8 @@ PROTOTYPES = {
     "qmcrt_buie_table": (C.c_int, [C.c_float, fp, fp, fp, fp]),
     "qmcrt_layout_radial_staggered": (C.c_int, [C.POINTER(LayoutParams), fp, C.c_int32, i32p]),
     "qmcrt_scn_parse": (C.c_int, [C.c_char_p, C.POINTER(Receiver), C.POINTER(GridParams), fp, fp, C.c_int32, i32p]),
+    "qmcrt_write_flux_csv": (C.c_int, [C.c_char_p, fp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "qmcrt_write_intercept_ratio": (C.c_int, [C.c_char_p, fp, C.c_int32, C.c_int32, C.c_float, C.c_int32, fp]),
     "qmcrt_scene_create": (C.c_int, [C.POINTER(Field), C.POINTER(Receiver), C.POINTER(GridParams), C.POINTER(C.c_void_p)]),
     "qmcrt_scene_destroy": (C.c_int, [C.c_void_p]),
     "qmcrt_scene_set_field": (C.c_int, [C.c_void_p, C.POINTER(Field), C.c_void_p]),

@@ -367,6 +367,8 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "the adjoint needs Poisson points and 0 < rays < 2^32");
   if (p->quirks & ~QMCRT_QUIRK_ZENITH_FRAME)
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint traces in corrected mode");
+  if (p->attenuation != QMCRT_ATTEN_NONE)
+    return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint has no attenuation term");
   if (!(sun->csr > 0.f && sun->csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   cudaStream_t st = (cudaStream_t)stream;
   qmcrt_tape* t = new qmcrt_tape();

@@ -297,6 +297,8 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
   if (params->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS | QMCRT_QUIRK_SELF_HIT |
                         QMCRT_QUIRK_PIXEL_EDGE))
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "batches trace in corrected mode only");
+  if (params->attenuation != QMCRT_ATTEN_NONE && params->attenuation != QMCRT_ATTEN_POLY_EXP)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
   if (params->point_mode != QMCRT_POINTS_POISSON || params->rays_per_point <= 0 || params->rays == 0 ||
       params->rays > 0xFFFFFFFFull)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "batches need Poisson points and 0 < rays < 2^32");
@@ -361,6 +363,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     a.b_inv = 1 / (t.params[1] + 1);
     a.b_inv_bucket = t.inv_bucket;
     a.rays = (uint32_t)params->rays;
+    a.atten = params->attenuation;
     a.rpp = params->rays_per_point;
     a.rpp_shift = (a.rpp & (a.rpp - 1)) ? -1 : __builtin_ctz((unsigned)a.rpp);
     a.key = make_uint2((uint32_t)params->seed, (uint32_t)(params->seed >> 32));

@@ -419,4 +419,58 @@ qmcrt_status qmcrt_scn_parse(const char* path, qmcrt_receiver* recv_out, qmcrt_g
   return QMCRT_OK;
 }
 
+// ------------------------------------------------------------ result files
+// The map is [height][width], row 0 at the receiver's v0 edge; both writers
+// walk it from the last row to the first (the top of the receiver first), as
+// ImageSaver::savetxt does (image_save.cpp:10-22).  Values below 1e-6 count as
+// zero (Epsilon, global_constant.h:6).
+
+static qmcrt_status open_out(const char* path, int32_t append, FILE** f) {
+  *f = std::fopen(path, append ? "a" : "w");
+  if (!*f) return set_error(QMCRT_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_write_flux_csv(const char* path, const float* h_map, int32_t width, int32_t height,
+                                  int32_t precision, int32_t append) {
+  if (!path || !h_map || width <= 0 || height <= 0 || precision < 0 || precision > 30)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "bad flux file arguments");
+  FILE* f;
+  qmcrt_status e = open_out(path, append, &f);
+  if (e) return e;
+  for (int r = height - 1; r >= 0; --r) {
+    const float* row = h_map + (size_t)r * width;
+    for (int c = 0; c < width; ++c) {
+      if ((double)row[c] < 1e-6) std::fputs("0,", f);
+      else std::fprintf(f, "%.*f,", precision, (double)row[c]);
+    }
+    std::fputc('\n', f);
+  }
+  bool bad = std::ferror(f) != 0;
+  if (std::fclose(f) != 0 || bad) return set_error(QMCRT_ERR_INVALID_ARGUMENT, std::string("write failed: ") + path);
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_write_intercept_ratio(const char* path, const float* h_map, int32_t width, int32_t height,
+                                         float total_energy, int32_t append, float* ratio_out) {
+  if (!h_map || width <= 0 || height <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "bad intercept arguments");
+  // float accumulation in the file's order (image_save.cpp:29-45)
+  float in = 0.0f;
+  for (int r = height - 1; r >= 0; --r) {
+    const float* row = h_map + (size_t)r * width;
+    for (int c = 0; c < width; ++c)
+      if (!((double)row[c] < 1e-6)) in += row[c];
+  }
+  float ratio = in / total_energy;
+  if (ratio_out) *ratio_out = ratio;
+  if (!path) return QMCRT_OK;
+  FILE* f;
+  qmcrt_status e = open_out(path, append, &f);
+  if (e) return e;
+  std::fprintf(f, "%g\n", (double)ratio);  // ostream's default: 6 significant digits
+  bool bad = std::ferror(f) != 0;
+  if (std::fclose(f) != 0 || bad) return set_error(QMCRT_ERR_INVALID_ARGUMENT, std::string("write failed: ") + path);
+  return QMCRT_OK;
+}
+
 }  // extern "C"

@@ -57,6 +57,7 @@ struct SunGeom {
   int32_t* entries = nullptr;    // [entry_cap]
   float4* cell_rect = nullptr;   // [3*entry_cap]
   float2* cell_yr = nullptr;     // [cells]
+  float2* coarse_yr = nullptr;   // [coarse_cells] two-level grid only
   int* field_yr = nullptr;       // [2]
   double* power = nullptr;       // [1] sum |n . sun| * A
 };
@@ -97,6 +98,7 @@ struct qmcrt_scene {
   int gdims[3];
   int64_t cells = 0, entry_cap = 0;
   int fine_div = 1;
+  int64_t coarse_cells = 0;  // fine_div > 1: cells of the coarse level
 
   // device field
   float *d_pos = nullptr, *d_size = nullptr, *d_aim = nullptr, *d_normal_in = nullptr;
@@ -111,6 +113,7 @@ struct qmcrt_scene {
   int32_t* d_entries = nullptr;     // [entry_cap]
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
   float2* d_cell_yr = nullptr;      // [cells] height range of each cell's rectangles
+  float2* d_coarse_yr = nullptr;    // [coarse_cells] the same per coarse cell (two-level grid)
   int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)
   qm::SunKey sun_key;
 

@@ -220,6 +220,24 @@ __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t*
   }
 }
 
+// Height range of each coarse cell of a two-level grid: the union of the
+// ranges of its div^3 fine cells (empty cells contribute nothing).
+__global__ void coarse_finish_kernel(int64_t coarse_cells, int div, int3 cdims, int gy, int gz, const float2* cell_yr,
+                                     float2* coarse_yr) {
+  int64_t cc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= coarse_cells) return;
+  int cz = (int)(cc % cdims.z), cy = (int)((cc / cdims.z) % cdims.y), cx = (int)(cc / ((int64_t)cdims.z * cdims.y));
+  float ylo = 3.0e38f, yhi = -3.0e38f;
+  for (int x = cx * div; x < (cx + 1) * div; ++x)
+    for (int y = cy * div; y < (cy + 1) * div; ++y)
+      for (int z = cz * div; z < (cz + 1) * div; ++z) {
+        float2 r = cell_yr[((int64_t)x * gy + y) * gz + z];
+        ylo = fminf(ylo, r.x);
+        yhi = fmaxf(yhi, r.y);
+      }
+  coarse_yr[cc] = make_float2(ylo, yhi);
+}
+
 // ------------------------------------------------------------ points
 struct PoissonArgs {
   int n;
@@ -415,6 +433,7 @@ SunGeom scene_geom(qmcrt_scene* s) {
   g.entries = s->d_entries;
   g.cell_rect = s->d_cell_rect;
   g.cell_yr = s->d_cell_yr;
+  g.coarse_yr = s->d_coarse_yr;
   g.field_yr = s->d_field_yr;
   g.power = reinterpret_cast<double*>(s->d_stats + 8);
   return g;
@@ -437,6 +456,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
   GALLOC(g->entries, (size_t)s->entry_cap);
   GALLOC(g->cell_rect, 3 * (size_t)s->entry_cap);
   GALLOC(g->cell_yr, (size_t)s->cells);
+  if (s->coarse_cells) GALLOC(g->coarse_yr, (size_t)s->coarse_cells);
   GALLOC(g->field_yr, 2);
   GALLOC(g->power, 1);
 #undef GALLOC
@@ -446,7 +466,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
 void free_sun_geom(SunGeom* g) {
   dev_free(g->normal); dev_free(g->frame); dev_free(g->rect); dev_free(g->cellbox); dev_free(g->cell_count);
   dev_free(g->cell_start); dev_free(g->entries); dev_free(g->cell_rect); dev_free(g->cell_yr); dev_free(g->field_yr);
-  dev_free(g->power);
+  dev_free(g->coarse_yr); dev_free(g->power);
 }
 
 // Aim every heliostat for the sun (normalised) and rebuild the grid into g:
@@ -484,6 +504,12 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
                                                                         g.cell_rect, g.cell_yr, g.field_yr);
   QM_CUDA(cudaGetLastError());
+  if (s->coarse_cells) {
+    int3 cd = make_int3(s->gdims[0] / s->fine_div, s->gdims[1] / s->fine_div, s->gdims[2] / s->fine_div);
+    coarse_finish_kernel<<<(unsigned)((s->coarse_cells + 127) / 128), 128, 0, st>>>(
+        s->coarse_cells, s->fine_div, cd, s->gdims[1], s->gdims[2], g.cell_yr, g.coarse_yr);
+    QM_CUDA(cudaGetLastError());
+  }
   return QMCRT_OK;
 }
 
@@ -628,18 +654,28 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
       hi[i] = std::max(hi[i], field->pos[3 * h + i] + std::max(r, rq));
     }
   }
+  // two-level grid: the coarse dims cover the bounds, the fine grid (the one
+  // that holds the registrations) has fine_div cells per coarse cell per axis
+  const int div = grid->fine_div > 1 ? grid->fine_div : 1;
+  if (div != 1 && div != 2 && div != 4 && div != 8) {
+    delete s;
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "fine_div must be 0, 1, 2, 4 or 8");
+  }
   for (int i = 0; i < 3; ++i) {
-    s->gcell[i] = grid->cell[i];
+    int cd;
     if (grid->explicit_bounds) {
       s->gpos[i] = grid->origin[i];
-      s->gdims[i] = std::max(1, (int)std::ceil((double)grid->extent[i] / grid->cell[i]));
+      cd = std::max(1, (int)std::ceil((double)grid->extent[i] / grid->cell[i]));
     } else {
       float g = (float)(lo[i] - grid->margin);
       s->gpos[i] = g;
-      s->gdims[i] = std::max(1, (int)std::ceil(((hi[i] + grid->margin) - (double)g) / grid->cell[i]));
+      cd = std::max(1, (int)std::ceil(((hi[i] + grid->margin) - (double)g) / grid->cell[i]));
     }
+    s->gcell[i] = grid->cell[i] / (float)div;  // exact: div is a power of two
+    s->gdims[i] = cd * div;
   }
   s->cells = (int64_t)s->gdims[0] * s->gdims[1] * s->gdims[2];
+  s->coarse_cells = div > 1 ? s->cells / ((int64_t)div * div * div) : 0;
   if (s->cells > (int64_t)64 * 1024 * 1024) {
     delete s;
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid has more than 2^26 cells; use larger cells");
@@ -655,7 +691,7 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   }
   s->entry_cap = cap;
   if (cap > 0x7FFFFFFF) { delete s; return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid registrations exceed 2^31"); }
-  s->fine_div = grid->fine_div > 1 ? grid->fine_div : 1;
+  s->fine_div = div;
   size_t n = (size_t)s->n;
   size_t res = (size_t)recv->res_x * recv->res_y;
 #define ALLOC(p, c)              \
@@ -683,6 +719,7 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_entries, (size_t)cap);
   ALLOC(s->d_cell_rect, 3 * (size_t)cap);
   ALLOC(s->d_cell_yr, (size_t)s->cells);
+  if (s->coarse_cells) ALLOC(s->d_coarse_yr, (size_t)s->coarse_cells);
   ALLOC(s->d_field_yr, 2);
   ALLOC(s->d_helio_weight, n);
   ALLOC(s->d_flag, 1);
@@ -715,7 +752,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_pos); dev_free(s->d_size); dev_free(s->d_aim); dev_free(s->d_normal_in);
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
-  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_yr); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_yr); dev_free(s->d_coarse_yr); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

@@ -66,7 +66,7 @@ static int sm_count() {
   return g_sm_count;
 }
 
-template <bool TABLES, bool RECORDS, bool STATS, bool CULL, int MINB = 1>
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
 static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
   auto k = trace_kernel<TABLES, RECORDS, STATS, CULL, MINB>;
   int per_sm = 0;
@@ -80,16 +80,21 @@ static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
 }
 
 template <bool TABLES, bool RECORDS>
-static cudaError_t dispatch2(const TraceArgs& a, bool stats, bool cull, cudaStream_t st) {
-  if (stats) return cull ? launch_trace<TABLES, RECORDS, true, true>(a, st) : launch_trace<TABLES, RECORDS, true, false>(a, st);
-  return cull ? launch_trace<TABLES, RECORDS, false, true>(a, st) : launch_trace<TABLES, RECORDS, false, false>(a, st);
+static cudaError_t dispatch2(const TraceArgs& a, bool stats, int cull, cudaStream_t st) {
+  if (stats) {
+    if (cull == 2) return launch_trace<TABLES, RECORDS, true, 2>(a, st);
+    return cull ? launch_trace<TABLES, RECORDS, true, 1>(a, st) : launch_trace<TABLES, RECORDS, true, 0>(a, st);
+  }
+  if (cull == 2) return launch_trace<TABLES, RECORDS, false, 2>(a, st);
+  return cull ? launch_trace<TABLES, RECORDS, false, 1>(a, st) : launch_trace<TABLES, RECORDS, false, 0>(a, st);
 }
 
-static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool stats, bool cull, int variant,
+static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool stats, int cull, int variant,
                             cudaStream_t st) {
   // the production path (no records, no statistics) is compiled for 4 resident
   // CTAs per SM (64 registers); variant 3 keeps the unconstrained build
-  if (variant != 3 && !tables && !records && !stats && cull) return launch_trace<false, false, false, true, 4>(a, st);
+  if (variant != 3 && !tables && !records && !stats && cull == 2) return launch_trace<false, false, false, 2, 4>(a, st);
+  if (variant != 3 && !tables && !records && !stats && cull) return launch_trace<false, false, false, 1, 4>(a, st);
   if (tables) return records ? dispatch2<true, true>(a, stats, cull, st) : dispatch2<true, false>(a, stats, cull, st);
   return records ? dispatch2<false, true>(a, stats, cull, st) : dispatch2<false, false>(a, stats, cull, st);
 }
@@ -179,6 +184,13 @@ void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, u
     a->ginv[i] = 1.0f / s->gcell[i];
     a->gdims[i] = s->gdims[i];
   }
+  a->coarse_yr = s->fine_div > 1 ? geo.coarse_yr : nullptr;
+  a->cshift = 0;
+  while ((1 << a->cshift) < s->fine_div) ++a->cshift;
+  for (int i = 0; i < 3; ++i) {
+    a->cdims[i] = s->gdims[i] >> a->cshift;
+    a->ccell[i] = s->gcell[i] * (float)s->fine_div;
+  }
   a->rtype = s->rg.type;
   for (int i = 0; i < 3; ++i) {
     a->rA[i] = s->rg.v0[i];
@@ -209,6 +221,9 @@ static qmcrt_status check_params(const qmcrt_trace_params* p) {
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "reflectivity must be in [0,1]");
   if (p->quirks & ~QMCRT_QUIRKS_REFERENCE) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown quirk bits");
   if (p->deposit != QMCRT_DEPOSIT_NEAREST) return set_error(QMCRT_ERR_NOT_SUPPORTED, "bilinear deposition is only used by the adjoint");
+  if (p->kernel_variant < 0 || p->kernel_variant > 4) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "kernel_variant must be 0..4");
+  if (p->attenuation != QMCRT_ATTEN_NONE && p->attenuation != QMCRT_ATTEN_POLY_EXP)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
   return QMCRT_OK;
 }
 
@@ -228,7 +243,9 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
   QM_CUDA(cudaEventRecord(s->ev[2], st));
   // vertical culling needs every rectangle registered in every cell it
   // touches and the origin cell tested: off under the two grid quirks
-  bool cull = p->kernel_variant != 2 && !(p->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS));
+  // (level 2 adds the coarse level of a two-level grid)
+  int cull = p->kernel_variant != 2 && !(p->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS));
+  if (cull && a.coarse_yr && p->kernel_variant != 4) cull = 2;
   QM_CUDA(dispatch(a, tables, records, stats != nullptr, cull, p->kernel_variant, st));
   QM_CUDA(cudaEventRecord(s->ev[3], st));
   double scale = (double)sun->dni * p->reflectivity * weight_scale / ((double)p->rays_per_point * s->rg.pixel_area);
@@ -288,6 +305,7 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   if ((e = ensure_points(s, p, st))) return e;
   TraceArgs a{};
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
+  a.atten = p->attenuation;
   a.rays = (uint32_t)(s->points * (int64_t)p->rays_per_point);
   a.rpp = p->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);
@@ -314,6 +332,7 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcr
   if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
   TraceArgs a{};
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
+  a.atten = p->attenuation;
   a.rays = (uint32_t)(t->points * t->rays_per_point);
   a.rpp = t->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);

@@ -30,6 +30,12 @@ struct TraceArgs {
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
   int gdims[3];
+  // two-level grid: each coarse cell covers 2^cshift fine cells per axis;
+  // coarse_yr is the union of its fine cells' height ranges (NULL: one level)
+  const float2* coarse_yr;
+  int cshift;
+  int cdims[3];
+  float ccell[3];
   // receiver
   int rtype;
   double rA[3], rE1[3], rE2[3];
@@ -56,7 +62,16 @@ struct TraceArgs {
   uint8_t* flags;
   int32_t* pixel;
   unsigned long long* stats;
+  int atten;  // QMCRT_ATTEN_*
 };
+
+// Atmospheric transmittance over the slant range d (m) from the mirror to the
+// receiver: the formula eta_aAlpha carries, disabled, at
+// rectgrid_raytracing.cu:120-127 (the reference returns 1).
+__device__ __forceinline__ float atten_eta(int mode, float d) {
+  if (mode != QMCRT_ATTEN_POLY_EXP) return 1.f;
+  return d <= 1000.f ? 0.99331f - 0.0001176f * d + 1.97e-8f * d * d : expf(-0.0001106f * d);
+}
 
 // max_less_index (scene_instance_process.cu:98-113) over the table in smem:
 // the largest i with cdf_y[i] <= value.
@@ -147,7 +162,12 @@ __device__ __forceinline__ float from_ordered(int i) { return __int_as_float(i >
 // registered in every cell it touches, a real hit is always found in the cell
 // holding the hit point, whose height range contains that point, so the
 // answer is unchanged.
-template <bool STATS, bool CULL>
+// TWO (with CULL, two-level grid): the same test one level up — a coarse cell
+// whose height range (the union of its fine cells') misses the ray's height
+// over the coarse cell is stepped through without touching any fine cell.
+// The fine walk itself is unchanged, so the set of cells that can hold a hit,
+// and therefore the answer, is the single-level one.
+template <bool STATS, bool CULL, bool TWO = false>
 __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, float fy0, float fy1, uint32_t& ntest,
                             uint32_t& ncell) {
   const bool selfhit = a.quirks & QMCRT_QUIRK_SELF_HIT;
@@ -176,26 +196,47 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
     float mg = 0.01f + 1e-5f * t1;
     return !(fmaxf(ya, yb) + mg < yr.x || fminf(ya, yb) - mg > yr.y);
   };
+  // whether the current coarse cell is stepped through, evaluated when the
+  // walk enters a coarse cell; its exit along each axis is that axis' next
+  // fine crossing plus the fine cells left in the coarse cell
+  bool cskip = false;
+  const int cm = TWO ? (1 << a.cshift) - 1 : 0;
+  auto coarse_eval = [&](float t0) {
+    const int cs = a.cshift;
+    int cc = ((ix >> cs) * a.cdims[1] + (iy >> cs)) * a.cdims[2] + (iz >> cs);
+    float ex = tx + dx * (float)(sx > 0 ? cm - (ix & cm) : (ix & cm));
+    float ey = ty + dy * (float)(sy > 0 ? cm - (iy & cm) : (iy & cm));
+    float ez = tz + dz * (float)(sz > 0 ? cm - (iz & cm) : (iz & cm));
+    float t1 = fminf(ex, fminf(ey, ez));
+    float2 yr = __ldg(a.coarse_yr + cc);
+    float ya = o.y + t0 * d.y, yb = o.y + t1 * d.y;
+    float mg = 0.05f + 1e-4f * t1;
+    cskip = fmaxf(ya, yb) + mg < yr.x || fminf(ya, yb) - mg > yr.y;
+  };
+  if (TWO) coarse_eval(0.f);
   if (!(a.quirks & QMCRT_QUIRK_SKIP_ORIGIN_CELL)) {
     int c = (ix * gy + iy) * gz + iz;
-    if (may_hit(c, 0.f, fminf(tx, fminf(ty, tz)))) {
+    if ((!TWO || !cskip) && may_hit(c, 0.f, fminf(tx, fminf(ty, tz)))) {
       if (STATS) ++ncell;
       if (cell_hit<STATS>(a, c, o, d, own, selfhit, ntest)) return true;
     }
   }
   for (int guard = gx + gy + gz + 2; guard > 0; --guard) {
     float tin;
+    bool cross = false;  // the step entered a new coarse cell
     if (tx < ty) {
       if (tx < tz) {
         ix += sx;
         if (ix >= gx || ix < 0) return false;
         tin = tx;
         tx += dx;
+        if (TWO) cross = (ix & cm) == (sx > 0 ? 0 : cm);
       } else {
         iz += sz;
         if (iz >= gz || iz < 0) return false;
         tin = tz;
         tz += dz;
+        if (TWO) cross = (iz & cm) == (sz > 0 ? 0 : cm);
       }
     } else {
       if (ty < tz) {
@@ -203,16 +244,22 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
         if (iy >= gy || iy < 0) return false;
         tin = ty;
         ty += dy;
+        if (TWO) cross = (iy & cm) == (sy > 0 ? 0 : cm);
       } else {
         iz += sz;
         if (iz >= gz || iz < 0) return false;
         tin = tz;
         tz += dz;
+        if (TWO) cross = (iz & cm) == (sz > 0 ? 0 : cm);
       }
     }
     if (CULL) {
       float y = o.y + tin * d.y, mg = 0.01f + 1e-5f * tin;
       if ((d.y > 0.f && y - mg > fy1) || (d.y < 0.f && y + mg < fy0)) return false;  // left the mirror layer
+    }
+    if (TWO) {
+      if (cross) coarse_eval(tin);
+      if (cskip) continue;
     }
     int c = (ix * gy + iy) * gz + iz;
     if (!may_hit(c, tin, fminf(tx, fminf(ty, tz)))) continue;
@@ -224,7 +271,7 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
 
 // Receiver intersection in FP64; returns true on a hit and the pixel index
 // (-1 when the hit falls outside the map, QMCRT_QUIRK_PIXEL_EDGE only).
-__device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int& pix) {
+__device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int& pix, double* t_out = nullptr) {
   double u, v;
   if (a.rtype == QMCRT_RECEIVER_CYLINDER) {
     double ox = o.x - a.cyl[0], oz = o.z - a.cyl[2], R = a.cyl[3], H = a.cyl[4];
@@ -243,6 +290,7 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
     }
     double phi = atan2(oz + t * d.z, ox + t * d.x);
     if (phi < 0) phi += 2.0 * 3.141592653589793;
+    if (t_out) *t_out = t;
     u = y / H;
     v = phi / (2.0 * 3.141592653589793);
   } else {
@@ -257,7 +305,9 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
     d3 qv = cross(T, E1);
     v = dot(d, qv) * inv;
     if (v < 0 || v > 1) return false;
-    if (dot(E2, qv) * inv < 1e-6) return false;
+    double t = dot(E2, qv) * inv;
+    if (t < 1e-6) return false;
+    if (t_out) *t_out = t;
   }
   int row = (int)(u * a.res_y), col = (int)(v * a.res_x);  // rectgrid_raytracing.cu:144
   if (a.quirks & QMCRT_QUIRK_PIXEL_EDGE) {
@@ -352,7 +402,8 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float* s_tab
   if (TABLES) {
     // (start + j) mod T, kept in [0, T) for any caller-provided start
     int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
-    int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) ? (g > 0 ? g - 1 : 0) : g;
+    // the reference's index restarts at each heliostat's launch
+    int64_t gp = (a.quirks & QMCRT_QUIRK_PREV_PERTURB) && g > 0 && __ldg(a.point_helio + g - 1) == R.h ? g - 1 : g;
     int64_t ib = (((int64_t)__ldg(a.start + gp) + j) % a.T + a.T) % a.T;
     R.sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
     R.tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
@@ -368,7 +419,9 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float* s_tab
 }
 
 // One ray: the body of map_tracing (rectgrid_raytracing.cu:164-195).
-template <bool TABLES, bool RECORDS, bool STATS, bool CULL, class Dep>
+// CULL: 0 no culling, 1 vertical culling, 2 vertical culling on both levels
+// of a two-level grid.
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep>
 __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit) {
   RaySetup R;
@@ -387,21 +440,24 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab
   const float3 of = to_f(o);
   uint8_t flag = 0;
   int pix = -1;
-  if (dda_blocked<STATS, CULL>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, c.test, c.cell)) {
+  double th = 0.0;
+  if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, c.test, c.cell)) {
     flag = QMCRT_RAY_SHADOWED;
   } else {
     d3 np = rnorm(apply(fr, (double)tl.x, (double)tl.y, (double)tl.z));
     double di = dot(ws, np);
     d3 rd = rnorm(ws - (2.0 * di) * np);  // reflect (i - 2 n (n.i)), normalise
-    if (dda_blocked<STATS, CULL>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
+    if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
       flag = QMCRT_RAY_BLOCKED;
-    } else if (receiver_hit(a, o, rd, pix)) {
+    } else if (receiver_hit(a, o, rd, pix, &th)) {
       flag = QMCRT_RAY_HIT;
       if (pix < 0) {
         flag |= QMCRT_RAY_OFFMAP;
       } else {
-        // calEnergy (rectgrid_raytracing.cu:129-133), eta = 1
-        deposit(pix, (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w);
+        // calEnergy (rectgrid_raytracing.cu:129-133) times eta(t) (:147)
+        float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w;
+        if (a.atten) e *= atten_eta(a.atten, (float)th);
+        deposit(pix, e);
       }
     }
   }
@@ -430,7 +486,7 @@ __device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned lo
 }
 
 // The plain tracer: one grid-stride pass over the rays of one trace.
-template <bool TABLES, bool RECORDS, bool STATS, bool CULL, int MINB = 1>
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
   __shared__ float s_tab[1025 + 1025 + 1024];
   __shared__ int s_guide[kBuieBuckets];

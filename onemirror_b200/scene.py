@@ -260,6 +260,35 @@ class Batch:
         return counts, flux, st
 
 
+def write_flux_csv(path, flux, precision=2, append=True):
+    """Flux map [res_y, res_x] (host array or tensor) as the reference's text
+    file (ImageSaver::savetxt, image_save.cpp:5-24)."""
+    m = _host_map(flux)
+    capi.check(capi.lib().qmcrt_write_flux_csv(str(path).encode(), capi.as_fp(m), m.shape[1], m.shape[0],
+                                               precision, 1 if append else 0))
+
+
+def write_intercept_ratio(path, flux, total_energy, append=True):
+    """Sum of the flux map over total_energy, written as the reference's
+    intercept-ratio line (image_save.cpp:26-48); returns the ratio.  path=None
+    writes nothing."""
+    m = _host_map(flux)
+    r = C.c_float()
+    capi.check(capi.lib().qmcrt_write_intercept_ratio(None if path is None else str(path).encode(), capi.as_fp(m),
+                                                      m.shape[1], m.shape[0], C.c_float(total_energy),
+                                                      1 if append else 0, C.byref(r)))
+    return r.value
+
+
+def _host_map(flux):
+    if isinstance(flux, torch.Tensor):
+        flux = flux.detach().cpu().numpy()
+    m = np.ascontiguousarray(flux, np.float32)
+    if m.ndim != 2:
+        raise ValueError("map must be 2-D [rows, cols]")
+    return m
+
+
 def image_smooth(d_map, radius, ratio, method=capi.TRIM_SORTED):
     """Trimmed-mean smoothing of a device map (uint32/int32 counts or float32)."""
     assert d_map.is_cuda and d_map.is_contiguous() and d_map.dim() == 2

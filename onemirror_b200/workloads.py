@@ -11,7 +11,8 @@ radial-staggered layout generator from a fixed seed.  Sizes:
          slope 2.5 mrad, 2^28 rays, 25 m cells.
   large  10000 heliostats 11x11 m surround field out to 1300 m, tower 200 m,
          cylinder R 8 m x H 18 m unrolled to 512x256, sun 20 deg, CSR 0.2,
-         slope 3 mrad, 2^31 rays, 12.5 m cells.
+         slope 3 mrad, 2^31 rays, two-level grid of 50 m coarse / 12.5 m
+         fine cells.
 """
 import ctypes as C
 from dataclasses import dataclass, field as dfield
@@ -113,12 +114,14 @@ def cylinder_receiver(tower, radius, height, res_x, res_y):
     return r
 
 
-def grid(cell, margin=1.0):
+def grid(cell, margin=1.0, fine_div=1):
+    """Grid of `cell` m cells; fine_div > 1 makes `cell` the coarse cell of a
+    two-level grid whose fine cells are cell / fine_div."""
     g = capi.GridParams()
     g.cell[:] = [cell, cell, cell]
     g.margin = margin
     g.explicit_bounds = 0
-    g.fine_div = 1
+    g.fine_div = fine_div
     return g
 
 
@@ -171,7 +174,7 @@ def large(rays=1 << 31, seed=7):
     pos = layout(n, 11.0, 11.0, 120.0, 1300.0, az_center=0.0, az_span=360.0, mount=6.5)
     size = np.tile(np.array([[11.0, 0.1, 11.0]], np.float32), (n, 1))
     rec = cylinder_receiver(200.0, 8.0, 18.0, 512, 256)
-    return Workload("large", pos, size, 0.003, rec, grid(12.5), make_sun(20.0, 180.0, 1000.0, 0.2),
+    return Workload("large", pos, size, 0.003, rec, grid(50.0, fine_div=4), make_sun(20.0, 180.0, 1000.0, 0.2),
                     params(rays, 256, 0.22, seed))
 
 

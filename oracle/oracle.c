@@ -478,6 +478,13 @@ int orc_receiver_hit(const orc_scene* s, const double o[3], const double d[3], u
   return 1;
 }
 
+/* atmospheric transmittance over the slant range d (m): eta_aAlpha's
+ * formula, commented out in the reference (rectgrid_raytracing.cu:120-127) */
+static double orc_eta(int mode, double d) {
+  if (mode != 1) return 1.0;
+  return d <= 1000.0 ? 0.99331 - 0.0001176 * d + 1.97e-8 * d * d : exp(-0.0001106 * d);
+}
+
 static inline void angle2xyz(double theta, double phi, double o[3]) {
   /* global_function.cuh:175-180 */
   o[0] = sin(theta) * cos(phi);
@@ -529,7 +536,7 @@ static void trace_one(const orc_scene* s, const orc_trace_cfg* c, const double s
   *flag = ORC_RAY_HIT;
   if (p < 0) { *flag |= ORC_RAY_OFFMAP; return; }
   *pix = p;
-  *e_out = fabs(dot3(sun_dir, np)) * weight; /* calEnergy rectgrid_raytracing.cu:129-133 */
+  *e_out = fabs(dot3(sun_dir, np)) * weight * orc_eta(c->atten, t); /* calEnergy rectgrid_raytracing.cu:129-133, eta :147 */
   (void)uv_out;
 }
 
@@ -584,7 +591,11 @@ static void trace_driver(const orc_scene* s, const orc_trace_cfg* c, const float
     double sl[3], tl[3], w;
     if (sun_local) {
       int64_t a = (start[m] + j) % T;
-      int64_t mp = (c->quirks & ORC_QUIRK_PREV_PERTURB) ? (m - 1 > 0 ? m - 1 : 0) : m;
+      /* rectgrid_raytracing.cu:183 in per-heliostat launches
+       * (recthelio_tracing.cpp:46-80): the local index restarts at each
+       * heliostat, so its points 0 and 1 both use point 0's offset */
+      int64_t mp = m;
+      if ((c->quirks & ORC_QUIRK_PREV_PERTURB) && m > 0 && c->point_helio[m - 1] == c->point_helio[m]) mp = m - 1;
       int64_t b = (start[mp] + j) % T;
       for (int i = 0; i < 3; ++i) { sl[i] = sun_local[3 * a + i]; tl[i] = turb_local[3 * b + i]; }
       w = 1.0;

@@ -147,6 +147,7 @@ typedef struct orc_trace_cfg {
   int threads;            /* OpenMP threads (0 = all) */
   int64_t ray_begin, ray_end; /* sub-range to trace (end=0: all) */
   int deposit;            /* 0 nearest, 1 bilinear */
+  int atten;              /* 0: eta = 1; 1: eta(d) of rectgrid_raytracing.cu:120-127 (disabled there) */
 } orc_trace_cfg;
 
 typedef struct orc_trace_out {

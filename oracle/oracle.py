@@ -33,7 +33,7 @@ class OrcTraceCfg(C.Structure):
                 ("cdf_y", fp), ("slope", fp), ("bparams", fp), ("seed", C.c_uint64), ("item", C.c_uint32),
                 ("rays", C.c_int64), ("rays_per_point", C.c_int), ("point_xz", fp), ("point_helio", i32p),
                 ("helio_weight", dp), ("quirks", C.c_uint32), ("threads", C.c_int), ("ray_begin", C.c_int64),
-                ("ray_end", C.c_int64), ("deposit", C.c_int)]
+                ("ray_end", C.c_int64), ("deposit", C.c_int), ("atten", C.c_int)]
 
 
 class OrcTraceOut(C.Structure):
@@ -205,7 +205,7 @@ class Scene:
         self.res = (receiver.res_y, receiver.res_x)
 
     def cfg(self, csr, seed, rays, rpp, point_xz, point_helio, weight=None, threads=0, ray_begin=0, ray_end=0,
-            quirks=None, dni=1000.0, rho=0.88, item=0):
+            quirks=None, dni=1000.0, rho=0.88, item=0, atten=0):
         c = OrcTraceCfg()
         c.sun_dir[:] = self.sun_dir
         c.dni, c.rho = dni, rho
@@ -225,6 +225,7 @@ class Scene:
         c.threads = threads
         c.ray_begin, c.ray_end = ray_begin, ray_end
         c.deposit = 0
+        c.atten = atten
         return c
 
     def _out(self, nrec, records, maps):

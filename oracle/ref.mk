@@ -21,7 +21,7 @@ FLAGS := -O2 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -Xcompiler
 SRCS_CU := scene_instance_process.cu random_generator.cu steps_for_raytracing.cu poisson_disk.cu \
            compact_sample.cu rectgrid_raytracing.cu ray_tracing.cu image_smooth.cu
 SRCS_CPP := scene_instance_process.cpp random_generator.cpp common_var.cpp heliostat.cpp grid.cpp receiver.cpp \
-            recthelio_tracing.cpp
+            recthelio_tracing.cpp image_save.cpp
 OBJS := $(addprefix $(OUT)/obj/,$(SRCS_CU:.cu=.cu.o) $(SRCS_CPP:.cpp=.cpp.o))
 SHIMS := device_ptr copy host_vector device_vector
 

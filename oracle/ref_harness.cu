@@ -6,7 +6,8 @@
 // angle2xyz, rotateY (global_function.cuh), the Buie table builder
 // samplelights::parameters_generate and max_less_index
 // (scene_instance_process.cu), the Max_heap/Min_heap classes (heap.cuh) and
-// RectangleHelio::CRotate (heliostat.cpp).
+// RectangleHelio::CRotate (heliostat.cpp), and the result writers
+// ImageSaver::savetxt (image_save.cpp).
 // Device pieces (need a GPU): RectGrid::CGridHelioMatch (grid.cpp),
 // ImageSmoother::image_smooth (image_smooth.cu), and the tracing kernel
 // map_tracing through ray_tracing (ray_tracing.cu) with caller-given tables.
@@ -19,6 +20,7 @@
 #include "grid.h"
 #include "heap.cuh"
 #include "heliostat.cuh"
+#include "image_save.h"
 #include "image_smooth.cuh"
 #include "random_generator.h"
 #include "ray_tracing.h"
@@ -293,6 +295,15 @@ int ref_receiver_vertices(const float* rpos, const float* rsize, const float* rn
   res_out[1] = r.resolution_.y;
   r.CClear();
   return 0;
+}
+
+// The two text writers of image_save.cpp (flux map, intercept ratio); both
+// append to `path`.
+void ref_save_flux_txt(const char* path, int w, int h, float* data, int precision) {
+  ImageSaver::savetxt(std::string(path), w, h, data, precision);
+}
+void ref_save_ratio_txt(const char* path, int w, int h, float* data, float total_energy) {
+  ImageSaver::savetxt(std::string(path), w, h, data, total_energy);
 }
 
 }  // extern "C"

@@ -127,6 +127,28 @@ def main():
         L.ref_helio_vertices(P(hp[i]), P(hs[i]), None, P(focus), P(sun), P(v_aimed[i]), P(n_aimed[i]))
     out.update(helio_pos=hp, helio_size=hs, helio_normal_in=hn, helio_v_given=v_given, helio_n_given=n_given,
                helio_focus=focus, helio_sun=sun, helio_v_aimed=v_aimed, helio_n_aimed=n_aimed)
+
+    # ImageSaver::savetxt (image_save.cpp:5-48): the flux file at two
+    # precisions and the intercept-ratio file, each appended twice to a fresh
+    # file (the reference opens with ios::app)
+    import tempfile
+    fmap = rng.uniform(0, 9e5, (9, 13)).astype(np.float32)
+    fmap[rng.random((9, 13)) < 0.3] = 0
+    fmap[0, :4] = [1e-7, 9.9e-7, 1e-6, 1.00001e-6]
+    fmap[1, :3] = [-3.5, 0.125, 2.5]
+    fmap[2, :3] = [123456.789, 0.004999, 0.005]
+    L.ref_save_flux_txt.argtypes = [C.c_char_p, C.c_int, C.c_int, fp, C.c_int]
+    L.ref_save_ratio_txt.argtypes = [C.c_char_p, C.c_int, C.c_int, fp, C.c_float]
+    total = float(np.float32(fmap[fmap >= 1e-6].astype(np.float64).sum() * 1.37))
+    with tempfile.TemporaryDirectory() as td:
+        for key, call in (("save_flux_p2", lambda p: L.ref_save_flux_txt(p, 13, 9, P(fmap), 2)),
+                          ("save_flux_p4", lambda p: L.ref_save_flux_txt(p, 13, 9, P(fmap), 4)),
+                          ("save_ratio", lambda p: L.ref_save_ratio_txt(p, 13, 9, P(fmap), C.c_float(total)))):
+            path = os.path.join(td, key + ".txt")
+            call(path.encode())
+            call(path.encode())
+            out[key] = np.frombuffer(open(path, "rb").read(), np.uint8)
+    out.update(save_map=fmap, save_total=np.float32(total))
     np.savez_compressed(os.path.join(HERE, "ref_host_vectors.npz"), **out)
     print("wrote", len(out), "arrays")
 

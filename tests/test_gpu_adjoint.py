@@ -127,3 +127,9 @@ def test_adjoint_argument_errors(case):
     p.deposit = capi.DEPOSIT_NEAREST
     with pytest.raises(capi.QmcrtError):
         sc.adjoint_forward(w.sun, p, target)
+    p = W.params(RAYS, 256, 0.5)
+    p.deposit = capi.DEPOSIT_BILINEAR
+    p.attenuation = capi.ATTEN_POLY_EXP
+    with pytest.raises(capi.QmcrtError) as e:
+        sc.adjoint_forward(w.sun, p, target)
+    assert e.value.status == capi.ERR_NOT_SUPPORTED

@@ -146,7 +146,7 @@ def run_pair(w, sc, sun, params, quirks=0):
     xz, helio = sc.read_points()
     weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
     cfg = ref.cfg(sun.csr, params.seed, int(params.rays), params.rays_per_point, xz, helio, weight, quirks=quirks,
-                  item=params.item)
+                  item=params.item, atten=params.attenuation)
     o = ref.trace_philox(cfg)
     return g, o
 
@@ -282,6 +282,107 @@ def test_big_fields_on_ray_ranges(name):
     sc.close()
 
 
+def test_two_level_grid_equals_its_fine_level():
+    """Large field on its 50 m / 12.5 m two-level grid: the coarse level only
+    steps through coarse cells whose heights the ray cannot meet, so flags,
+    pixels, maps and even the counts of tested cells and rectangles equal a
+    walk of the fine level alone (kernel_variant 4); the fine grid is the one
+    a single-level 12.5 m scene builds."""
+    w = W.large(rays=1 << 22)
+    sc = SolarScene.from_workload(w)
+    gi = sc.grid_info()
+    assert gi.fine_div == 4 and list(gi.cell) == [12.5, 12.5, 12.5]
+    assert all(d % 4 == 0 for d in gi.dims)
+    g2 = sc.trace(w.sun, w.params, records=True)
+    f2, p2, c2 = g2["flags"].clone(), g2["pixel"].clone(), g2["counts"].clone()
+    w.params.kernel_variant = 4
+    g1 = sc.trace(w.sun, w.params, records=True)
+    assert torch.equal(f2, g1["flags"]) and torch.equal(p2, g1["pixel"]) and torch.equal(c2, g1["counts"])
+    s1, s2 = g1["stats"], g2["stats"]
+    assert (s1.rect_tests, s1.dda_cells) == (s2.rect_tests, s2.dda_cells)
+    # production kernels (no records, no statistics; separately compiled, so
+    # the compiler's FMA contraction may differ and a ray on a rectangle edge
+    # may flip): the same maps up to a few such rays
+    w.params.kernel_variant = 0
+    m2 = sc.trace(w.sun, w.params, stats=False)["counts"].clone()
+    w.params.kernel_variant = 4
+    m1 = sc.trace(w.sun, w.params, stats=False)["counts"]
+    edge = 2 * max(1, int(1e-5 * c2.sum().item()))
+    assert (m2 - c2).abs().sum().item() <= edge and (m1 - c2).abs().sum().item() <= edge
+    # a single-level scene with the fine cell size builds the same grid
+    w1 = W.large(rays=1 << 22)
+    w1.grid = W.grid(12.5)
+    sc1 = SolarScene.from_workload(w1)
+    gi1 = sc1.grid_info()
+    if list(gi1.dims) == list(gi.dims):
+        a, b = sc.read_grid(), sc1.read_grid()
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    sc1.close()
+    sc.close()
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_attenuation_equals_oracle(name):
+    """eta(d) of the mirror-to-receiver leg (QMCRT_ATTEN_POLY_EXP): records and
+    maps against the oracle; the large field's slant ranges pass 1000 m, so
+    both branches of the formula run.  Attenuation scales energies only: the
+    count map is the plain trace's."""
+    w = W.small() if name == "small" else W.large(rays=1 << 22)
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    p.attenuation = capi.ATTEN_POLY_EXP
+    g, o = run_pair(w, sc, w.sun, p)
+    check_pair(w, g, o)
+    p.attenuation = capi.ATTEN_NONE
+    g0 = sc.trace(w.sun, p, records=True)
+    assert torch.equal(g0["counts"], g["counts"])
+    r = (g["energy"].double().sum() / g0["energy"].double().sum()).item()
+    assert (0.9 if name == "small" else 0.8) < r < 0.99, r
+    sc.close()
+
+
+def test_smoothing_heaps_bit_exact_with_reference_gpu_kernel():
+    """QMCRT_TRIM_HEAPS against ImageSmoother::image_smooth's output on a B200."""
+    from test_oracle_pins import GV
+    for k in range(len(GV["smooth_params"])):
+        r, ratio = GV["smooth_params"][k]
+        d = torch.as_tensor(GV["smooth_in_%d" % k], device="cuda")
+        out = image_smooth(d, int(r), float(ratio), capi.TRIM_HEAPS)
+        assert out.cpu().numpy().tobytes() == GV["smooth_out_%d" % k].tobytes(), k
+
+
+def test_trace_tables_image_matches_reference_map_tracing():
+    """Table mode with the reference's quirks against the receiver image the
+    reference's own map_tracing produced on a B200 for the same 9-heliostat
+    scene, grid and tables (same bar as the oracle's pin)."""
+    from test_oracle_pins import GV, TRACE_QUIRKS, assert_trace_image_matches
+    res_x, res_y = (int(v) for v in GV["trace_res"])
+    rec = W.flat_receiver(0.0, 1.0, 1.0, res_x, res_y, normal=tuple(float(v) for v in GV["trace_rnorm"]))
+    rec.pos[:] = [float(v) for v in GV["trace_rpos"]]
+    rec.size[:] = [float(v) for v in GV["trace_rsize"]]
+    grid = W.grid(float(GV["trace_inter"][0]))
+    grid.explicit_bounds = 1
+    grid.origin[:] = [float(v) for v in GV["trace_gpos"]]
+    grid.extent[:] = [float(v) for v in GV["trace_gsize"]]
+    sc = SolarScene(GV["trace_pos"], GV["trace_size"], rec, grid, sigma=0.0, normal=GV["trace_normal"])
+    sun = W.make_sun(45.0, 180.0, 1000.0, 0.1)
+    sun.dir[:] = [float(v) for v in GV["trace_sun"]]
+    lights = int(GV["trace_lights"])
+    pl = float(GV["trace_pl"])
+    xz, helio = sc.points(W.params(0, lights, pl, mode=capi.POINTS_GRID))
+    p = W.params(0, lights, pl, quirks=TRACE_QUIRKS)
+    g = sc.trace_tables(sun, p, GV["trace_sun_local"], GV["trace_turb_local"], GV["trace_start"], xz, helio)
+    assert_trace_image_matches(g["energy"].cpu().numpy(), GV["trace_image"], len(helio) * lights)
+    sc.close()
+
+
+def test_grid_fine_div_must_be_a_power_of_two():
+    w = W.small()
+    w.grid = W.grid(10.0, fine_div=3)
+    with pytest.raises(capi.QmcrtError):
+        SolarScene.from_workload(w)
+
+
 def test_smoothing_u32_sorted_bit_exact():
     rng = np.random.default_rng(4)
     for (h, w_), r, ratio in [((128, 128), 2, 0.2), ((67, 201), 3, 0.1), ((1, 1), 2, 0.2), ((5, 300), 7, 0.45),
@@ -370,6 +471,12 @@ def test_trace_argument_errors(small):
     p.quirks = 1 << 20
     with pytest.raises(capi.QmcrtError):
         sc.trace(w.sun, p)
+    for field, value in (("attenuation", 7), ("kernel_variant", 9)):
+        p = W.params(int(w.params.rays), 256, 0.3)
+        setattr(p, field, value)
+        with pytest.raises(capi.QmcrtError) as e:
+            sc.trace(w.sun, p)
+        assert e.value.status == capi.ERR_INVALID_ARGUMENT
     # the scene still works after rejected calls
     g = sc.trace(w.sun, w.params)
     assert g["stats"].rays == w.params.rays

@@ -2,10 +2,13 @@
 
 tests/golden/ref_host_vectors.npz holds outputs of the reference's host-callable
 functions (global_function.cuh, scene_instance_process.cu, heap.cuh,
-heliostat.cpp) compiled from its sources by oracle/ref.mk and driven by
-tests/golden/gen_ref_vectors.py.  FP32 reference values against the FP64
-oracle: float-exact where the oracle replicates float arithmetic (Buie table,
-heaps), within FP32 rounding elsewhere.
+heliostat.cpp, image_save.cpp) compiled from its sources by oracle/ref.mk and
+driven by tests/golden/gen_ref_vectors.py.  tests/golden/ref_gpu_vectors.npz
+holds outputs of the reference's CUDA code run on a B200 by
+tests/golden/gen_ref_gpu_vectors.py: its smoothing kernel, its grid CSR and the
+receiver image of its map_tracing kernel.  FP32 reference values against the
+FP64 oracle: float-exact where the oracle replicates float arithmetic (Buie
+table, heaps, smoothing, grid), within FP32 rounding elsewhere.
 """
 import ctypes as C
 import os
@@ -18,7 +21,47 @@ from oracle import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 V = np.load(os.path.join(HERE, "golden", "ref_host_vectors.npz"))
+GV = np.load(os.path.join(HERE, "golden", "ref_gpu_vectors.npz"))
 D3 = C.c_double * 3
+# the reference quirks the traced-image pin runs with (SELF_HIT never fires in
+# this scene: no FP32 self-intersection survives the reference's t > 1e-6)
+TRACE_QUIRKS = capi.QUIRK_SKIP_ORIGIN_CELL | capi.QUIRK_AABB_RADIUS | capi.QUIRK_PREV_PERTURB | capi.QUIRK_PIXEL_EDGE
+
+
+class _Recv:
+    """Receiver attributes in the layout O.Scene reads."""
+
+    def __init__(self, pos, size, normal, face, res_x, res_y):
+        self.type = 0
+        self.pos, self.size, self.normal = list(pos), list(size), list(normal)
+        self.face, self.res_x, self.res_y = face, res_x, res_y
+
+
+def trace_pin_oracle_image(quirks):
+    """The oracle's raw |cos| image of the traced-image pin's scene and tables."""
+    g = GV
+    res_x, res_y = (int(v) for v in g["trace_res"])
+    rec = _Recv(g["trace_rpos"], g["trace_rsize"], g["trace_rnorm"], 0, res_x, res_y)
+    dims = [int(v) for v in np.ceil(g["trace_gsize"] / g["trace_inter"])]
+    sc = O.Scene(g["trace_pos"], g["trace_size"], 0.0, rec, float(g["trace_inter"][0]), 0.0, list(g["trace_sun"]),
+                 quirks=quirks, normal=g["trace_normal"], grid_bounds=(list(g["trace_gpos"]), list(g["trace_inter"]), dims))
+    xz, helio = O.points_grid(g["trace_size"], float(g["trace_pl"]))
+    lights = int(g["trace_lights"])
+    cfg = sc.cfg(0.1, 1, len(helio) * lights, lights, xz, helio, quirks=quirks)
+    o = sc.trace_tables(cfg, g["trace_sun_local"], g["trace_turb_local"], g["trace_start"])
+    return o["energy"].reshape(res_y, res_x), o["stats"]
+
+
+def assert_trace_image_matches(img, ref, rays):
+    """Maps of the same rays differ only by rays whose pixel or visibility
+    flips at an edge: each moves at most its energy |cos| <= 1 between two
+    pixels.  Bar: at most 1e-4 of the rays, no pixel off by more than two
+    rays' energy, equal totals."""
+    diff = np.abs(img.astype(np.float64) - ref.astype(np.float64))
+    per_ray = ref.sum() / rays
+    assert diff.sum() <= 2 * 1e-4 * rays * per_ray, diff.sum() / ref.sum()
+    assert diff.max() <= 2.0
+    assert abs(img.sum() - ref.sum()) <= 1e-4 * ref.sum()
 
 
 def test_local2world_matches_reference():
@@ -111,3 +154,33 @@ def test_heliostat_vertices_match_reference():
         assert np.allclose(v[:, 0], ref_v[:, 0], atol=5e-5)
         assert np.allclose(v[:, 1], ref_v[:, 1], atol=5e-5)
         assert np.allclose(v[:, 2], ref_v[:, 3], atol=5e-5)
+
+
+def test_smoothing_bit_exact_with_reference_gpu_kernel():
+    """ImageSmoother::image_smooth run on a B200 (texture reads, per-thread heaps)."""
+    for k in range(len(GV["smooth_params"])):
+        r, ratio = GV["smooth_params"][k]
+        out = O.smooth_f32(GV["smooth_in_%d" % k], int(r), float(ratio), capi.TRIM_HEAPS)
+        assert out.tobytes() == GV["smooth_out_%d" % k].tobytes(), k
+
+
+def test_grid_csr_equals_reference_grid():
+    """RectGrid::CGridHelioMatch's CSR (registration cubes, QUIRK_AABB_RADIUS)."""
+    rec = _Recv([0, 80, 0], [4, 4, 0.5], [0, 0, -1], 0, 16, 16)
+    sc = O.Scene(GV["grid_pos"], GV["grid_size"], 0.0, rec, 10.0, 0.0, [0.0, -0.7, 0.7], quirks=capi.QUIRK_AABB_RADIUS,
+                 normal=GV["grid_normal"],
+                 grid_bounds=(list(GV["grid_gpos"]), list(GV["grid_inter"]), [int(v) for v in GV["grid_dims"]]))
+    assert np.array_equal(sc.cell_start, GV["grid_start"])
+    assert np.array_equal(sc.entries[: sc.cell_start[-1]], GV["grid_entries"])
+
+
+def test_traced_image_matches_reference_map_tracing():
+    """The receiver image of the reference's map_tracing (per-heliostat
+    launches over explicit tables) against the oracle in table mode with the
+    reference's quirks; the corrected method differs visibly, so the quirks
+    are what is being matched."""
+    ref = GV["trace_image"]
+    img, st = trace_pin_oracle_image(TRACE_QUIRKS)
+    assert_trace_image_matches(img, ref, int(st[0]))
+    corrected, _ = trace_pin_oracle_image(0)
+    assert np.abs(corrected - ref).sum() > 1e-2 * ref.sum()
