@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling runs; multiple of 256)")
     ap.add_argument("--variant", type=int, default=0, help="trace kernel variant (qmcrt_trace_params.kernel_variant)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-versus-sequential section")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
     ap.add_argument("--cell", type=float, default=0.0, help="override the grid cell size (m; the coarse cell of a two-level grid)")
     ap.add_argument("--fine-div", type=int, default=-1, help="override the two-level grid split (1 = one level)")
     return ap.parse_args()
@@ -419,9 +420,11 @@ def b200_arm(a, rank, world, local):
                "d2h_bytes_per_step": int(d2h), "call": "qmcrt_trace_host"}
 
     batch = adj = None
-    if rank == 0 and world == 1 and not a.no_batch and a.workload == "mid" and not a.rays:
-        batch = batch_section()
-        adj = adjoint_section()
+    if rank == 0 and world == 1 and a.workload == "mid" and not a.rays:
+        if not a.no_batch:
+            batch = batch_section()
+        if not a.no_adjoint:
+            adj = adjoint_section()
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         ob = oracle_sample(w, a.cpu_seconds)

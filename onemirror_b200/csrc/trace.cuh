@@ -370,14 +370,18 @@ __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float* 
   uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
   float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
   float st, ct, sp, cp;
+  // The azimuths and the Box-Muller log use the hardware approximations
+  // (__sincosf, __logf: absolute errors near 2^-21): they scale milliradian
+  // polar angles, so a direction moves by ~1e-9 rad, far below FP32 rounding
+  // of the geometry that follows.
   sincos_small(th, &st, &ct);  // th <= 9.3 mrad
-  sincospif(2.f * u24f(r.y), &sp, &cp);
+  __sincosf(6.28318531f * u24f(r.y), &sp, &cp);
   *sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
-  float z = sqrtf(-2.f * logf(u24f(r.z))) * cospif(2.f * u24f(r.w));
+  float z = sqrtf(-2.f * __logf(u24f(r.z))) * __cosf(6.28318531f * u24f(r.w));
   float ths = sigma * z;
   uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
   sincos_small(ths, &st, &ct);
-  sincospif(2.f * u24f(extra), &sp, &cp);
+  __sincosf(6.28318531f * u24f(extra), &sp, &cp);
   *tl = f3(st * cp, ct, st * sp);
 }
 
@@ -433,33 +437,25 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab
     return;
   }
   const int h = R.h;
-  const frame64& fr = R.fr;
   const d3 o = R.o, ws = R.ws;
-  const float3 tl = R.tl;
-  const float w = R.w;
   const float3 of = to_f(o);
+  // perturbed normal, reflected direction (i - 2 n (n.i), normalised) and
+  // energy first, so that the mirror frame is dead before the walks
+  const d3 np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
+  const d3 rd = rnorm(ws - (2.0 * dot(ws, np)) * np);
+  // calEnergy (rectgrid_raytracing.cu:129-133)
+  const float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * R.w;
   uint8_t flag = 0;
   int pix = -1;
   double th = 0.0;
   if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, c.test, c.cell)) {
     flag = QMCRT_RAY_SHADOWED;
-  } else {
-    d3 np = rnorm(apply(fr, (double)tl.x, (double)tl.y, (double)tl.z));
-    double di = dot(ws, np);
-    d3 rd = rnorm(ws - (2.0 * di) * np);  // reflect (i - 2 n (n.i)), normalise
-    if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
-      flag = QMCRT_RAY_BLOCKED;
-    } else if (receiver_hit(a, o, rd, pix, &th)) {
-      flag = QMCRT_RAY_HIT;
-      if (pix < 0) {
-        flag |= QMCRT_RAY_OFFMAP;
-      } else {
-        // calEnergy (rectgrid_raytracing.cu:129-133) times eta(t) (:147)
-        float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w;
-        if (a.atten) e *= atten_eta(a.atten, (float)th);
-        deposit(pix, e);
-      }
-    }
+  } else if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
+    flag = QMCRT_RAY_BLOCKED;
+  } else if (receiver_hit(a, o, rd, pix, &th)) {
+    flag = QMCRT_RAY_HIT;
+    if (pix < 0) flag |= QMCRT_RAY_OFFMAP;
+    else deposit(pix, a.atten ? e * atten_eta(a.atten, (float)th) : e);  // times eta(t) (:147)
   }
   if (RECORDS) {
     if (a.flags) a.flags[ray] = flag;
