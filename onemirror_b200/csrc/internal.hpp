@@ -56,7 +56,7 @@ struct SunGeom {
   int32_t* cell_start = nullptr; // [cells+1]
   int32_t* entries = nullptr;    // [entry_cap]
   float4* cell_rect = nullptr;   // [3*entry_cap]
-  float2* cell_yr = nullptr;     // [cells]
+  int4* cell_info = nullptr;     // [cells] first, end, ylo bits, yhi bits
   float2* coarse_yr = nullptr;   // [coarse_cells] two-level grid only
   int* field_yr = nullptr;       // [2]
   double* power = nullptr;       // [1] sum |n . sun| * A
@@ -112,7 +112,7 @@ struct qmcrt_scene {
   int32_t* d_cell_start = nullptr;  // [cells+1]
   int32_t* d_entries = nullptr;     // [entry_cap]
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
-  float2* d_cell_yr = nullptr;      // [cells] height range of each cell's rectangles
+  int4* d_cell_info = nullptr;      // [cells] run of each cell's rectangles and their height range
   float2* d_coarse_yr = nullptr;    // [coarse_cells] the same per coarse cell (two-level grid)
   int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)
   qm::SunKey sun_key;

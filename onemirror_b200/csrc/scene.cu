@@ -186,11 +186,12 @@ __device__ __forceinline__ int ordered(float f) {
 }
 
 // Sort each cell's list ascending (the reference's push_back order,
-// grid.cpp:36-44), lay the rectangles out cell-major, and record the height
-// range [ylo, yhi] of the rectangles registered in each cell (for the
-// traversal's vertical culling) and of the whole field.
+// grid.cpp:36-44), lay the rectangles out cell-major, and write each cell's
+// record {first, end, ylo, yhi}: its run of rectangles and their height range
+// (for the traversal's vertical culling; one 16-byte load per DDA step), and
+// the height range of the whole field.
 __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t* entries,
-                                   const float4* rect, float4* cell_rect, float2* cell_yr, int* field_yr) {
+                                   const float4* rect, float4* cell_rect, int4* cell_info, int* field_yr) {
   int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   int b = start[c], e = start[c + 1];
@@ -213,7 +214,7 @@ __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t*
     ylo = fminf(ylo, fminf(fminf(y0, y1), fminf(y2, y3)));
     yhi = fmaxf(yhi, fmaxf(fmaxf(y0, y1), fmaxf(y2, y3)));
   }
-  cell_yr[c] = make_float2(ylo, yhi);
+  cell_info[c] = make_int4(b, e, __float_as_int(ylo), __float_as_int(yhi));
   if (e > b) {
     atomicMin(field_yr, ordered(ylo));
     atomicMax(field_yr + 1, ordered(yhi));
@@ -222,7 +223,7 @@ __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t*
 
 // Height range of each coarse cell of a two-level grid: the union of the
 // ranges of its div^3 fine cells (empty cells contribute nothing).
-__global__ void coarse_finish_kernel(int64_t coarse_cells, int div, int3 cdims, int gy, int gz, const float2* cell_yr,
+__global__ void coarse_finish_kernel(int64_t coarse_cells, int div, int3 cdims, int gy, int gz, const int4* cell_info,
                                      float2* coarse_yr) {
   int64_t cc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (cc >= coarse_cells) return;
@@ -231,9 +232,9 @@ __global__ void coarse_finish_kernel(int64_t coarse_cells, int div, int3 cdims, 
   for (int x = cx * div; x < (cx + 1) * div; ++x)
     for (int y = cy * div; y < (cy + 1) * div; ++y)
       for (int z = cz * div; z < (cz + 1) * div; ++z) {
-        float2 r = cell_yr[((int64_t)x * gy + y) * gz + z];
-        ylo = fminf(ylo, r.x);
-        yhi = fmaxf(yhi, r.y);
+        int4 r = cell_info[((int64_t)x * gy + y) * gz + z];
+        ylo = fminf(ylo, __int_as_float(r.z));
+        yhi = fmaxf(yhi, __int_as_float(r.w));
       }
   coarse_yr[cc] = make_float2(ylo, yhi);
 }
@@ -432,7 +433,7 @@ SunGeom scene_geom(qmcrt_scene* s) {
   g.cell_start = s->d_cell_start;
   g.entries = s->d_entries;
   g.cell_rect = s->d_cell_rect;
-  g.cell_yr = s->d_cell_yr;
+  g.cell_info = s->d_cell_info;
   g.coarse_yr = s->d_coarse_yr;
   g.field_yr = s->d_field_yr;
   g.power = reinterpret_cast<double*>(s->d_stats + 8);
@@ -455,7 +456,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
   GALLOC(g->cell_start, (size_t)s->cells + 1);
   GALLOC(g->entries, (size_t)s->entry_cap);
   GALLOC(g->cell_rect, 3 * (size_t)s->entry_cap);
-  GALLOC(g->cell_yr, (size_t)s->cells);
+  GALLOC(g->cell_info, (size_t)s->cells);
   if (s->coarse_cells) GALLOC(g->coarse_yr, (size_t)s->coarse_cells);
   GALLOC(g->field_yr, 2);
   GALLOC(g->power, 1);
@@ -465,7 +466,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
 
 void free_sun_geom(SunGeom* g) {
   dev_free(g->normal); dev_free(g->frame); dev_free(g->rect); dev_free(g->cellbox); dev_free(g->cell_count);
-  dev_free(g->cell_start); dev_free(g->entries); dev_free(g->cell_rect); dev_free(g->cell_yr); dev_free(g->field_yr);
+  dev_free(g->cell_start); dev_free(g->entries); dev_free(g->cell_rect); dev_free(g->cell_info); dev_free(g->field_yr);
   dev_free(g->coarse_yr); dev_free(g->power);
 }
 
@@ -502,12 +503,12 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
                                                   s->gdims[1], s->gdims[2], s->entry_cap);
   QM_CUDA(cudaGetLastError());
   cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
-                                                                        g.cell_rect, g.cell_yr, g.field_yr);
+                                                                        g.cell_rect, g.cell_info, g.field_yr);
   QM_CUDA(cudaGetLastError());
   if (s->coarse_cells) {
     int3 cd = make_int3(s->gdims[0] / s->fine_div, s->gdims[1] / s->fine_div, s->gdims[2] / s->fine_div);
     coarse_finish_kernel<<<(unsigned)((s->coarse_cells + 127) / 128), 128, 0, st>>>(
-        s->coarse_cells, s->fine_div, cd, s->gdims[1], s->gdims[2], g.cell_yr, g.coarse_yr);
+        s->coarse_cells, s->fine_div, cd, s->gdims[1], s->gdims[2], g.cell_info, g.coarse_yr);
     QM_CUDA(cudaGetLastError());
   }
   return QMCRT_OK;
@@ -718,7 +719,7 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_cell_start, (size_t)s->cells + 1);
   ALLOC(s->d_entries, (size_t)cap);
   ALLOC(s->d_cell_rect, 3 * (size_t)cap);
-  ALLOC(s->d_cell_yr, (size_t)s->cells);
+  ALLOC(s->d_cell_info, (size_t)s->cells);
   if (s->coarse_cells) ALLOC(s->d_coarse_yr, (size_t)s->coarse_cells);
   ALLOC(s->d_field_yr, 2);
   ALLOC(s->d_helio_weight, n);
@@ -752,7 +753,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_pos); dev_free(s->d_size); dev_free(s->d_aim); dev_free(s->d_normal_in);
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
-  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_yr); dev_free(s->d_coarse_yr); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

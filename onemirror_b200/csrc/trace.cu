@@ -175,8 +175,7 @@ void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, u
   a->sigma = s->d_sigma;
   a->weight = s->d_helio_weight;
   a->crect = geo.cell_rect;
-  a->cstart = geo.cell_start;
-  a->cell_yr = geo.cell_yr;
+  a->cinfo = geo.cell_info;
   a->field_yr = geo.field_yr;
   for (int i = 0; i < 3; ++i) {
     a->gpos[i] = s->gpos[i];

@@ -25,8 +25,7 @@ struct TraceArgs {
   const float* weight;  // [n] area per point; NULL -> 1
   // grid
   const float4* crect;
-  const int32_t* cstart;
-  const float2* cell_yr;  // [cells] height range of each cell's rectangles
+  const int4* cinfo;      // [cells] {first, end, ylo, yhi (float bits)}: the cell's run of crect
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
   int gdims[3];
@@ -120,9 +119,8 @@ __device__ __forceinline__ void sincos_small(float x, float* s, float* c) {
 // parallelogram test of rayParallelogramIntersect (global_function.cuh:78-105)
 // with the divisions by det folded into the comparisons.
 template <bool STATS>
-__device__ __forceinline__ bool cell_hit(const TraceArgs& a, int c, float3 o, float3 d, int own, bool selfhit,
+__device__ __forceinline__ bool cell_hit(const TraceArgs& a, int b, int e, float3 o, float3 d, int own, bool selfhit,
                                          uint32_t& ntest) {
-  int b = __ldg(a.cstart + c), e = __ldg(a.cstart + c + 1);
   for (int k = b; k < e; ++k) {
     float4 r0 = __ldg(a.crect + 3 * k);
     if (__float_as_int(r0.w) == own && !selfhit) continue;
@@ -189,12 +187,11 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
   float dx = px ? a.gcell[0] * qx : big, dy = py ? a.gcell[1] * qy : big, dz = pz ? a.gcell[2] * qz : big;
   // true if the cell may hold a hit: the ray's height over [t0, t1], widened
   // by a margin far above FP32 error, meets the cell's rectangle heights
-  auto may_hit = [&](int c, float t0, float t1) -> bool {
+  auto may_hit = [&](int4 ci, float t0, float t1) -> bool {
     if (!CULL) return true;
-    float2 yr = __ldg(a.cell_yr + c);
     float ya = o.y + t0 * d.y, yb = o.y + t1 * d.y;
     float mg = 0.01f + 1e-5f * t1;
-    return !(fmaxf(ya, yb) + mg < yr.x || fminf(ya, yb) - mg > yr.y);
+    return !(fmaxf(ya, yb) + mg < __int_as_float(ci.z) || fminf(ya, yb) - mg > __int_as_float(ci.w));
   };
   // whether the current coarse cell is stepped through, evaluated when the
   // walk enters a coarse cell; its exit along each axis is that axis' next
@@ -215,10 +212,12 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
   };
   if (TWO) coarse_eval(0.f);
   if (!(a.quirks & QMCRT_QUIRK_SKIP_ORIGIN_CELL)) {
-    int c = (ix * gy + iy) * gz + iz;
-    if ((!TWO || !cskip) && may_hit(c, 0.f, fminf(tx, fminf(ty, tz)))) {
-      if (STATS) ++ncell;
-      if (cell_hit<STATS>(a, c, o, d, own, selfhit, ntest)) return true;
+    if (!TWO || !cskip) {
+      const int4 ci = __ldg(a.cinfo + ((ix * gy + iy) * gz + iz));
+      if (may_hit(ci, 0.f, fminf(tx, fminf(ty, tz)))) {
+        if (STATS) ++ncell;
+        if (cell_hit<STATS>(a, ci.x, ci.y, o, d, own, selfhit, ntest)) return true;
+      }
     }
   }
   for (int guard = gx + gy + gz + 2; guard > 0; --guard) {
@@ -261,10 +260,10 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
       if (cross) coarse_eval(tin);
       if (cskip) continue;
     }
-    int c = (ix * gy + iy) * gz + iz;
-    if (!may_hit(c, tin, fminf(tx, fminf(ty, tz)))) continue;
+    const int4 ci = __ldg(a.cinfo + ((ix * gy + iy) * gz + iz));
+    if (!may_hit(ci, tin, fminf(tx, fminf(ty, tz)))) continue;
     if (STATS) ++ncell;
-    if (cell_hit<STATS>(a, c, o, d, own, selfhit, ntest)) return true;
+    if (cell_hit<STATS>(a, ci.x, ci.y, o, d, own, selfhit, ntest)) return true;
   }
   return false;
 }
