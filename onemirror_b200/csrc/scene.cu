@@ -677,6 +677,19 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   }
   s->cells = (int64_t)s->gdims[0] * s->gdims[1] * s->gdims[2];
   s->coarse_cells = div > 1 ? s->cells / ((int64_t)div * div * div) : 0;
+  // explicit bounds must contain every heliostat centre: a walk ends at the
+  // grid's edge, so an occluder outside it would never be tested (the
+  // reference indexes its cell vectors out of range there, grid.cpp:36-44)
+  if (grid->explicit_bounds)
+    for (int h = 0; h < s->n; ++h)
+      for (int i = 0; i < 3; ++i) {
+        double p = field->pos[3 * h + i], g0 = s->gpos[i], g1 = g0 + (double)s->gdims[i] * s->gcell[i];
+        if (!(p >= g0 && p < g1)) {
+          delete s;
+          return set_error(QMCRT_ERR_INVALID_ARGUMENT,
+                           "heliostat " + std::to_string(h) + " lies outside the explicit grid bounds");
+        }
+      }
   if (s->cells > (int64_t)64 * 1024 * 1024) {
     delete s;
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "grid has more than 2^26 cells; use larger cells");

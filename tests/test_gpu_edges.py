@@ -1,0 +1,151 @@
+"""Edge cases of the CUDA path against the FP64 oracle (same bar as
+test_gpu_parity): one heliostat, rays-per-point that is not a power of two,
+regular grid points through the full trace, given normals / tilts /
+per-heliostat slope errors, a sun below the horizon, zero DNI, accumulation,
+the largest ray count, and the arguments that must be rejected."""
+import numpy as np
+import pytest
+
+from onemirror_b200 import capi, workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from onemirror_b200.scene import SolarScene  # noqa: E402
+from test_gpu_parity import check_pair  # noqa: E402
+
+
+def trace_pair(w, sc, sun, params):
+    """GPU records and maps plus the oracle's on the same points and Philox stream."""
+    g = sc.trace(sun, params, records=True)
+    torch.cuda.synchronize()
+    gi = sc.grid_info()
+    ref = O.Scene(sc.pos, sc.size, sc.slope_sigma if sc.slope_sigma is not None else sc.sigma, w.receiver,
+                  w.grid.cell[0], w.grid.margin, list(sun.dir), quirks=params.quirks, aim=sc.aim, normal=sc.normal,
+                  tilt=sc.tilt, grid_csr=sc.read_grid(), grid_bounds=(list(gi.origin), list(gi.cell), list(gi.dims)))
+    xz, helio = sc.read_points()
+    weight = np.asarray(sc.size[:, 0] * sc.size[:, 2], np.float64) / np.bincount(helio, minlength=sc.n)
+    rays = int(g["stats"].rays)
+    cfg = ref.cfg(sun.csr, params.seed, rays, params.rays_per_point, xz, helio, weight, quirks=params.quirks,
+                  item=params.item)
+    return g, ref.trace_philox(cfg)
+
+
+def test_single_heliostat_spot_fits_the_receiver():
+    pos = np.array([[0.0, 1.5, -40.0]], np.float32)
+    size = np.array([[2.0, 0.05, 2.0]], np.float32)
+    rec = W.flat_receiver(20.0, 6.0, 6.0, 96, 96)
+    w = W.Workload("one", pos, size, 0.002, rec, W.grid(5.0), W.make_sun(50.0, 180.0), W.params(64 * 256, 256, 0.2))
+    sc = SolarScene.from_workload(w)
+    g, o = trace_pair(w, sc, w.sun, w.params)
+    check_pair(w, g, o)
+    st = g["stats"]
+    assert st.shadowed == 0 and st.blocked == 0 and st.hit == st.rays and st.offmap == 0
+    assert abs(st.intercept_ratio - 1.0) < 1e-3  # every ray lands (reflectivity cancels in the ratio)
+    sc.close()
+
+
+def test_rays_per_point_not_a_power_of_two():
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    p = W.params(w.n * 16 * 100, 100, 0.3, seed=17)
+    g, o = trace_pair(w, sc, w.sun, p)
+    check_pair(w, g, o)
+    sc.close()
+
+
+def test_regular_grid_points_through_the_full_trace():
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    p = W.params(0, 64, 0.25, seed=19, mode=capi.POINTS_GRID)
+    g, o = trace_pair(w, sc, w.sun, p)
+    assert g["stats"].rays == w.n * 8 * 8 * 64  # 2 x 2 m mirrors, 0.25 m cells
+    check_pair(w, g, o)
+    sc.close()
+
+
+def test_given_normals_tilts_and_per_heliostat_slope_errors():
+    w = W.small()
+    rng = np.random.default_rng(5)
+    ref = O.Scene(w.pos, w.size, w.sigma, w.receiver, w.grid.cell[0], w.grid.margin, list(w.sun.dir))
+    normal = ref.normal + rng.normal(0, 0.01, ref.normal.shape)
+    normal = (normal / np.linalg.norm(normal, axis=1, keepdims=True)).astype(np.float32)
+    slope = rng.uniform(0.001, 0.004, w.n).astype(np.float32)
+    sc = SolarScene(w.pos, w.size, w.receiver, w.grid, sigma=w.sigma, normal=normal, slope_sigma=slope)
+    g, o = trace_pair(w, sc, w.sun, w.params)
+    check_pair(w, g, o)
+    sc.close()
+    tilt = rng.normal(0, 0.004, (w.n, 2)).astype(np.float32)
+    sc = SolarScene(w.pos, w.size, w.receiver, w.grid, sigma=w.sigma, tilt=tilt)
+    g, o = trace_pair(w, sc, w.sun, W.params(int(w.params.rays), 256, 0.3, seed=23))
+    check_pair(w, g, o)
+    sc.close()
+
+
+def test_sun_below_the_horizon():
+    """An incident direction pointing up: the mirrors face away from the
+    receiver; whatever the geometry gives, both sides give the same."""
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    sun = W.make_sun(-5.0, 180.0)
+    g, o = trace_pair(w, sc, sun, W.params(int(w.params.rays), 256, 0.3, seed=29))
+    check_pair(w, g, o)
+    sc.close()
+
+
+def test_zero_dni_and_accumulation():
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    ref = sc.trace(w.sun, w.params)
+    counts, flux = ref["counts"].clone(), ref["flux"].clone()
+    dark = W.make_sun(45.0, 180.0, 0.0, 0.1)
+    g = sc.trace(dark, w.params)
+    assert torch.equal(g["counts"], counts) and float(g["flux"].abs().max()) == 0.0
+    assert g["stats"].total_power == 0.0
+    out = sc._outputs(0, False)
+    sc.trace(w.sun, w.params, stats=False, outputs=out)
+    p = W.params(int(w.params.rays), 256, 0.3)
+    p.accumulate = 1
+    sc.trace(w.sun, p, stats=False, outputs=out)
+    assert torch.equal(out[1]["counts"], 2 * counts)
+    assert torch.allclose(out[1]["flux"], 2 * flux, rtol=1e-6, atol=1e-3)
+    sc.close()
+
+
+def test_largest_ray_count():
+    """2^32 - 4096 rays (ray ids fill 32 bits; 2^20 - 1 points x 4096): the
+    count map still sums to the hits; 2^32 rays are rejected before anything
+    is allocated or launched."""
+    w = W.mid()
+    w.params = W.params((1 << 32) - 4096, 4096, 0.18)
+    sc = SolarScene.from_workload(w)
+    g = sc.trace(w.sun, w.params)
+    st = g["stats"]
+    assert st.rays == (1 << 32) - 4096
+    assert g["counts"].sum().item() == st.hit - st.offmap
+    assert 0.5 < st.hit / st.rays < 0.8
+    p = W.params(1 << 32, 4096, 0.18)
+    with pytest.raises(capi.QmcrtError) as e:
+        sc.trace(w.sun, p)
+    assert e.value.status == capi.ERR_INVALID_ARGUMENT
+    sc.close()
+
+
+def test_rejected_fields_and_grids():
+    w = W.small()
+    with pytest.raises(capi.QmcrtError):  # empty field
+        SolarScene(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), w.receiver, w.grid)
+    g = W.grid(10.0)
+    g.explicit_bounds = 1
+    g.origin[:] = [-20.0, -1.0, -20.0]   # a box that misses most of the field
+    g.extent[:] = [40.0, 20.0, 40.0]
+    with pytest.raises(capi.QmcrtError) as e:
+        SolarScene(w.pos, w.size, w.receiver, g)
+    assert e.value.status == capi.ERR_INVALID_ARGUMENT and "outside the explicit grid" in str(e.value)
+    bad = W.grid(0.0)
+    with pytest.raises(capi.QmcrtError):
+        SolarScene(w.pos, w.size, w.receiver, bad)
