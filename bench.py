@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
     ap.add_argument("--cell", type=float, default=0.0, help="override the grid cell size (m; the coarse cell of a two-level grid)")
     ap.add_argument("--fine-div", type=int, default=-1, help="override the two-level grid split (1 = one level)")
+    ap.add_argument("--sun-elev", type=float, default=None, help="override the sun elevation (degrees)")
     return ap.parse_args()
 
 
@@ -319,6 +320,7 @@ def b200_arm(a, rank, world, local):
     p.kernel_variant = a.variant
     rays = int(p.rays)
     base_az = 180.0
+    sun_elev = a.sun_elev if a.sun_elev is not None else {"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload]
 
     # FP32 issue-rate peak, measured live (best of 5 bursts)
     sink = torch.zeros(8192, device=dev)
@@ -338,7 +340,7 @@ def b200_arm(a, rank, world, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
     def one(k, item, want_stats=False):
-        el, az = {"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload], base_az + 0.01 * k
+        el, az = sun_elev, base_az + 0.01 * k
         sun = W.make_sun(el, az, w.sun.dni, w.sun.csr)
         p.item = item
         r = sc.trace(sun, p, stats=want_stats, outputs=outs)
@@ -406,7 +408,7 @@ def b200_arm(a, rank, world, local):
                 if world > 1:
                     dist.barrier()
                 t0 = time.perf_counter()
-            sun = W.make_sun({"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload], base_az - 0.01 * (k + 1),
+            sun = W.make_sun(sun_elev, base_az - 0.01 * (k + 1),
                              w.sun.dni, w.sun.csr)
             p.item = D.shard_item(rank, 9000 + k)
             capi.check(capi.lib().qmcrt_trace_host(sc.h, C.byref(f), C.byref(sun), C.byref(p),

@@ -163,9 +163,10 @@ typedef struct qmcrt_trace_params {
   uint32_t quirks;         /* QMCRT_QUIRK_* */
   int32_t deposit;         /* QMCRT_DEPOSIT_* */
   int32_t accumulate;      /* 0: zero the output maps first; 1: add into them */
-  int32_t kernel_variant;  /* 0 or 1: default (fastest); 2: no vertical culling (every cell on the path
+  int32_t kernel_variant;  /* 0 or 1: default (fastest: Philox rays test their heliostat's occluder
+                              candidates); 2: grid walk without vertical culling (every cell on the path
                               tested); 3: the production kernel without its 4-CTA register cap;
-                              4: a two-level grid walked on its fine level only */
+                              4: grid walk, a two-level grid on its fine level only; 5: grid walk */
   uint32_t item;           /* Philox stream (counter word 2): distinct items give independent ray sets
                               (shards of one trace, items of a batch) */
   int32_t attenuation;     /* QMCRT_ATTEN_*: atmospheric transmittance of the mirror-to-receiver leg */
@@ -233,6 +234,27 @@ typedef struct qmcrt_layout_params {
   uint64_t seed;
 } qmcrt_layout_params;
 
+/* A faceted paraboloid heliostat (SceneFileProc::SceneFileRead,
+ * scene_file_proc.cpp:288-341): rows x cols flat square facets of side
+ * `facet` whose centres sit on the paraboloid y = x^2/a^2 + z^2/b^2 of the
+ * heliostat's local frame at pitch facet + gap, each canted to the
+ * paraboloid's normal (-2x/a^2, 1, -2z/b^2) there.  The local frame is
+ * (e1, n, e1 x n) with n the heliostat normal and e1 horizontal; it is placed
+ * at `centre`.  Every facet is one rectangle with a given normal in a
+ * qmcrt_field.  The reference's own scene: a = b (its arguments A, B),
+ * 3 x 3 facets of sqrt(2)/3 m, gap 0.1 m, thickness 0.1 m. */
+typedef struct qmcrt_facet_params {
+  float a, b;            /* paraboloid coefficients (m) */
+  float normal[3];       /* heliostat normal (mirrorNormal), unit */
+  float centre[3];       /* world position of the paraboloid's vertex */
+  int32_t rows, cols;    /* facets along local z and x */
+  float facet;           /* facet side (m) */
+  float gap;             /* gap between facets (m) */
+  float thickness;       /* facet thickness (m) */
+  int32_t reference_frame; /* 1: the reference's e1 = (n.z, 0, -n.x) / sqrt(n.x^2 + n.y^2), which is not a unit
+                              vector in general (scene_file_proc.cpp:300-316); 0: e1 normalised */
+} qmcrt_facet_params;
+
 typedef struct qmcrt_scene qmcrt_scene;
 typedef struct qmcrt_tape qmcrt_tape;
 typedef struct qmcrt_batch qmcrt_batch;
@@ -268,6 +290,12 @@ qmcrt_status qmcrt_buie_table(float csr, float* cdf_x /*[1025]*/, float* cdf_y /
 /* Radial-staggered layout: writes up to `capacity` heliostat centres. */
 qmcrt_status qmcrt_layout_radial_staggered(const qmcrt_layout_params* p, float* h_pos,
                                            int32_t capacity, int32_t* n_out);
+
+/* Facets of one paraboloid heliostat into h_pos / h_size / h_normal [3 x
+ * rows x cols] (row-major over local z then x, as the reference lists them);
+ * *n_out = rows x cols.  Normals are unit length. */
+qmcrt_status qmcrt_layout_paraboloid_facets(const qmcrt_facet_params* p, float* h_pos, float* h_size, float* h_normal,
+                                            int32_t capacity, int32_t* n_out);
 
 /* Parse a reference .scn scene file (scene_file_proc.cpp:41-286) into
  * caller-visible arrays.  Call once with h_pos == NULL to get the counts. */

@@ -94,6 +94,12 @@ class Timing(C.Structure):
     _fields_ = [("setup_ms", C.c_float), ("trace_kernel_ms", C.c_float), ("finalize_ms", C.c_float)]
 
 
+class FacetParams(C.Structure):
+    _fields_ = [("a", C.c_float), ("b", C.c_float), ("normal", C.c_float * 3), ("centre", C.c_float * 3),
+                ("rows", C.c_int32), ("cols", C.c_int32), ("facet", C.c_float), ("gap", C.c_float),
+                ("thickness", C.c_float), ("reference_frame", C.c_int32)]
+
+
 class LayoutParams(C.Structure):
     _fields_ = [("n", C.c_int32), ("helio_w", C.c_float), ("helio_h", C.c_float), ("thickness", C.c_float),
                 ("r_min", C.c_float), ("r_max", C.c_float), ("az_center_deg", C.c_float),
@@ -122,6 +128,7 @@ PROTOTYPES = {
     "qmcrt_buie_table": (C.c_int, [C.c_float, fp, fp, fp, fp]),
     "qmcrt_layout_radial_staggered": (C.c_int, [C.POINTER(LayoutParams), fp, C.c_int32, i32p]),
     "qmcrt_scn_parse": (C.c_int, [C.c_char_p, C.POINTER(Receiver), C.POINTER(GridParams), fp, fp, C.c_int32, i32p]),
+    "qmcrt_layout_paraboloid_facets": (C.c_int, [C.POINTER(FacetParams), fp, fp, fp, C.c_int32, i32p]),
     "qmcrt_write_flux_csv": (C.c_int, [C.c_char_p, fp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "qmcrt_write_intercept_ratio": (C.c_int, [C.c_char_p, fp, C.c_int32, C.c_int32, C.c_float, C.c_int32, fp]),
     "qmcrt_scene_create": (C.c_int, [C.POINTER(Field), C.POINTER(Receiver), C.POINTER(GridParams), C.POINTER(C.c_void_p)]),

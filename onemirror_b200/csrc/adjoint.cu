@@ -148,14 +148,20 @@ __device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, doub
 template <bool CULL>
 __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, float fy0, float fy1, d3* np, d3* rd,
                                          double* u, double* v) {
+  // with CULL (corrected mode) the heliostat's occluder candidates answer the
+  // visibility questions (the grid walk where there are none)
   uint32_t nt = 0, nc = 0;
   const float3 of = to_f(R.o);
-  if (dda_blocked<false, CULL>(a, of, f3((float)-R.ws.x, (float)-R.ws.y, (float)-R.ws.z), R.h, fy0, fy1, nt, nc))
+  const float3 sd = f3((float)-R.ws.x, (float)-R.ws.y, (float)-R.ws.z);
+  if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc)
+           : dda_blocked<false, false>(a, of, sd, R.h, fy0, fy1, nt, nc))
     return false;
   *np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
   double di = dot(R.ws, *np);
   *rd = rnorm(R.ws - (2.0 * di) * *np);
-  if (dda_blocked<false, CULL>(a, of, to_f(*rd), R.h, fy0, fy1, nt, nc)) return false;
+  if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(*rd), fy0, fy1, nt, nc)
+           : dda_blocked<false, false>(a, of, to_f(*rd), R.h, fy0, fy1, nt, nc))
+    return false;
   return receiver_uv(a, R.o, *rd, u, v);
 }
 
@@ -402,6 +408,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.t.b_C = t->buie.params[5];
   A.t.b_inv = 1 / (t->buie.params[1] + 1);
   A.t.b_inv_bucket = t->buie.inv_bucket;
+  if (!t->buie.within_alpha) A.t.cand = A.t.cand_n = nullptr;  // walk the grid
   A.t.rays = (uint32_t)p->rays;
   A.t.rpp = p->rays_per_point;
   A.t.rpp_shift = (A.t.rpp & (A.t.rpp - 1)) ? -1 : __builtin_ctz((unsigned)A.t.rpp);
@@ -459,6 +466,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   A.t.b_C = t->buie.params[5];
   A.t.b_inv = 1 / (t->buie.params[1] + 1);
   A.t.b_inv_bucket = t->buie.inv_bucket;
+  if (!t->buie.within_alpha) A.t.cand = A.t.cand_n = nullptr;
   A.t.rays = t->args.t.rays;
   A.t.rpp = t->args.t.rpp;
   A.t.rpp_shift = t->args.t.rpp_shift;

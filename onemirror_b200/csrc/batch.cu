@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
       const TileDeposit<T> dep{s_cnt, s_en, s_anchor[2] ? s_anchor[0] : -(1 << 30), s_anchor[1], s_a.res_x,
                                s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, true>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep);
+        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep);
       __syncthreads();
       if (s_anchor[2]) {  // flush the tile's non-zero pixels, then clear it
         for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
     } else {
       const GlobalDeposit dep{s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, true>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep);
+        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep);
     }
     __syncthreads();  // everyone is done with s_c / s_a / the tile before the next chunk
   }
@@ -356,6 +356,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     fill_trace_args(it.scene, it.geo, &it.sun, 0, &a);
     const BuieTable& t = b->tables[csr];
     a.buie = b->d_tables[csr];
+    if (!t.within_alpha) a.cand = a.cand_n = nullptr;  // the item's rays walk the grid
     a.b_total = t.params[3];
     a.b_core = t.params[2];
     a.b_B = t.params[4];

@@ -69,6 +69,9 @@ QMCRT_HD uint4 philox4x32_10(uint4 c, uint2 k) {
 // Uniform in (0,1) from the top 24 bits: exact in float and double.
 QMCRT_HD float u24f(uint32_t w) { return ((float)(w >> 8) + 0.5f) * (1.0f / 16777216.0f); }
 
+// Occluder candidates kept per heliostat and walk direction.
+constexpr int kCandCap = 32;
+
 constexpr uint32_t kTagTrace = 0x51A7u;
 constexpr uint32_t kTagPoisson = 0x9015u;
 constexpr uint32_t kPoissonKey0 = 0x5A17C0DEu;

@@ -419,6 +419,63 @@ qmcrt_status qmcrt_scn_parse(const char* path, qmcrt_receiver* recv_out, qmcrt_g
   return QMCRT_OK;
 }
 
+// ------------------------------------------------------------ faceted heliostat
+qmcrt_status qmcrt_layout_paraboloid_facets(const qmcrt_facet_params* p, float* h_pos, float* h_size, float* h_normal,
+                                            int32_t capacity, int32_t* n_out) {
+  if (!p || !n_out) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!(p->a > 0) || !(p->b > 0) || p->rows < 1 || p->cols < 1 || !(p->facet > 0) || !(p->gap >= 0) ||
+      !(p->thickness >= 0))
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "paraboloid facets need a, b, facet > 0, rows, cols >= 1, gap >= 0");
+  const int64_t n = (int64_t)p->rows * p->cols;
+  if (n > 0x7FFFFFFF) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "too many facets");
+  *n_out = (int32_t)n;
+  if (!h_pos && !h_size && !h_normal) return QMCRT_OK;
+  if (capacity < n) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "capacity too small");
+  double nv[3] = {p->normal[0], p->normal[1], p->normal[2]};
+  const double ln = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+  if (!(ln > 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "heliostat normal is zero");
+  if (!p->reference_frame)
+    for (double& c : nv) c /= ln;
+  // horizontal axis e1 (scene_file_proc.cpp:300-316): the reference divides
+  // (n.z, 0, -n.x) by sqrt(n.x^2 + n.y^2); the corrected frame by its length
+  double e1[3];
+  const double t = p->reference_frame ? std::sqrt(nv[0] * nv[0] + nv[1] * nv[1]) : std::sqrt(nv[0] * nv[0] + nv[2] * nv[2]);
+  if (nv[2] > 0 && t > 0) {
+    e1[0] = nv[2] / t; e1[1] = 0; e1[2] = -nv[0] / t;
+  } else if (nv[2] < 0 && t > 0) {
+    e1[0] = -nv[2] / t; e1[1] = 0; e1[2] = nv[0] / t;
+  } else {
+    e1[0] = 0; e1[1] = 0; e1[2] = 1;
+  }
+  // third axis e1 x n (:317-319)
+  const double e2[3] = {e1[1] * nv[2] - e1[2] * nv[1], e1[2] * nv[0] - e1[0] * nv[2], e1[0] * nv[1] - e1[1] * nv[0]};
+  const double pitch = (double)p->facet + p->gap, a2 = (double)p->a * p->a, b2 = (double)p->b * p->b;
+  int64_t k = 0;
+  for (int r = 0; r < p->rows; ++r)
+    for (int c = 0; c < p->cols; ++c, ++k) {
+      // facet centre on the paraboloid (:289-297) and its normal (:325-327)
+      const double x = (c - 0.5 * (p->cols - 1)) * pitch, z = (r - 0.5 * (p->rows - 1)) * pitch;
+      const double y = x * x / a2 + z * z / b2;
+      const double ln_[3] = {-2.0 * x / a2, 1.0, -2.0 * z / b2};
+      double w[3], m[3];
+      for (int i = 0; i < 3; ++i) {
+        w[i] = x * e1[i] + y * nv[i] + z * e2[i] + p->centre[i];
+        m[i] = ln_[0] * e1[i] + ln_[1] * nv[i] + ln_[2] * e2[i];
+      }
+      const double lm = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+      for (int i = 0; i < 3; ++i) {
+        if (h_pos) h_pos[3 * k + i] = (float)w[i];
+        if (h_normal) h_normal[3 * k + i] = (float)(m[i] / lm);
+      }
+      if (h_size) {
+        h_size[3 * k] = p->facet;
+        h_size[3 * k + 1] = p->thickness;
+        h_size[3 * k + 2] = p->facet;
+      }
+    }
+  return QMCRT_OK;
+}
+
 // ------------------------------------------------------------ result files
 // The map is [height][width], row 0 at the receiver's v0 edge; both writers
 // walk it from the last row to the first (the top of the receiver first), as

@@ -36,6 +36,7 @@ struct BuieTable {
   std::vector<float> host;  // cdf_x | cdf_y | slope | guide (int bits)
   float params[6];          // k, gamma, core, total, B, C
   float inv_bucket = 0;     // guide buckets per unit of CDF
+  bool within_alpha = false; // every sample lies within kSunAlphaMax of the sun axis
 };
 
 // Build the table exactly as set_samplelights does (float arithmetic).
@@ -47,6 +48,13 @@ qmcrt_status receiver_setup(const qmcrt_receiver& r, ReceiverGeom* g);
 // Device geometry of a field for one sun position: aimed normals and frames,
 // rectangle records and the grid CSR.  A scene owns one; a batch owns one per
 // (field, sun) item.
+// Largest angle of a Buie sun sample from the sun axis (rad): the aureole
+// ends at 9.3 mrad for every CSR; the host checks each table against it.
+constexpr double kSunAlphaMax = 9.31e-3;
+// Largest |z| of the slope-error deviate sqrt(-2 ln u1) cos(2 pi u2) with
+// 24-bit uniforms (u1 >= 2^-25): 5.89, in units of sigma.
+constexpr double kSlopeZMax = 6.0;
+
 struct SunGeom {
   double* normal = nullptr;      // [3n]
   double* frame = nullptr;       // [9n] u, n, v
@@ -58,6 +66,8 @@ struct SunGeom {
   float4* cell_rect = nullptr;   // [3*entry_cap]
   int4* cell_info = nullptr;     // [cells] first, end, ylo bits, yhi bits
   float2* coarse_yr = nullptr;   // [coarse_cells] two-level grid only
+  int* cand = nullptr;           // [n][2][kCandCap] occluder candidates of each heliostat's shadow / block rays
+  int* cand_n = nullptr;         // [n][2] their counts (> kCandCap: too many, the rays walk the grid)
   int* field_yr = nullptr;       // [2]
   double* power = nullptr;       // [1] sum |n . sun| * A
 };
@@ -89,6 +99,7 @@ struct qmcrt_scene {
   uint64_t field_version = 0;
   bool has_aim = false, has_normal = false, has_tilt = false;
   std::vector<float> h_pos, h_size;
+  float ytop = 0.f;  // highest point any mirror can reach (centre + half-diagonal)
   qmcrt_receiver recv{};
   qm::ReceiverGeom rg;
   qmcrt_grid_params gp{};
@@ -114,6 +125,8 @@ struct qmcrt_scene {
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
   int4* d_cell_info = nullptr;      // [cells] run of each cell's rectangles and their height range
   float2* d_coarse_yr = nullptr;    // [coarse_cells] the same per coarse cell (two-level grid)
+  int* d_cand = nullptr;            // [n][2][kCandCap] occluder candidates (shadow, block)
+  int* d_cand_n = nullptr;          // [n][2]
   int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)
   qm::SunKey sun_key;
 

@@ -239,6 +239,90 @@ __global__ void coarse_finish_kernel(int64_t coarse_cells, int div, int3 cdims, 
   coarse_yr[cc] = make_float2(ylo, yhi);
 }
 
+// Occluder candidates of each heliostat's rays (corrected mode, Philox
+// sampling): every heliostat k whose bounding sphere some ray of heliostat h
+// can reach on its way to the sun (shadow) or after reflection (block).  A
+// ray starts within R_h of h's centre and leaves inside a cone about the
+// walk's axis: the sun axis widened by the largest Buie angle for shadow
+// rays; the nominal reflection widened by that angle plus twice the largest
+// slope deviation (zmax sigma: the Box-Muller deviate of 24-bit uniforms is at
+// most 5.89 in magnitude) for block rays.  Once every ray of the cone rises, a
+// sphere entirely below the lowest ray of the cone is out of reach too.
+struct CandArgs {
+  int n;
+  const float *pos, *size, *sigma;
+  const double* frame;
+  double sun[3];      // incident direction, unit
+  double sun_alpha;   // largest angle of a sun sample from the sun axis (rad)
+  double zmax;        // largest |z| of the slope deviate, in units of sigma
+  int* cand;          // [n][2][kCandCap]
+  int* cand_n;        // [n][2]
+};
+
+__device__ __forceinline__ double bound_radius(const float* size, int h) {
+  double x = size[3 * h], y = size[3 * h + 1], z = size[3 * h + 2];
+  return 0.5 * sqrt(x * x + y * y + z * z) + 0.01;  // + 1 cm for FP32 rounding of records and origins
+}
+
+// Can a ray from within Rh of ch, leaving within angle atan(tan_a) of the
+// unit axis d, meet the sphere (ck, Rk)?  At axial distance t a ray is at most
+// Rh + (t + Rh) tan_a from the axis; rays rise at least dymin per unit length.
+__device__ __forceinline__ bool cone_reaches(d3 ch, double Rh, d3 d, double tan_a, double dymin, d3 ck, double Rk) {
+  const d3 q = ck - ch;
+  const double t = dot(q, d), rr = Rh + Rk;
+  if (t < -rr) return false;
+  const d3 v = q - t * d;
+  const double lim = rr + (fmax(t, 0.0) + rr) * tan_a;
+  if (dot(v, v) > lim * lim) return false;
+  if (dymin > 1e-3 && t - Rk > Rh + (ck.y + Rk - (ch.y - Rh)) / dymin) return false;
+  return true;
+}
+
+__global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int h = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (h >= a.n) return;  // h is uniform across the warp
+  const d3 ch = mk(a.pos[3 * h], a.pos[3 * h + 1], a.pos[3 * h + 2]);
+  const double Rh = bound_radius(a.size, h);
+  const double* F = a.frame + 9 * h;
+  const d3 nh = mk(F[3], F[4], F[5]);
+  const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
+  const d3 ds = mk(-s.x, -s.y, -s.z);
+  const d3 db = s - (2.0 * dot(s, nh)) * nh;
+  const double as = a.sun_alpha + 1e-6, ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
+  const double ts = tan(as), tb = tan(ab);
+  const double ys = sin(asin(fmin(fmax(ds.y, -1.0), 1.0)) - as), yb = sin(asin(fmin(fmax(db.y, -1.0), 1.0)) - ab);
+  int* Ls = a.cand + (int64_t)2 * h * kCandCap;
+  int* Lb = Ls + kCandCap;
+  int ns = 0, nb = 0;
+  const unsigned below = (1u << lane) - 1u;
+  for (int k0 = 0; k0 < a.n; k0 += 32) {
+    const int k = k0 + lane;
+    bool rs = false, rb = false;
+    if (k < a.n && k != h) {
+      const d3 ck = mk(a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]);
+      const double Rk = bound_radius(a.size, k);
+      rs = cone_reaches(ch, Rh, ds, ts, ys, ck, Rk);
+      rb = cone_reaches(ch, Rh, db, tb, yb, ck, Rk);
+    }
+    const unsigned ms = __ballot_sync(0xffffffffu, rs), mb = __ballot_sync(0xffffffffu, rb);
+    if (rs) {
+      const int slot = ns + __popc(ms & below);
+      if (slot < kCandCap) Ls[slot] = k;
+    }
+    if (rb) {
+      const int slot = nb + __popc(mb & below);
+      if (slot < kCandCap) Lb[slot] = k;
+    }
+    ns += __popc(ms);
+    nb += __popc(mb);
+  }
+  if (lane == 0) {
+    a.cand_n[2 * h] = ns;
+    a.cand_n[2 * h + 1] = nb;
+  }
+}
+
 // ------------------------------------------------------------ points
 struct PoissonArgs {
   int n;
@@ -399,6 +483,11 @@ qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st)
   bool sizes_changed = s->h_size.size() != 3 * n || std::memcmp(s->h_size.data(), f->size, 3 * n * sizeof(float)) != 0;
   s->h_pos.assign(f->pos, f->pos + 3 * n);
   s->h_size.assign(f->size, f->size + 3 * n);
+  s->ytop = -3.0e38f;
+  for (size_t h = 0; h < n; ++h) {
+    const float* z = f->size + 3 * h;
+    s->ytop = std::max(s->ytop, f->pos[3 * h + 1] + 0.5f * std::sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2]));
+  }
   s->field_version++;
   if (sizes_changed) s->points_key = PointsKey{};
   return QMCRT_OK;
@@ -435,6 +524,8 @@ SunGeom scene_geom(qmcrt_scene* s) {
   g.cell_rect = s->d_cell_rect;
   g.cell_info = s->d_cell_info;
   g.coarse_yr = s->d_coarse_yr;
+  g.cand = s->d_cand;
+  g.cand_n = s->d_cand_n;
   g.field_yr = s->d_field_yr;
   g.power = reinterpret_cast<double*>(s->d_stats + 8);
   return g;
@@ -458,6 +549,8 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
   GALLOC(g->cell_rect, 3 * (size_t)s->entry_cap);
   GALLOC(g->cell_info, (size_t)s->cells);
   if (s->coarse_cells) GALLOC(g->coarse_yr, (size_t)s->coarse_cells);
+  GALLOC(g->cand, 2 * kCandCap * n);
+  GALLOC(g->cand_n, 2 * n);
   GALLOC(g->field_yr, 2);
   GALLOC(g->power, 1);
 #undef GALLOC
@@ -467,7 +560,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
 void free_sun_geom(SunGeom* g) {
   dev_free(g->normal); dev_free(g->frame); dev_free(g->rect); dev_free(g->cellbox); dev_free(g->cell_count);
   dev_free(g->cell_start); dev_free(g->entries); dev_free(g->cell_rect); dev_free(g->cell_info); dev_free(g->field_yr);
-  dev_free(g->coarse_yr); dev_free(g->power);
+  dev_free(g->coarse_yr); dev_free(g->cand); dev_free(g->cand_n); dev_free(g->power);
 }
 
 // Aim every heliostat for the sun (normalised) and rebuild the grid into g:
@@ -496,6 +589,19 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   QM_CUDA(cudaMemsetAsync(g.cell_count, 0, s->cells * sizeof(int32_t), st));
   QM_CUDA(cudaMemsetAsync(g.power, 0, sizeof(double), st));
   aim_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(a);
+  QM_CUDA(cudaGetLastError());
+  CandArgs ca{};
+  ca.n = s->n;
+  ca.pos = s->d_pos;
+  ca.size = s->d_size;
+  ca.sigma = s->d_sigma;
+  ca.frame = g.frame;
+  for (int i = 0; i < 3; ++i) ca.sun[i] = sun[i];
+  ca.sun_alpha = kSunAlphaMax;
+  ca.zmax = kSlopeZMax;
+  ca.cand = g.cand;
+  ca.cand_n = g.cand_n;
+  cand_kernel<<<(s->n + 3) / 4, 128, 0, st>>>(ca);
   QM_CUDA(cudaGetLastError());
   scan_kernel<<<1, 1024, 0, st>>>(g.cell_count, g.cell_start, s->cells, s->entry_cap, s->d_flag, g.field_yr);
   QM_CUDA(cudaGetLastError());
@@ -734,6 +840,8 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_cell_rect, 3 * (size_t)cap);
   ALLOC(s->d_cell_info, (size_t)s->cells);
   if (s->coarse_cells) ALLOC(s->d_coarse_yr, (size_t)s->coarse_cells);
+  ALLOC(s->d_cand, 2 * kCandCap * n);
+  ALLOC(s->d_cand_n, 2 * n);
   ALLOC(s->d_field_yr, 2);
   ALLOC(s->d_helio_weight, n);
   ALLOC(s->d_flag, 1);
@@ -766,7 +874,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_pos); dev_free(s->d_size); dev_free(s->d_aim); dev_free(s->d_normal_in);
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
-  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_cand); dev_free(s->d_cand_n); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

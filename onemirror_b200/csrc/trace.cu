@@ -81,6 +81,8 @@ static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
 
 template <bool TABLES, bool RECORDS>
 static cudaError_t dispatch2(const TraceArgs& a, bool stats, int cull, cudaStream_t st) {
+  if (cull == 3 && !TABLES)
+    return stats ? launch_trace<false, RECORDS, true, 3>(a, st) : launch_trace<false, RECORDS, false, 3>(a, st);
   if (stats) {
     if (cull == 2) return launch_trace<TABLES, RECORDS, true, 2>(a, st);
     return cull ? launch_trace<TABLES, RECORDS, true, 1>(a, st) : launch_trace<TABLES, RECORDS, true, 0>(a, st);
@@ -93,6 +95,7 @@ static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool 
                             cudaStream_t st) {
   // the production path (no records, no statistics) is compiled for 4 resident
   // CTAs per SM (64 registers); variant 3 keeps the unconstrained build
+  if (variant != 3 && !tables && !records && !stats && cull == 3) return launch_trace<false, false, false, 3, 4>(a, st);
   if (variant != 3 && !tables && !records && !stats && cull == 2) return launch_trace<false, false, false, 2, 4>(a, st);
   if (variant != 3 && !tables && !records && !stats && cull) return launch_trace<false, false, false, 1, 4>(a, st);
   if (tables) return records ? dispatch2<true, true>(a, stats, cull, st) : dispatch2<true, false>(a, stats, cull, st);
@@ -124,6 +127,12 @@ void buie_with_guide(float csr, BuieTable* t) {
   }
   t->inv_bucket = inv_bucket;
   t->csr = csr;
+  // the largest angle the sampler returns: the aureole's end (u -> 1) or the
+  // core's last node, computed as the kernel computes it, plus rounding
+  const double core_max = h[1024];
+  const double aur_max = std::pow((double)(t->params[3] - t->params[2]) * t->params[4] + t->params[5],
+                                  1.0 / ((double)t->params[1] + 1.0));
+  t->within_alpha = std::max(core_max, aur_max) * 1e-3 * (1.0 + 1e-5) <= kSunAlphaMax;
 }
 
 static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
@@ -184,6 +193,9 @@ void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, u
     a->gdims[i] = s->gdims[i];
   }
   a->coarse_yr = s->fine_div > 1 ? geo.coarse_yr : nullptr;
+  a->cand = geo.cand;
+  a->cand_n = geo.cand_n;
+  a->rect = geo.rect;
   a->cshift = 0;
   while ((1 << a->cshift) < s->fine_div) ++a->cshift;
   for (int i = 0; i < 3; ++i) {
@@ -220,7 +232,7 @@ static qmcrt_status check_params(const qmcrt_trace_params* p) {
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "reflectivity must be in [0,1]");
   if (p->quirks & ~QMCRT_QUIRKS_REFERENCE) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown quirk bits");
   if (p->deposit != QMCRT_DEPOSIT_NEAREST) return set_error(QMCRT_ERR_NOT_SUPPORTED, "bilinear deposition is only used by the adjoint");
-  if (p->kernel_variant < 0 || p->kernel_variant > 4) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "kernel_variant must be 0..4");
+  if (p->kernel_variant < 0 || p->kernel_variant > 5) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "kernel_variant must be 0..5");
   if (p->attenuation != QMCRT_ATTEN_NONE && p->attenuation != QMCRT_ATTEN_POLY_EXP)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
   return QMCRT_OK;
@@ -245,6 +257,12 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
   // (level 2 adds the coarse level of a two-level grid)
   int cull = p->kernel_variant != 2 && !(p->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS));
   if (cull && a.coarse_yr && p->kernel_variant != 4) cull = 2;
+  // Philox rays of the corrected method test their heliostat's occluder
+  // candidates instead of walking the grid (variants 4 and 5 walk the grid)
+  // (the lists leave out the ray's own heliostat: not under QMCRT_QUIRK_SELF_HIT)
+  if (cull && !tables && a.cand && s->buie.within_alpha && !(p->quirks & QMCRT_QUIRK_SELF_HIT) &&
+      p->kernel_variant != 4 && p->kernel_variant != 5)
+    cull = 3;
   QM_CUDA(dispatch(a, tables, records, stats != nullptr, cull, p->kernel_variant, st));
   QM_CUDA(cudaEventRecord(s->ev[3], st));
   double scale = (double)sun->dni * p->reflectivity * weight_scale / ((double)p->rays_per_point * s->rg.pixel_area);

@@ -26,6 +26,11 @@ struct TraceArgs {
   // grid
   const float4* crect;
   const int4* cinfo;      // [cells] {first, end, ylo, yhi (float bits)}: the cell's run of crect
+  // per-heliostat occluder candidates ([n][2][kCandCap], counts [n][2]) and
+  // the heliostats' own rectangle records [3n]; NULL: walk the grid
+  const int* cand;
+  const int* cand_n;
+  const float4* rect;
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
   int gdims[3];
@@ -115,32 +120,35 @@ __device__ __forceinline__ void sincos_small(float x, float* s, float* c) {
   }
 }
 
-// One grid cell: any rectangle other than `own` hit at t > eps?  The
-// parallelogram test of rayParallelogramIntersect (global_function.cuh:78-105)
-// with the divisions by det folded into the comparisons.
+// Does the ray o + t d hit the parallelogram A, E1, E2 at t > eps?  The test
+// of rayParallelogramIntersect (global_function.cuh:78-105) with the
+// divisions by det folded into the comparisons.
+__device__ __forceinline__ bool rect_hit(float4 r0, float4 r1, float4 r2, float3 o, float3 d) {
+  float3 E1 = f3(r1.x, r1.y, r1.z), E2 = f3(r2.x, r2.y, r2.z);
+  float3 T = f3(o.x - r0.x, o.y - r0.y, o.z - r0.z);
+  float3 pv = cross(d, E2);
+  float det = dot(E1, pv);
+  if (fabsf(det) < kEps) return false;
+  float sg = det < 0.f ? -1.f : 1.f, ad = fabsf(det);
+  float un = dot(T, pv) * sg;
+  if (un < 0.f || un > ad) return false;
+  float3 qv = cross(T, E1);
+  float vn = dot(d, qv) * sg;
+  if (vn < 0.f || vn > ad) return false;
+  float tn = dot(E2, qv) * sg;
+  return tn >= kEps * ad;
+}
+
+// One grid cell (its run [b, e) of cell-major records): any rectangle other
+// than `own` hit?
 template <bool STATS>
 __device__ __forceinline__ bool cell_hit(const TraceArgs& a, int b, int e, float3 o, float3 d, int own, bool selfhit,
                                          uint32_t& ntest) {
   for (int k = b; k < e; ++k) {
     float4 r0 = __ldg(a.crect + 3 * k);
     if (__float_as_int(r0.w) == own && !selfhit) continue;
-    float4 r1 = __ldg(a.crect + 3 * k + 1);
-    float4 r2 = __ldg(a.crect + 3 * k + 2);
     if (STATS) ++ntest;
-    float3 E1 = f3(r1.x, r1.y, r1.z), E2 = f3(r2.x, r2.y, r2.z);
-    float3 T = f3(o.x - r0.x, o.y - r0.y, o.z - r0.z);
-    float3 pv = cross(d, E2);
-    float det = dot(E1, pv);
-    if (fabsf(det) < kEps) continue;
-    float sg = det < 0.f ? -1.f : 1.f, ad = fabsf(det);
-    float un = dot(T, pv) * sg;
-    if (un < 0.f || un > ad) continue;
-    float3 qv = cross(T, E1);
-    float vn = dot(d, qv) * sg;
-    if (vn < 0.f || vn > ad) continue;
-    float tn = dot(E2, qv) * sg;
-    if (tn < kEps * ad) continue;
-    return true;
+    if (rect_hit(r0, __ldg(a.crect + 3 * k + 1), __ldg(a.crect + 3 * k + 2), o, d)) return true;
   }
   return false;
 }
@@ -264,6 +272,25 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
     if (!may_hit(ci, tin, fminf(tx, fminf(ty, tz)))) continue;
     if (STATS) ++ncell;
     if (cell_hit<STATS>(a, ci.x, ci.y, o, d, own, selfhit, ntest)) return true;
+  }
+  return false;
+}
+
+// Any-hit over heliostat h's occluder candidates for one walk (which = 0:
+// toward the sun, 1: after the reflection).  Every heliostat a ray of h can
+// meet is in the list, so the answer is the grid walk's; all lanes of a warp
+// share h, so they run the same candidates with broadcast loads.  A list that
+// overflowed, or no lists (cand_n NULL), falls back to the grid walk.
+template <bool STATS>
+__device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int which, float3 o, float3 d, float fy0,
+                                             float fy1, uint32_t& ntest, uint32_t& ncell) {
+  const int m = a.cand_n ? __ldg(a.cand_n + 2 * h + which) : kCandCap + 1;  // no lists: walk
+  if (m > kCandCap) return dda_blocked<STATS, true>(a, o, d, h, fy0, fy1, ntest, ncell);
+  const int* L = a.cand + (2 * h + which) * kCandCap;
+  for (int i = 0; i < m; ++i) {
+    const int k = __ldg(L + i);
+    if (STATS) ++ntest;
+    if (rect_hit(__ldg(a.rect + 3 * k), __ldg(a.rect + 3 * k + 1), __ldg(a.rect + 3 * k + 2), o, d)) return true;
   }
   return false;
 }
@@ -423,7 +450,8 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float* s_tab
 
 // One ray: the body of map_tracing (rectgrid_raytracing.cu:164-195).
 // CULL: 0 no culling, 1 vertical culling, 2 vertical culling on both levels
-// of a two-level grid.
+// of a two-level grid, 3 the per-heliostat occluder candidates (Philox
+// sampling only: their cones bound the sampler's directions).
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep>
 __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit) {
@@ -447,9 +475,12 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab
   uint8_t flag = 0;
   int pix = -1;
   double th = 0.0;
-  if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, f3((float)-ws.x, (float)-ws.y, (float)-ws.z), h, fy0, fy1, c.test, c.cell)) {
+  const float3 sdir = f3((float)-ws.x, (float)-ws.y, (float)-ws.z);
+  if (CULL == 3 ? list_blocked<STATS>(a, h, 0, of, sdir, fy0, fy1, c.test, c.cell)
+                : dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, sdir, h, fy0, fy1, c.test, c.cell)) {
     flag = QMCRT_RAY_SHADOWED;
-  } else if (dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
+  } else if (CULL == 3 ? list_blocked<STATS>(a, h, 1, of, to_f(rd), fy0, fy1, c.test, c.cell)
+                       : dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
     flag = QMCRT_RAY_BLOCKED;
   } else if (receiver_hit(a, o, rd, pix, &th)) {
     flag = QMCRT_RAY_HIT;

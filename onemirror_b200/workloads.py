@@ -78,6 +78,25 @@ def layout(n, w, h, r_min, r_max, az_center=0.0, az_span=120.0, spacing=0.0, jit
     return pos
 
 
+def paraboloid_facets(a, b, normal, centre, rows=3, cols=3, facet=2 ** 0.5 / 3, gap=0.1, thickness=0.1,
+                      reference_frame=False):
+    """Facets of one paraboloid heliostat (qmcrt_layout_paraboloid_facets):
+    pos, size and unit normals [rows*cols, 3]; the defaults are the
+    reference's own 3 x 3 heliostat."""
+    p = capi.FacetParams()
+    p.a, p.b = a, b
+    p.normal[:] = list(normal)
+    p.centre[:] = list(centre)
+    p.rows, p.cols, p.facet, p.gap, p.thickness = rows, cols, facet, gap, thickness
+    p.reference_frame = 1 if reference_frame else 0
+    n = rows * cols
+    pos, size, nrm = (np.zeros((n, 3), np.float32) for _ in range(3))
+    got = C.c_int32()
+    capi.check(capi.lib().qmcrt_layout_paraboloid_facets(C.byref(p), capi.as_fp(pos), capi.as_fp(size),
+                                                         capi.as_fp(nrm), n, C.byref(got)))
+    return pos, size, nrm
+
+
 def sun_dir(elev, azim):
     d = (C.c_float * 3)()
     capi.check(capi.lib().qmcrt_sun_direction(elev, azim, d))

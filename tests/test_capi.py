@@ -11,7 +11,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from onemirror_b200 import capi
+from onemirror_b200 import capi, workloads as W
 from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -146,3 +146,55 @@ def test_scn_parser_errors(tmp_path):
     bad.write_text("Recv 0\npos 0 1 2\nend\nGrid 0\ninter 1 1 1\nn 2\nend\ngap 0 0\nmatrix 1 1\nhelio 0 0 0\n1 0.1 1\n")
     assert L.qmcrt_scn_parse(str(bad).encode(), None, None, None, None, 0, C.byref(n)) == capi.ERR_INVALID_ARGUMENT
     assert b"declares 2" in L.qmcrt_last_error()
+
+
+def _reference_facets(a, b, n, centre):
+    """The 3 x 3 facet layout of SceneFileProc::SceneFileRead
+    (scene_file_proc.cpp:288-341) restated in float64: centres on the local
+    lattice +-(sqrt(2)/3 + 0.1), heights x^2/a^2 + z^2/b^2, the frame
+    mirrorToGround with e1 = (n.z, 0, -n.x) / sqrt(n.x^2 + n.y^2) (sign by
+    n.z), n, e1 x n, and normals (-2x/a^2, 1, -2z/b^2) through the same frame."""
+    d = np.sqrt(2.0) / 3 + 0.1
+    cx = np.array([-d, 0, d] * 3)
+    cz = np.repeat([-d, 0.0, d], 3)
+    cy = cx * cx / a / a + cz * cz / b / b
+    t = np.sqrt(n[0] ** 2 + n[1] ** 2)
+    if n[2] > 0:
+        e1 = np.array([n[2] / t, 0, -n[0] / t])
+    elif n[2] < 0:
+        e1 = np.array([-n[2] / t, 0, n[0] / t])
+    else:
+        e1 = np.array([0.0, 0, 1])
+    M = np.stack([e1, n, np.cross(e1, n)], 1)
+    pos = (M @ np.stack([cx, cy, cz])).T + centre
+    nrm = (M @ np.stack([-2 * cx / a / a, np.ones(9), -2 * cz / b / b])).T
+    return pos, nrm / np.linalg.norm(nrm, axis=1, keepdims=True)
+
+
+def test_paraboloid_facets_reproduce_the_reference_layout():
+    n = np.array([0.3, 0.9, -0.2])
+    n /= np.linalg.norm(n)
+    centre = np.array([1.0, 2.0, 100.0])
+    pos, size, nrm = W.paraboloid_facets(8.0, 8.0, n, centre, reference_frame=True)
+    rp, rn = _reference_facets(8.0, 8.0, n.astype(np.float32).astype(np.float64), centre)
+    assert np.allclose(pos, rp, atol=2e-5) and np.allclose(nrm, rn, atol=1e-6)
+    assert np.allclose(size, [[np.sqrt(2) / 3, 0.1, np.sqrt(2) / 3]] * 9, atol=1e-7)
+
+
+def test_paraboloid_facets_corrected_frame_geometry():
+    n = np.array([0.3, 0.9, -0.2])
+    n /= np.linalg.norm(n)
+    centre = np.array([1.0, 2.0, 100.0])
+    pos, size, nrm = W.paraboloid_facets(6.0, 9.0, n, centre, rows=3, cols=5, facet=0.5, gap=0.05)
+    e1 = np.array([-n[2], 0, n[0]]) / np.hypot(n[0], n[2])  # n.z < 0 branch
+    e2 = np.cross(e1, n)
+    rel = pos.astype(np.float64) - centre
+    x, y, z = rel @ e1, rel @ n, rel @ e2
+    assert np.allclose(y, x * x / 36 + z * z / 81, atol=2e-5)
+    assert np.allclose(np.unique(np.round(x, 4)), (np.arange(5) - 2) * 0.55, atol=1e-4)
+    assert np.allclose(np.linalg.norm(nrm, axis=1), 1, atol=1e-6)
+    g = np.stack([-2 * x / 36, np.ones_like(x), -2 * z / 81], 1)
+    gw = g[:, :1] * e1 + g[:, 1:2] * n + g[:, 2:] * e2
+    assert np.allclose(nrm, gw / np.linalg.norm(gw, axis=1, keepdims=True), atol=1e-6)
+    with pytest.raises(capi.QmcrtError):
+        W.paraboloid_facets(0.0, 8.0, n, centre)

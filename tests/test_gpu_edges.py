@@ -149,3 +149,25 @@ def test_rejected_fields_and_grids():
     bad = W.grid(0.0)
     with pytest.raises(capi.QmcrtError):
         SolarScene(w.pos, w.size, w.receiver, bad)
+
+
+def test_faceted_paraboloid_heliostat():
+    """The reference's own kind of scene (scene_file_proc.cpp:288-341, 422-444):
+    one heliostat of 3 x 3 canted facets on a paraboloid, 100 m south of a
+    1.4 x 1.4 m receiver facing +z; each facet is a rectangle with its given
+    normal."""
+    sun = W.make_sun(50.0, 180.0)
+    sd = np.array(sun.dir[:], np.float64)
+    centre = np.array([0.0, 4.0, 100.0])
+    aim = np.array([0.0, 13.0, 0.0])
+    to_rec = (aim - centre) / np.linalg.norm(aim - centre)
+    n = to_rec - sd / np.linalg.norm(sd)
+    n /= np.linalg.norm(n)
+    pos, size, nrm = W.paraboloid_facets(20.0, 20.0, n, centre)
+    rec = W.flat_receiver(13.0, 1.4, 1.4, 140, 140, normal=(0.0, 0.0, 1.0))
+    w = W.Workload("facets", pos, size, 0.001, rec, W.grid(1.0), sun, W.params(9 * 64 * 256, 256, 0.03, seed=31))
+    sc = SolarScene(pos, size, rec, w.grid, sigma=w.sigma, normal=nrm)
+    g, o = trace_pair(w, sc, sun, w.params)
+    check_pair(w, g, o)
+    assert g["stats"].intercept_ratio > 0.5
+    sc.close()

@@ -297,6 +297,7 @@ def test_two_level_grid_equals_its_fine_level():
     gi = sc.grid_info()
     assert gi.fine_div == 4 and list(gi.cell) == [12.5, 12.5, 12.5]
     assert all(d % 4 == 0 for d in gi.dims)
+    w.params.kernel_variant = 5  # walk the grid (not the candidate lists)
     g2 = sc.trace(w.sun, w.params, records=True)
     f2, p2, c2 = g2["flags"].clone(), g2["pixel"].clone(), g2["counts"].clone()
     w.params.kernel_variant = 4
@@ -307,7 +308,7 @@ def test_two_level_grid_equals_its_fine_level():
     # production kernels (no records, no statistics; separately compiled, so
     # the compiler's FMA contraction may differ and a ray on a rectangle edge
     # may flip): the same maps up to a few such rays
-    w.params.kernel_variant = 0
+    w.params.kernel_variant = 5
     m2 = sc.trace(w.sun, w.params, stats=False)["counts"].clone()
     w.params.kernel_variant = 4
     m1 = sc.trace(w.sun, w.params, stats=False)["counts"]
@@ -342,6 +343,25 @@ def test_attenuation_equals_oracle(name):
     assert torch.equal(g0["counts"], g["counts"])
     r = (g["energy"].double().sum() / g0["energy"].double().sum()).item()
     assert (0.9 if name == "small" else 0.8) < r < 0.99, r
+    sc.close()
+
+
+@pytest.mark.parametrize("name,elev", [("small", 45.0), ("small", 12.0), ("mid", 30.0), ("mid", 8.0), ("large", 20.0)])
+def test_candidate_lists_equal_the_grid_walk(name, elev):
+    """Philox rays test only their heliostat's occluder candidates (the
+    heliostats a cone bounding the sampler's directions can reach); every
+    flag, pixel and count equals the grid walk's (kernel_variant 5), and only
+    rays of overflowing lists walk cells."""
+    w = W.small() if name == "small" else W.BUILDERS[name](rays=1 << 22)
+    sun = W.make_sun(elev, 200.0, 1000.0, w.sun.csr)
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    g = sc.trace(sun, p, records=True)
+    f, px, cnt = g["flags"].clone(), g["pixel"].clone(), g["counts"].clone()
+    p.kernel_variant = 5
+    g5 = sc.trace(sun, p, records=True)
+    assert torch.equal(f, g5["flags"]) and torch.equal(px, g5["pixel"]) and torch.equal(cnt, g5["counts"])
+    assert g["stats"].dda_cells < g5["stats"].dda_cells  # only overflowing lists walk
     sc.close()
 
 
