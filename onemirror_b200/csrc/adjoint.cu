@@ -222,7 +222,7 @@ __global__ void loss_kernel(LossArgs a) {
 __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(s * a.x + b.x, s * a.y + b.y, s * a.z + b.z); }
 
 template <bool CULL>
-__global__ void __launch_bounds__(kAdjThreads) adjoint_backward_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const AdjArgs A) {
   __shared__ float s_tab[1025 + 1025 + 1024];
   __shared__ int s_guide[kBuieBuckets];
   const TraceArgs& a = A.t;
@@ -326,11 +326,16 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_backward_kernel(const Adj
   }
 }
 
-static int adj_blocks(uint64_t rays) {
-  int dev = 0, sms = 148;
+// Grid of a grid-stride adjoint kernel: as many CTAs as stay resident
+// together (more would leave the last ones running nearly alone).
+template <class K>
+static int adj_blocks(K kernel, uint64_t rays) {
+  int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * 4, (rays + kAdjThreads - 1) / kAdjThreads));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAdjThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * per_sm, (rays + kAdjThreads - 1) / kAdjThreads));
 }
 
 }  // namespace qm
@@ -408,7 +413,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.t.b_C = t->buie.params[5];
   A.t.b_inv = 1 / (t->buie.params[1] + 1);
   A.t.b_inv_bucket = t->buie.inv_bucket;
-  if (!t->buie.within_alpha) A.t.cand = A.t.cand_n = nullptr;  // walk the grid
+  if (!t->buie.within_alpha) { A.t.cand = nullptr; A.t.cand_n = nullptr; }  // walk the grid
   A.t.rays = (uint32_t)p->rays;
   A.t.rpp = p->rays_per_point;
   A.t.rpp_shift = (A.t.rpp & (A.t.rpp - 1)) ? -1 : __builtin_ctz((unsigned)A.t.rpp);
@@ -432,7 +437,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.saved = saved;
   A.G = t->d_G;
   A.jac = t->d_jac;
-  const int blocks = adj_blocks(p->rays);
+  const int blocks = adj_blocks(adjoint_forward_kernel<true>, p->rays);
   QM_CUDA(cudaMemcpyAsync(t->d_buie, t->buie.host.data(), t->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
   QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
@@ -466,7 +471,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   A.t.b_C = t->buie.params[5];
   A.t.b_inv = 1 / (t->buie.params[1] + 1);
   A.t.b_inv_bucket = t->buie.inv_bucket;
-  if (!t->buie.within_alpha) A.t.cand = A.t.cand_n = nullptr;
+  if (!t->buie.within_alpha) { A.t.cand = nullptr; A.t.cand_n = nullptr; }
   A.t.rays = t->args.t.rays;
   A.t.rpp = t->args.t.rpp;
   A.t.rpp_shift = t->args.t.rpp_shift;
@@ -496,7 +501,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   QM_CUDA(cudaMemsetAsync(d_grad_tilt, 0, 2 * (size_t)s->n * sizeof(float), st));
   frame_jacobian_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(j);
   QM_CUDA(cudaGetLastError());
-  adjoint_backward_kernel<true><<<adj_blocks(A.t.rays), kAdjThreads, 0, st>>>(A);
+  adjoint_backward_kernel<true><<<adj_blocks(adjoint_backward_kernel<true>, A.t.rays), kAdjThreads, 0, st>>>(A);
   QM_CUDA(cudaGetLastError());
   return QMCRT_OK;
 }

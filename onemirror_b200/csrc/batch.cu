@@ -356,7 +356,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     fill_trace_args(it.scene, it.geo, &it.sun, 0, &a);
     const BuieTable& t = b->tables[csr];
     a.buie = b->d_tables[csr];
-    if (!t.within_alpha) a.cand = a.cand_n = nullptr;  // the item's rays walk the grid
+    if (!t.within_alpha) { a.cand = nullptr; a.cand_n = nullptr; }  // the item's rays walk the grid
     a.b_total = t.params[3];
     a.b_core = t.params[2];
     a.b_B = t.params[4];

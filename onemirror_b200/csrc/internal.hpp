@@ -66,7 +66,7 @@ struct SunGeom {
   float4* cell_rect = nullptr;   // [3*entry_cap]
   int4* cell_info = nullptr;     // [cells] first, end, ylo bits, yhi bits
   float2* coarse_yr = nullptr;   // [coarse_cells] two-level grid only
-  int* cand = nullptr;           // [n][2][kCandCap] occluder candidates of each heliostat's shadow / block rays
+  float4* cand = nullptr;        // [n][2][kCandCap][3] rectangle records of each heliostat's shadow / block candidates
   int* cand_n = nullptr;         // [n][2] their counts (> kCandCap: too many, the rays walk the grid)
   int* field_yr = nullptr;       // [2]
   double* power = nullptr;       // [1] sum |n . sun| * A
@@ -125,7 +125,7 @@ struct qmcrt_scene {
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
   int4* d_cell_info = nullptr;      // [cells] run of each cell's rectangles and their height range
   float2* d_coarse_yr = nullptr;    // [coarse_cells] the same per coarse cell (two-level grid)
-  int* d_cand = nullptr;            // [n][2][kCandCap] occluder candidates (shadow, block)
+  float4* d_cand = nullptr;         // [n][2][kCandCap][3] occluder candidates' rectangle records (shadow, block)
   int* d_cand_n = nullptr;          // [n][2]
   int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)
   qm::SunKey sun_key;

@@ -255,7 +255,8 @@ struct CandArgs {
   double sun[3];      // incident direction, unit
   double sun_alpha;   // largest angle of a sun sample from the sun axis (rad)
   double zmax;        // largest |z| of the slope deviate, in units of sigma
-  int* cand;          // [n][2][kCandCap]
+  const float4* rect;  // [3n] every heliostat's rectangle record
+  float4* cand;        // [n][2][kCandCap][3] the candidates' records, inline
   int* cand_n;        // [n][2]
 };
 
@@ -292,8 +293,8 @@ __global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
   const double as = a.sun_alpha + 1e-6, ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
   const double ts = tan(as), tb = tan(ab);
   const double ys = sin(asin(fmin(fmax(ds.y, -1.0), 1.0)) - as), yb = sin(asin(fmin(fmax(db.y, -1.0), 1.0)) - ab);
-  int* Ls = a.cand + (int64_t)2 * h * kCandCap;
-  int* Lb = Ls + kCandCap;
+  float4* Ls = a.cand + (int64_t)2 * h * kCandCap * 3;
+  float4* Lb = Ls + kCandCap * 3;
   int ns = 0, nb = 0;
   const unsigned below = (1u << lane) - 1u;
   for (int k0 = 0; k0 < a.n; k0 += 32) {
@@ -308,11 +309,13 @@ __global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
     const unsigned ms = __ballot_sync(0xffffffffu, rs), mb = __ballot_sync(0xffffffffu, rb);
     if (rs) {
       const int slot = ns + __popc(ms & below);
-      if (slot < kCandCap) Ls[slot] = k;
+      if (slot < kCandCap)
+        for (int j = 0; j < 3; ++j) Ls[3 * slot + j] = a.rect[3 * k + j];
     }
     if (rb) {
       const int slot = nb + __popc(mb & below);
-      if (slot < kCandCap) Lb[slot] = k;
+      if (slot < kCandCap)
+        for (int j = 0; j < 3; ++j) Lb[3 * slot + j] = a.rect[3 * k + j];
     }
     ns += __popc(ms);
     nb += __popc(mb);
@@ -549,7 +552,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
   GALLOC(g->cell_rect, 3 * (size_t)s->entry_cap);
   GALLOC(g->cell_info, (size_t)s->cells);
   if (s->coarse_cells) GALLOC(g->coarse_yr, (size_t)s->coarse_cells);
-  GALLOC(g->cand, 2 * kCandCap * n);
+  GALLOC(g->cand, 2 * 3 * kCandCap * n);
   GALLOC(g->cand_n, 2 * n);
   GALLOC(g->field_yr, 2);
   GALLOC(g->power, 1);
@@ -599,6 +602,7 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   for (int i = 0; i < 3; ++i) ca.sun[i] = sun[i];
   ca.sun_alpha = kSunAlphaMax;
   ca.zmax = kSlopeZMax;
+  ca.rect = g.rect;
   ca.cand = g.cand;
   ca.cand_n = g.cand_n;
   cand_kernel<<<(s->n + 3) / 4, 128, 0, st>>>(ca);
@@ -840,7 +844,7 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_cell_rect, 3 * (size_t)cap);
   ALLOC(s->d_cell_info, (size_t)s->cells);
   if (s->coarse_cells) ALLOC(s->d_coarse_yr, (size_t)s->coarse_cells);
-  ALLOC(s->d_cand, 2 * kCandCap * n);
+  ALLOC(s->d_cand, 2 * 3 * kCandCap * n);
   ALLOC(s->d_cand_n, 2 * n);
   ALLOC(s->d_field_yr, 2);
   ALLOC(s->d_helio_weight, n);

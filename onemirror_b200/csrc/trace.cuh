@@ -1,5 +1,6 @@
 // trace.cuh — device side of the tracer: arguments, Buie sampling, the FP32
-// 3D-DDA any-hit traversal, the FP64 receiver intersection and the kernel.
+// any-hit tests (per-heliostat occluder candidates, or the 3D-DDA grid walk),
+// the FP64 receiver intersection and the kernel.
 #pragma once
 #include <stdint.h>
 
@@ -26,11 +27,12 @@ struct TraceArgs {
   // grid
   const float4* crect;
   const int4* cinfo;      // [cells] {first, end, ylo, yhi (float bits)}: the cell's run of crect
-  // per-heliostat occluder candidates ([n][2][kCandCap], counts [n][2]) and
-  // the heliostats' own rectangle records [3n]; NULL: walk the grid
-  const int* cand;
-  const int* cand_n;
-  const float4* rect;
+  // per-heliostat occluder candidates: for each heliostat and walk (shadow,
+  // block) the candidates' rectangle records inline, and their counts
+  // (> kCandCap: the list overflowed); NULL: walk the grid
+  const float4* cand;   // [n][2][kCandCap][3]
+  const int* cand_n;    // [n][2]
+  const float4* rect;   // [3n] every heliostat's own rectangle record
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
   int gdims[3];
@@ -286,11 +288,10 @@ __device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int whic
                                              float fy1, uint32_t& ntest, uint32_t& ncell) {
   const int m = a.cand_n ? __ldg(a.cand_n + 2 * h + which) : kCandCap + 1;  // no lists: walk
   if (m > kCandCap) return dda_blocked<STATS, true>(a, o, d, h, fy0, fy1, ntest, ncell);
-  const int* L = a.cand + (2 * h + which) * kCandCap;
+  const float4* L = a.cand + (size_t)(2 * h + which) * (kCandCap * 3);
   for (int i = 0; i < m; ++i) {
-    const int k = __ldg(L + i);
     if (STATS) ++ntest;
-    if (rect_hit(__ldg(a.rect + 3 * k), __ldg(a.rect + 3 * k + 1), __ldg(a.rect + 3 * k + 2), o, d)) return true;
+    if (rect_hit(__ldg(L + 3 * i), __ldg(L + 3 * i + 1), __ldg(L + 3 * i + 2), o, d)) return true;
   }
   return false;
 }
