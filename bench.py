@@ -247,20 +247,21 @@ def adjoint_section(reps=5):
     outs = sc._outputs(0, False)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     tf, tb, tp = [], [], []
+    tape = None  # one tape for all iterations, as an optimisation loop would keep it
     for it in range(reps + 2):
         ev[0].record()
         sc.trace(w.sun, plain_p, stats=False, outputs=outs)
         ev[1].record()
-        tape, _, _ = sc.adjoint_forward(w.sun, w.params, target, want_loss=False, flux=False)
+        tape, _, _ = sc.adjoint_forward(w.sun, w.params, target, want_loss=False, flux=False, tape=tape)
         ev[2].record()
         sc.adjoint_backward(tape)
         ev[3].record()
         ev[3].synchronize()
-        SolarScene.tape_free(tape)
         if it >= 2:
             tp.append(ev[0].elapsed_time(ev[1]))
             tf.append(ev[1].elapsed_time(ev[2]))
             tb.append(ev[2].elapsed_time(ev[3]))
+    SolarScene.tape_free(tape)
     sc.close()
     f, b, p = statistics.median(tf), statistics.median(tb), statistics.median(tp)
     return {"heliostats": w.n, "rays": int(w.params.rays), "params": 4 * w.n, "plain_trace_ms": p,

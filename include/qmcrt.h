@@ -460,7 +460,12 @@ qmcrt_status qmcrt_batch_read(qmcrt_batch* batch, int32_t item, uint32_t* h_coun
  * the cap recompute their visibility in the backward pass), writes the flux
  * map to d_flux (may be NULL) and, if `loss` is not NULL, synchronises and
  * returns L.  qmcrt_adjoint_backward writes d_grad_aim [2n] and d_grad_tilt
- * [2n] (device). */
+ * [2n] (device).
+ * `tape` is in/out: *tape == NULL makes a new tape; a tape returned by an
+ * earlier call on the same scene is reused, its device buffers kept where
+ * they are large enough (an optimisation loop then allocates nothing after
+ * its first step).  Reuse it on the stream it last ran on, or after that
+ * stream has finished with it. */
 qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* scene, const qmcrt_sun* sun, const qmcrt_trace_params* params,
                                    const float* d_target, uint64_t state_bytes_max, float* d_flux, double* loss,
                                    qmcrt_tape** tape, void* stream);

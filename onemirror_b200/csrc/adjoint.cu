@@ -173,8 +173,11 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_forward_kernel(const AdjA
   load_buie(a.buie, s_tab, s_guide);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride) {
+  // chunks of consecutive rays taken grid-stride, as in the plain tracer
+  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = ((uint64_t)a.rays + chunk - 1) / chunk;
+  for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x)
+  for (uint64_t r64 = ch * chunk + threadIdx.x, r1 = min((ch + 1) * chunk, (uint64_t)a.rays); r64 < r1;
+       r64 += blockDim.x) {
     const uint32_t ray = (uint32_t)r64;
     RaySetup R;
     ray_setup<false>(a, s_tab, s_guide, ray, R);
@@ -232,9 +235,11 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
   const float3 E1 = f3((float)a.rE1[0], (float)a.rE1[1], (float)a.rE1[2]);
   const float3 E2 = f3((float)a.rE2[0], (float)a.rE2[1], (float)a.rE2[2]);
   const float3 sd = f3((float)a.sdir[0], (float)a.sdir[1], (float)a.sdir[2]);
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t end = ((uint64_t)a.rays + 31) / 32 * 32;  // whole warps keep the shuffles converged
-  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < end; r64 += stride) {
+  // chunks of consecutive rays (a multiple of 32) taken grid-stride
+  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = (end + chunk - 1) / chunk;
+  for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x)
+  for (uint64_t r64 = ch * chunk + threadIdx.x, r1 = min((ch + 1) * chunk, end); r64 < r1; r64 += blockDim.x) {
     float gk[4] = {0.f, 0.f, 0.f, 0.f};
     int h = -1;
     if (r64 < a.rays) {
@@ -353,6 +358,10 @@ struct qmcrt_tape {
   double* d_loss = nullptr;
   float* d_energy = nullptr;
   bool cull = true;
+  // capacities, so that a tape passed back to qmcrt_adjoint_forward reuses its buffers
+  uint64_t cap_tape = 0;
+  int64_t cap_res = 0;
+  int cap_n = 0;
 };
 
 namespace qm {
@@ -371,7 +380,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
                                    const float* d_target, uint64_t state_bytes_max, float* d_flux, double* loss,
                                    qmcrt_tape** tape, void* stream) {
   if (!s || !sun || !p || !d_target || !tape) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
-  *tape = nullptr;
+  if (*tape && (*tape)->scene != s) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "a tape is reused only on its own scene");
   if (s->rg.type != QMCRT_RECEIVER_FLAT) return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint needs a flat receiver");
   if (p->deposit != QMCRT_DEPOSIT_BILINEAR) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "the adjoint deposits bilinearly");
   if (p->point_mode != QMCRT_POINTS_POISSON || p->rays == 0 || p->rays > 0xFFFFFFFFull)
@@ -382,27 +391,47 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint has no attenuation term");
   if (!(sun->csr > 0.f && sun->csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   cudaStream_t st = (cudaStream_t)stream;
-  qmcrt_tape* t = new qmcrt_tape();
+  // a tape from an earlier call keeps its buffers where they are large enough
+  const bool fresh = *tape == nullptr;
+  qmcrt_tape* t = fresh ? new qmcrt_tape() : *tape;
+  auto fail = [&](qmcrt_status e) {
+    if (fresh) qmcrt_tape_free(t);
+    return e;
+  };
   t->scene = s;
   t->sun = *sun;
   t->params = *p;
   qmcrt_status e;
   int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
   uint64_t saved = state_bytes_max == 0 ? p->rays : std::min<uint64_t>(p->rays, state_bytes_max);
-  cudaError_t ce = cudaMalloc(&t->d_tape, std::max<uint64_t>(saved, 1));
-  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_G, res * sizeof(float));
-  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_jac, 36 * (size_t)s->n * sizeof(float));
-  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_loss, sizeof(double));
-  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_energy, res * sizeof(float));
-  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_buie, (1025 + 1025 + 1024 + kBuieBuckets) * sizeof(float));
-  if (ce != cudaSuccess) {
-    qmcrt_tape_free(t);
-    return cuda_error(ce, "adjoint tape allocation");
+  cudaError_t ce = cudaSuccess;
+  if (saved > t->cap_tape) {
+    cudaFree(t->d_tape);
+    t->d_tape = nullptr;
+    t->cap_tape = 0;
+    ce = cudaMalloc(&t->d_tape, std::max<uint64_t>(saved, 1));
+    if (ce == cudaSuccess) t->cap_tape = saved;
   }
-  if ((e = tape_geometry(t, st))) {
-    qmcrt_tape_free(t);
-    return e;
+  if (ce == cudaSuccess && res > t->cap_res) {
+    cudaFree(t->d_G);
+    cudaFree(t->d_energy);
+    t->d_G = t->d_energy = nullptr;
+    t->cap_res = 0;
+    ce = cudaMalloc(&t->d_G, res * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMalloc(&t->d_energy, res * sizeof(float));
+    if (ce == cudaSuccess) t->cap_res = res;
   }
+  if (ce == cudaSuccess && s->n > t->cap_n) {
+    cudaFree(t->d_jac);
+    t->d_jac = nullptr;
+    t->cap_n = 0;
+    ce = cudaMalloc(&t->d_jac, 36 * (size_t)s->n * sizeof(float));
+    if (ce == cudaSuccess) t->cap_n = s->n;
+  }
+  if (ce == cudaSuccess && !t->d_loss) ce = cudaMalloc(&t->d_loss, sizeof(double));
+  if (ce == cudaSuccess && !t->d_buie) ce = cudaMalloc(&t->d_buie, (1025 + 1025 + 1024 + kBuieBuckets) * sizeof(float));
+  if (ce != cudaSuccess) return fail(cuda_error(ce, "adjoint tape allocation"));
+  if ((e = tape_geometry(t, st))) return fail(e);
   buie_with_guide(sun->csr, &t->buie);
   AdjArgs& A = t->args;
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &A.t);
@@ -438,6 +467,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.G = t->d_G;
   A.jac = t->d_jac;
   const int blocks = adj_blocks(adjoint_forward_kernel<true>, p->rays);
+  *tape = t;  // from here on the caller owns it, also when a launch below fails
   QM_CUDA(cudaMemcpyAsync(t->d_buie, t->buie.host.data(), t->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
   QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
@@ -452,7 +482,6 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
     QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
     QM_CUDA(cudaStreamSynchronize(st));
   }
-  *tape = t;
   return QMCRT_OK;
 }
 

@@ -11,6 +11,7 @@ namespace qm {
 
 constexpr int kTraceThreads = 256;
 constexpr int kBuieBuckets = 1024;  // guide-table buckets over the core CDF
+constexpr int kChunkBlocks = 16;    // rays per CTA chunk = kChunkBlocks x blockDim
 
 struct TraceArgs {
   // sun: frame of local2world for the sun direction, and the direction
@@ -524,9 +525,16 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   }
   RayCounters c;
   const GlobalDeposit dep{a.counts, a.energy};
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t r64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r64 < a.rays; r64 += stride)
-    trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep);
+  // chunks of kChunkBlocks x 256 consecutive rays (16 sample points at 256
+  // rays per point) taken grid-stride: a CTA stays on one heliostat for most
+  // of a chunk, so its frame and candidates stay in L1, and the chunks are
+  // small enough to keep the SMs evenly loaded
+  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = ((uint64_t)a.rays + chunk - 1) / chunk;
+  for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const uint64_t r1 = min((ch + 1) * chunk, (uint64_t)a.rays);
+    for (uint64_t r64 = ch * chunk + threadIdx.x; r64 < r1; r64 += blockDim.x)
+      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep);
+  }
   if (STATS) flush_counters(c, a.stats);
 }
 

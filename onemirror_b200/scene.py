@@ -167,10 +167,11 @@ class SolarScene:
         r["stats"] = st
         return r
 
-    def adjoint_forward(self, sun, params, target, state_bytes_max=0, want_loss=True, flux=True):
+    def adjoint_forward(self, sun, params, target, state_bytes_max=0, want_loss=True, flux=True, tape=None):
         """Bilinear forward pass + loss against `target` (device [res] W/m^2).
-        Returns (tape, loss or None, flux map or None)."""
-        tape = C.c_void_p()
+        Returns (tape, loss or None, flux map or None); pass the tape of an
+        earlier call back in to reuse its device buffers."""
+        tape = C.c_void_p(tape.value if isinstance(tape, C.c_void_p) else tape)
         loss = C.c_double()
         fl = torch.zeros(self.res, dtype=torch.float32, device="cuda") if flux else None
         capi.check(capi.lib().qmcrt_adjoint_forward(self.h, C.byref(sun), C.byref(params), _ptr(target),

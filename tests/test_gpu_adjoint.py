@@ -133,3 +133,27 @@ def test_adjoint_argument_errors(case):
     with pytest.raises(capi.QmcrtError) as e:
         sc.adjoint_forward(w.sun, p, target)
     assert e.value.status == capi.ERR_NOT_SUPPORTED
+
+
+def test_reused_tape_gives_the_same_gradients(case):
+    """A tape passed back to qmcrt_adjoint_forward keeps its buffers; the
+    results equal those of a fresh tape.  A tape is refused on another scene."""
+    w, sc, target = case
+    loss0, flux0, g0 = gpu_grad(sc, w, target)
+    tape, loss1, _ = sc.adjoint_forward(w.sun, w.params, target)
+    for _ in range(2):
+        tape, loss2, flux2 = sc.adjoint_forward(w.sun, w.params, target, tape=tape)
+    ga, gt = sc.adjoint_backward(tape)
+    g2 = np.concatenate([ga.cpu().numpy(), gt.cpu().numpy()], 1)
+    # float atomics deposit in no fixed order: the last bits vary between runs
+    assert abs(loss1 - loss2) <= 1e-7 * loss0 and abs(loss2 - loss0) <= 1e-7 * loss0
+    assert np.allclose(flux2.cpu().numpy(), flux0, rtol=0, atol=1e-6 * flux0.max())
+    assert np.allclose(g2, g0, rtol=1e-5, atol=1e-6 * np.abs(g0).max())
+    other = W.differentiable(n=50, rays=1 << 16)
+    sc2 = SolarScene(other.pos, other.size, other.receiver, other.grid, sigma=other.sigma, aim=other.aim.copy(),
+                     tilt=other.extra["tilt"].copy())
+    t2 = torch.as_tensor(other.extra["target"], device="cuda")
+    with pytest.raises(capi.QmcrtError):
+        sc2.adjoint_forward(other.sun, other.params, t2, tape=tape)
+    SolarScene.tape_free(tape)
+    sc2.close()
