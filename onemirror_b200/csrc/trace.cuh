@@ -468,10 +468,14 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab
   const int h = R.h;
   const d3 o = R.o, ws = R.ws;
   const float3 of = to_f(o);
-  // perturbed normal, reflected direction (i - 2 n (n.i), normalised) and
-  // energy first, so that the mirror frame is dead before the walks
+  // perturbed normal, reflected direction (i - 2 n (n.i)) and energy first,
+  // so that the mirror frame is dead before the walks.  The reflection keeps
+  // the length of ws (1 to float rounding of the sample), and nothing that
+  // uses rd depends on its length beyond that: the receiver's (u, v), the
+  // rectangle tests and the walk's cell order are scale-free, the slant range
+  // for attenuation moves by ~1e-7 relative; so rd is not renormalised.
   const d3 np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
-  const d3 rd = rnorm(ws - (2.0 * dot(ws, np)) * np);
+  const d3 rd = ws - (2.0 * dot(ws, np)) * np;
   // calEnergy (rectgrid_raytracing.cu:129-133)
   const float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * R.w;
   uint8_t flag = 0;
