@@ -279,6 +279,60 @@ __device__ __forceinline__ bool cone_reaches(d3 ch, double Rh, d3 d, double tan_
   return true;
 }
 
+// Second, tighter test for a pair that passed cone_reaches: the two mirrors'
+// parallelograms (corners from the FP32 rectangle records, widened by mu for
+// their rounding) projected along the cone axis d onto the plane across it.
+// A ray from a point p of mirror h meeting a point q of mirror k travels
+// (q - p).d >= 0 along d and at most (q - p).d tan(alpha) across it, so the
+// projections can be at most rho = (max_k a - min_h a) tan(alpha) apart
+// (a = axial coordinate).  A separating axis of the two projected
+// parallelograms with a larger gap rules the pair out; the axes tried are the
+// projected edge normals (an axis that degenerates is skipped, which only
+// keeps the pair).
+__device__ bool sat_reaches(const float4* rh, const float4* rk, d3 d, double tan_a) {
+  const double mu = 0.01;
+  d3 e1 = fabs(d.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
+  e1 = e1 - dot(e1, d) * d;
+  e1 = (1.0 / sqrt(dot(e1, e1))) * e1;
+  const d3 e2 = cross(d, e1);
+  double px[2][4], py[2][4], amin_h = 1e300, amax_k = -1e300;
+  double ex[2][2], ey[2][2];
+  for (int m = 0; m < 2; ++m) {
+    const float4* r = m ? rk : rh;
+    const d3 A = mk(r[0].x, r[0].y, r[0].z), E1 = mk(r[1].x, r[1].y, r[1].z), E2 = mk(r[2].x, r[2].y, r[2].z);
+    const d3 c[4] = {A, A + E1, A + E2, A + E1 + E2};
+    for (int i = 0; i < 4; ++i) {
+      const double ax = dot(c[i], d);
+      if (m) amax_k = fmax(amax_k, ax);
+      else amin_h = fmin(amin_h, ax);
+      px[m][i] = dot(c[i], e1);
+      py[m][i] = dot(c[i], e2);
+    }
+    ex[m][0] = dot(E1, e1); ey[m][0] = dot(E1, e2);
+    ex[m][1] = dot(E2, e1); ey[m][1] = dot(E2, e2);
+  }
+  const double da = amax_k - amin_h + 2.0 * mu;
+  if (da < 0.0) return false;  // k lies wholly behind h along every ray
+  const double rho = da * tan_a + 2.0 * mu;
+  for (int m = 0; m < 2; ++m)
+    for (int j = 0; j < 2; ++j) {
+      double nx = -ey[m][j], ny = ex[m][j];
+      const double l = sqrt(nx * nx + ny * ny);
+      if (!(l > 1e-9)) continue;
+      nx /= l;
+      ny /= l;
+      double lo[2] = {1e300, 1e300}, hi[2] = {-1e300, -1e300};
+      for (int q = 0; q < 2; ++q)
+        for (int i = 0; i < 4; ++i) {
+          const double v = px[q][i] * nx + py[q][i] * ny;
+          lo[q] = fmin(lo[q], v);
+          hi[q] = fmax(hi[q], v);
+        }
+      if (lo[1] - hi[0] > rho || lo[0] - hi[1] > rho) return false;
+    }
+  return true;
+}
+
 __global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
   const int lane = threadIdx.x & 31;
   const int h = blockIdx.x * 4 + (threadIdx.x >> 5);
@@ -303,8 +357,8 @@ __global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
     if (k < a.n && k != h) {
       const d3 ck = mk(a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]);
       const double Rk = bound_radius(a.size, k);
-      rs = cone_reaches(ch, Rh, ds, ts, ys, ck, Rk);
-      rb = cone_reaches(ch, Rh, db, tb, yb, ck, Rk);
+      rs = cone_reaches(ch, Rh, ds, ts, ys, ck, Rk) && sat_reaches(a.rect + 3 * h, a.rect + 3 * k, ds, ts);
+      rb = cone_reaches(ch, Rh, db, tb, yb, ck, Rk) && sat_reaches(a.rect + 3 * h, a.rect + 3 * k, db, tb);
     }
     const unsigned ms = __ballot_sync(0xffffffffu, rs), mb = __ballot_sync(0xffffffffu, rb);
     if (rs) {
