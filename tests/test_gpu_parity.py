@@ -365,6 +365,32 @@ def test_candidate_lists_equal_the_grid_walk(name, elev):
     sc.close()
 
 
+def test_overflowing_candidate_lists_walk_the_grid():
+    """A row of 60 small mirrors laid along the sun's horizontal direction
+    under a 1 degree sun: the first mirrors' shadow rays graze over more than
+    32 others, so those lists overflow and their rays walk the grid (cells
+    walked > 0); every flag, pixel and count still equals the pure walk's."""
+    sun = W.make_sun(1.0, 150.0, 1000.0, 0.1)
+    sd = np.array(sun.dir[:], np.float64)
+    toward = -np.array([sd[0], 0.0, sd[2]])
+    toward /= np.linalg.norm(toward)
+    p0 = np.array([0.0, 1.5, -40.0])
+    pos = np.array([p0 + 1.5 * i * toward for i in range(60)], np.float32)
+    size = np.tile(np.array([[1.0, 0.05, 1.0]], np.float32), (60, 1))
+    rec = W.flat_receiver(30.0, 6.0, 6.0, 64, 64)
+    w = W.Workload("row", pos, size, 0.002, rec, W.grid(5.0), sun, W.params(60 * 16 * 256, 256, 0.1, seed=3))
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    g = sc.trace(sun, p, records=True)
+    f, px, cnt = g["flags"].clone(), g["pixel"].clone(), g["counts"].clone()
+    assert g["stats"].dda_cells > 0  # some lists overflowed
+    assert g["stats"].shadowed > 0
+    p.kernel_variant = 5
+    g5 = sc.trace(sun, p, records=True)
+    assert torch.equal(f, g5["flags"]) and torch.equal(px, g5["pixel"]) and torch.equal(cnt, g5["counts"])
+    sc.close()
+
+
 def test_smoothing_heaps_bit_exact_with_reference_gpu_kernel():
     """QMCRT_TRIM_HEAPS against ImageSmoother::image_smooth's output on a B200."""
     from test_oracle_pins import GV
