@@ -401,8 +401,8 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* scene, const qmcrt_sun* sun,
                                 const qmcrt_table_inputs* tables, const qmcrt_trace_params* params,
                                 const qmcrt_outputs* out, qmcrt_trace_stats* stats, void* stream);
 
-/* End-to-end call on host buffers: upload the field, trace, download the
- * maps.  h_counts / h_flux may be NULL.  Synchronises. */
+/* End-to-end call on host buffers: upload the field (NULL: keep the scene's),
+ * trace, download the maps.  h_counts / h_flux may be NULL.  Synchronises. */
 qmcrt_status qmcrt_trace_host(qmcrt_scene* scene, const qmcrt_field* field, const qmcrt_sun* sun,
                               const qmcrt_trace_params* params, uint32_t* h_counts, float* h_flux,
                               qmcrt_trace_stats* stats, void* stream);

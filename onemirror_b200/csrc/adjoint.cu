@@ -27,6 +27,7 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
 void buie_with_guide(float csr, BuieTable* t);
 
 constexpr int kAdjThreads = 256;
+constexpr int kAdjTileMax = 120;  // 57.6 KB of tile + 16 KB of Buie table: 3 CTAs per SM
 
 // ------------------------------------------------------------ dual numbers
 // value + derivatives with respect to the 4 parameters of one heliostat
@@ -118,6 +119,7 @@ __global__ void frame_jacobian_kernel(JacArgs a) {
 
 struct AdjArgs {
   TraceArgs t;
+  int tile, tile_r0, tile_c0;  // forward: block-private tile of tile x tile pixels at (row r0, col c0); 0: none
   double ew[3], eh[3];  // receiver width / height unit axes (flat receivers)
   uint8_t* tape;        // one visibility byte per ray
   uint64_t saved;       // rays with a byte in the tape
@@ -129,7 +131,7 @@ struct AdjArgs {
 
 // Receiver hit with the continuous (u, v) (flat receivers): along E1 (rows)
 // and E2 (columns), each in [0, 1]; t along the ray.
-__device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, double* u, double* v) {
+__device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, double* u, double* v, double* t) {
   d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
   d3 pv = cross(d, E2);
   double det = dot(E1, pv);
@@ -141,13 +143,35 @@ __device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, doub
   d3 qv = cross(T, E1);
   *v = dot(d, qv) * inv;
   if (*v < 0 || *v > 1) return false;
-  return dot(E2, qv) * inv >= 1e-6;
+  *t = dot(E2, qv) * inv;
+  return *t >= 1e-6;
+}
+
+// Reflection geometry of one ray: the perturbed unit normal and reflected
+// unit direction, and the lengths they had before normalising (for the
+// derivative of the normalisation in the backward pass).
+struct Refl {
+  d3 np, rd;
+  double lnp, lr;
+};
+
+__device__ __forceinline__ Refl reflect_ray(const RaySetup& R) {
+  Refl g;
+  const d3 npr = apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z);
+  const double q = dot(npr, npr), iq = rsqrt(q);
+  g.np = iq * npr;
+  g.lnp = q * iq;
+  const d3 rr = R.ws - (2.0 * dot(R.ws, g.np)) * g.np;
+  const double q2 = dot(rr, rr), iq2 = rsqrt(q2);
+  g.rd = iq2 * rr;
+  g.lr = q2 * iq2;
+  return g;
 }
 
 // Visibility and hit geometry of one ray (shadow, reflection, block, receiver).
 template <bool CULL>
-__device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, float fy0, float fy1, d3* np, d3* rd,
-                                         double* u, double* v) {
+__device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, float fy0, float fy1, Refl* g,
+                                         double* u, double* v, double* t) {
   // with CULL (corrected mode) the heliostat's occluder candidates answer the
   // visibility questions (the grid walk where there are none)
   uint32_t nt = 0, nc = 0;
@@ -156,20 +180,23 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
   if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc)
            : dda_blocked<false, false>(a, of, sd, R.h, fy0, fy1, nt, nc))
     return false;
-  *np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
-  double di = dot(R.ws, *np);
-  *rd = rnorm(R.ws - (2.0 * di) * *np);
-  if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(*rd), fy0, fy1, nt, nc)
-           : dda_blocked<false, false>(a, of, to_f(*rd), R.h, fy0, fy1, nt, nc))
+  *g = reflect_ray(R);
+  if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(g->rd), fy0, fy1, nt, nc)
+           : dda_blocked<false, false>(a, of, to_f(g->rd), R.h, fy0, fy1, nt, nc))
     return false;
-  return receiver_uv(a, R.o, *rd, u, v);
+  return receiver_uv(a, R.o, g->rd, u, v, t);
 }
 
 template <bool CULL>
-__global__ void __launch_bounds__(kAdjThreads) adjoint_forward_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const AdjArgs A) {
   __shared__ float s_tab[1025 + 1025 + 1024];
   __shared__ int s_guide[kBuieBuckets];
+  // block-private tile of the energy map: many heliostats aim at the same
+  // spot, so global atomics on it would queue at the hot pixels
+  extern __shared__ float s_tile[];
+  const int T = A.tile, r0 = A.tile_r0, c0 = A.tile_c0;
   const TraceArgs& a = A.t;
+  for (int i = threadIdx.x; i < T * T; i += blockDim.x) s_tile[i] = 0.f;
   load_buie(a.buie, s_tab, s_guide);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
@@ -181,12 +208,12 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_forward_kernel(const AdjA
     const uint32_t ray = (uint32_t)r64;
     RaySetup R;
     ray_setup<false>(a, s_tab, s_guide, ray, R);
-    d3 np, rd;
-    double u, v;
-    const bool hit = ray_hits<CULL>(a, R, fy0, fy1, &np, &rd, &u, &v);
+    Refl g;
+    double u, v, t;
+    const bool hit = ray_hits<CULL>(a, R, fy0, fy1, &g, &u, &v, &t);
     if (r64 < A.saved) A.tape[r64] = hit ? 1 : 0;
     if (!hit) continue;
-    float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * R.w;
+    float e = (float)fabs(g.np.x * a.sdir[0] + g.np.y * a.sdir[1] + g.np.z * a.sdir[2]) * R.w;
     float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
     int i0 = (int)floorf(px), j0 = (int)floorf(py);
     float fx = px - (float)i0, fy = py - (float)j0;
@@ -194,8 +221,16 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_forward_kernel(const AdjA
     for (int k = 0; k < 4; ++k) {
       int ci = i0 + (k & 1), cj = j0 + (k >> 1);
       if (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) continue;
-      atomicAdd(a.energy + cj * a.res_x + ci, e * wgt[k]);
+      if ((unsigned)(cj - r0) < (unsigned)T && (unsigned)(ci - c0) < (unsigned)T)
+        atomicAdd(s_tile + (cj - r0) * T + (ci - c0), e * wgt[k]);
+      else
+        atomicAdd(a.energy + cj * a.res_x + ci, e * wgt[k]);
     }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
+    const float v = s_tile[i];
+    if (v != 0.f) atomicAdd(a.energy + (r0 + i / T) * a.res_x + (c0 + i % T), v);
   }
 }
 
@@ -248,17 +283,16 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
       ray_setup<false>(a, s_tab, s_guide, ray, R);
       h = R.h;
       bool hit;
-      d3 np, rd;
-      double u = 0, v = 0;
+      Refl g;
+      double u = 0, v = 0, tr = 0;
       if (r64 < A.saved) {
         hit = A.tape[r64] != 0;
         if (hit) {  // rebuild the hit geometry without the traversals
-          np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
-          rd = rnorm(R.ws - (2.0 * dot(R.ws, np)) * np);
-          hit = receiver_uv(a, R.o, rd, &u, &v);
+          g = reflect_ray(R);
+          hit = receiver_uv(a, R.o, g.rd, &u, &v, &tr);
         }
       } else {
-        hit = ray_hits<CULL>(a, R, fy0, fy1, &np, &rd, &u, &v);
+        hit = ray_hits<CULL>(a, R, fy0, fy1, &g, &u, &v, &tr);
       }
       if (hit) {
         // bilinear corners and the adjoint map there
@@ -274,21 +308,15 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         const float gWx = (1.f - fy) * (Gc[1] - Gc[0]) + fy * (Gc[3] - Gc[2]);
         const float gWy = (1.f - fx) * (Gc[2] - Gc[0]) + fx * (Gc[3] - Gc[1]);
         // forward quantities in float
-        const float3 npf = to_f(np), rdf = to_f(rd), wsf = to_f(R.ws);
-        d3 npr = apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z);
-        const float lnp = (float)sqrt(dot(npr, npr));
-        d3 rr = R.ws - (2.0 * dot(R.ws, np)) * np;
-        const float lr = (float)sqrt(dot(rr, rr));
+        const float3 npf = to_f(g.np), rdf = to_f(g.rd), wsf = to_f(R.ws);
+        const float lnp = (float)g.lnp, lr = (float)g.lr;
         const float nws = dot(npf, wsf);
         const float sdn = dot(sd, npf);
         const float e = fabsf(sdn) * R.w, sg = sdn < 0.f ? -1.f : 1.f;
         // t along the reflected ray to the receiver plane (for d(hit) = do + t dr)
         const float3 cr = cross(E2, rdf);
         const float den = dot(E1, cr);
-        d3 Tt = R.o - mk(a.rA[0], a.rA[1], a.rA[2]);
-        d3 qv = cross(Tt, mk(a.rE1[0], a.rE1[1], a.rE1[2]));
-        const float t = (float)(dot(mk(a.rE2[0], a.rE2[1], a.rE2[2]), qv) /
-                                dot(mk(a.rE1[0], a.rE1[1], a.rE1[2]), cross(rd, mk(a.rE2[0], a.rE2[1], a.rE2[2]))));
+        const float t = (float)tr;
         const float* J = A.jac + 36 * h;
         const float x = R.xz.x, z = R.xz.y, hy = R.hy;
         for (int k = 0; k < 4; ++k) {
@@ -334,11 +362,11 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
 // Grid of a grid-stride adjoint kernel: as many CTAs as stay resident
 // together (more would leave the last ones running nearly alone).
 template <class K>
-static int adj_blocks(K kernel, uint64_t rays) {
+static int adj_blocks(K kernel, uint64_t rays, size_t smem = 0) {
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAdjThreads, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAdjThreads, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * per_sm, (rays + kAdjThreads - 1) / kAdjThreads));
 }
@@ -466,12 +494,19 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.saved = saved;
   A.G = t->d_G;
   A.jac = t->d_jac;
-  const int blocks = adj_blocks(adjoint_forward_kernel<true>, p->rays);
+  // the tile: the map's central T x T pixels, T as large as keeps 3 CTAs
+  // (with the 16 KB Buie table) on an SM
+  A.tile = std::min({s->rg.res_x, s->rg.res_y, kAdjTileMax});
+  A.tile_r0 = (s->rg.res_y - A.tile) / 2;
+  A.tile_c0 = (s->rg.res_x - A.tile) / 2;
+  const size_t tile_bytes = (size_t)A.tile * A.tile * sizeof(float);
+  QM_CUDA(cudaFuncSetAttribute(adjoint_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes));
+  const int blocks = adj_blocks(adjoint_forward_kernel<true>, p->rays, tile_bytes);
   *tape = t;  // from here on the caller owns it, also when a launch below fails
   QM_CUDA(cudaMemcpyAsync(t->d_buie, t->buie.host.data(), t->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
   QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
-  adjoint_forward_kernel<true><<<blocks, kAdjThreads, 0, st>>>(A);
+  adjoint_forward_kernel<true><<<blocks, kAdjThreads, tile_bytes, st>>>(A);
   QM_CUDA(cudaGetLastError());
   LossArgs la{t->d_energy, d_target, d_flux, t->d_G,
               (float)((double)sun->dni * p->reflectivity / ((double)p->rays_per_point * s->rg.pixel_area)), res,

@@ -368,7 +368,7 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcr
 qmcrt_status qmcrt_trace_host(qmcrt_scene* s, const qmcrt_field* field, const qmcrt_sun* sun,
                               const qmcrt_trace_params* p, uint32_t* h_counts, float* h_flux,
                               qmcrt_trace_stats* stats, void* stream) {
-  if (!s) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "scene is NULL");
+  if (!s || !sun || !p) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
   cudaStream_t st = (cudaStream_t)stream;
   qmcrt_status e;
   if (field && (e = qmcrt_scene_set_field(s, field, stream))) return e;
