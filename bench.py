@@ -91,6 +91,61 @@ def oracle_sample(w, seconds, threads=0):
             "ranges": nr, "rays_per_range": per, "stats": [int(x) for x in st]}
 
 
+def flux_rmse(sc, w, p, ranges=512, per=8192):
+    """Flux error of the benchmark configuration.
+
+    Monte Carlo: two independent ray sets of the configuration's size (Philox
+    items 0 and 1) give maps F0, F1; one map's RMSE is RMS(F0 - F1) / sqrt 2,
+    stated in W/m^2 and relative to the peak and to the mean over lit pixels.
+    Against the FP64 oracle on identical rays (item 0, the oracle's sun and
+    points): `ranges` ray ranges of `per` rays spread over the field, per-ray
+    agreement of flags and receiver pixels, and the RMSE of the count map of
+    those rays relative to the oracle's RMS count."""
+    import torch
+    from oracle import oracle as O
+    rays = int(p.rays)
+    item0 = p.item
+    p.item = 0
+    r0 = sc.trace(w.sun, p, records=True, stats=False)
+    p.item = 1
+    r1 = sc.trace(w.sun, p, records=False, stats=False)
+    p.item = item0
+    f0 = r0["flux"].double()
+    f1 = r1["flux"].double()
+    mc = float(torch.sqrt(torch.mean((f0 - f1) ** 2) / 2.0))
+    mean = 0.5 * (f0 + f1)
+    lit = mean > 0
+    starts = np.linspace(0, rays - per, ranges).astype(np.int64)
+    idx = torch.as_tensor((starts[:, None] + np.arange(per)[None, :]).ravel(), device=r0["flags"].device)
+    gf = r0["flags"][idx].cpu().numpy()
+    gp = r0["pixel"][idx].cpu().numpy()
+    del r0, r1
+    cell = w.grid.cell[0] / max(w.grid.fine_div, 1)
+    osc = O.Scene(w.pos, w.size, w.sigma, w.receiver, cell, w.grid.margin, list(w.sun.dir), aim=w.aim)
+    rpp = p.rays_per_point
+    xz, helio = O.points_poisson(w.size, rays // rpp, p.point_spacing, p.seed)
+    of = np.empty_like(gf)
+    op = np.empty_like(gp)
+    oc = np.zeros(w.res[0] * w.res[1], np.float64)
+    for i, b in enumerate(starts):
+        cfg = osc.cfg(w.sun.csr, p.seed, rays, rpp, xz, helio, threads=os.cpu_count(), ray_begin=int(b),
+                      ray_end=int(b) + per)
+        r = osc.trace_philox(cfg, records=True, maps=True)
+        of[i * per:(i + 1) * per] = r["flags"]
+        op[i * per:(i + 1) * per] = r["pixel"]
+        oc += r["counts"]
+    gc = np.bincount(gp[gp >= 0], minlength=oc.size).astype(np.float64)
+    same = (gf == of) & (gp == op)
+    return {"mc_rmse_w_m2": mc, "mc_rmse_rel_peak": mc / float(mean.max()),
+            "mc_rmse_rel_lit_mean": mc / float(mean[lit].mean()),
+            "mc_method": "two independent %d-ray maps (Philox items 0, 1): RMS(F0 - F1) / sqrt 2" % rays,
+            "oracle_rays": int(gf.size), "oracle_ray_agreement": float(same.mean()),
+            "oracle_rays_differing": int((~same).sum()),
+            "oracle_count_map_rmse_rel": float(np.sqrt(np.mean((gc - oc) ** 2)) / np.sqrt(np.mean(oc ** 2))),
+            "oracle_method": "%d ray ranges x %d rays spread over the field, identical rays traced by the FP64 "
+                             "oracle" % (ranges, per)}
+
+
 def flops_per_ray(stats):
     """Algorithmic FP32 flops per ray of the reference algorithm: fixed per-ray
     work 192, 30 per traversal set-up (one traversal for shadowed rays, two
@@ -438,8 +493,10 @@ def b200_arm(a, rank, world, local):
                "sample": "%d ray ranges x %d rays spread over the field (%d rays, %.1f s), FP64 oracle"
                          % (ob["ranges"], ob["rays_per_range"], ob["rays"], ob["seconds"])}
         ref_stats = ob["stats"]
+        accuracy = flux_rmse(sc, w, p)
     else:
         ref_stats = None
+        accuracy = None
     # Algorithmic flops per ray: the per-ray figure of the reference algorithm
     # (fixed work + traversal set-ups + 54 per rectangle test + 4 per DDA cell)
     # with the oracle's counts of rectangle tests and cells on a sample of the
@@ -479,7 +536,7 @@ def b200_arm(a, rank, world, local):
                        "l2": "flushed between timed steps (256 MB write)",
                        "grid": grid_name(w.grid),
                        "step": "aim + occluder candidates + grid build + trace + flux scaling + trimmed-mean smoothing"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "flux_rmse": accuracy,
             "gpu_launches": launches * a.steps,
             "launches_per_step": per_step,
             "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
