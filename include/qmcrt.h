@@ -348,6 +348,18 @@ qmcrt_status qmcrt_scene_read_grid(qmcrt_scene* scene, int32_t* h_cell_start, in
 qmcrt_status qmcrt_scene_read_geometry(qmcrt_scene* scene, double* h_normals, double* h_vertices,
                                        void* stream);
 
+/* Copy the occluder candidates of the current sun (no reference
+ * counterpart; they replace the grid walk of NotCollision,
+ * rectgrid_raytracing.cu:38-117, for Philox traces): h_counts [2n] holds
+ * each heliostat's shadow and block candidate counts (above QMCRT_CAND_CAP:
+ * the rays walk the grid), h_ids [2n*QMCRT_CAND_CAP] (may be NULL) their
+ * heliostat ids, -1 past the count.  exhaustive = 1 recomputes them by testing every pair instead
+ * of the bucket search (same sets; the order within a list may differ).
+ * Needs a sun set for the current field.  Syncs. */
+#define QMCRT_CAND_CAP 32
+qmcrt_status qmcrt_scene_read_candidates(qmcrt_scene* scene, int32_t exhaustive, int32_t* h_counts,
+                                         int32_t* h_ids, void* stream);
+
 /* Micro-heliostat sample points for (seed, rays, rays_per_point, mode,
  * spacing) (set_possion_microhelio_centers steps_for_raytracing.cu:105-158,
  * set_microhelio_centers :67-103).  Cached in the scene.  points_out: count. */

@@ -25,6 +25,7 @@ RECEIVER_FLAT, RECEIVER_CYLINDER = 0, 1
 POINTS_POISSON, POINTS_GRID = 0, 1
 DEPOSIT_NEAREST, DEPOSIT_BILINEAR = 0, 1
 ATTEN_NONE, ATTEN_POLY_EXP = 0, 1
+CAND_CAP = 32  # QMCRT_CAND_CAP: occluder candidates kept per heliostat and walk
 TRIM_SORTED, TRIM_HEAPS = 0, 1
 RAY_SHADOWED, RAY_BLOCKED, RAY_HIT, RAY_OFFMAP = 1, 2, 4, 8
 
@@ -138,6 +139,7 @@ PROTOTYPES = {
     "qmcrt_scene_grid_info": (C.c_int, [C.c_void_p, C.POINTER(GridInfo)]),
     "qmcrt_scene_read_grid": (C.c_int, [C.c_void_p, i32p, i32p, C.c_void_p]),
     "qmcrt_scene_read_geometry": (C.c_int, [C.c_void_p, dp, dp, C.c_void_p]),
+    "qmcrt_scene_read_candidates": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, C.c_void_p]),
     "qmcrt_scene_sample_points": (C.c_int, [C.c_void_p, C.POINTER(TraceParams), C.POINTER(C.c_int64), C.c_void_p]),
     "qmcrt_scene_read_points": (C.c_int, [C.c_void_p, fp, i32p, C.c_void_p]),
     "qmcrt_sample_points_noalloc": (C.c_int, [fp, C.c_int32, C.c_int64, C.c_float, C.c_uint64, C.c_void_p,

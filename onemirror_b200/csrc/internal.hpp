@@ -55,6 +55,17 @@ constexpr double kSunAlphaMax = 9.31e-3;
 // 24-bit uniforms (u1 >= 2^-25): 5.89, in units of sigma.
 constexpr double kSlopeZMax = 6.0;
 
+// Heliostat centres bucketed on a 2D grid over (x, z), rebuilt on the host
+// whenever the field is uploaded: the candidate search visits only the
+// buckets a cone can reach.  The header lives in device memory so that a
+// captured graph reads the current field's values.
+struct CandBuckets {
+  double x0, z0, inv;  // grid origin (smallest centre x, z) and 1 / bucket size
+  int nbx, nbz;        // buckets along x and z; bucket (bx, bz) is bz * nbx + bx
+  double ytop;         // largest centre height + bounding radius over the field
+  double rmax;         // largest bounding radius (half-diagonal + 1 cm)
+};
+
 struct SunGeom {
   double* normal = nullptr;      // [3n]
   double* frame = nullptr;       // [9n] u, n, v
@@ -100,6 +111,13 @@ struct qmcrt_scene {
   bool has_aim = false, has_normal = false, has_tilt = false;
   std::vector<float> h_pos, h_size;
   float ytop = 0.f;  // highest point any mirror can reach (centre + half-diagonal)
+  // centre buckets of the candidate search (host copies stay alive for the async uploads)
+  int64_t bucket_cap = 0;                    // capacity of the bucket table (buckets)
+  qm::CandBuckets h_buckets{};
+  std::vector<int32_t> h_bucket_start, h_bucket_ids;
+  qm::CandBuckets* d_buckets = nullptr;      // [1]
+  int32_t* d_bucket_start = nullptr;         // [bucket_cap + 1] first index of each bucket in d_bucket_ids
+  int32_t* d_bucket_ids = nullptr;           // [n] heliostat ids by bucket, ascending within a bucket
   qmcrt_receiver recv{};
   qm::ReceiverGeom rg;
   qmcrt_grid_params gp{};

@@ -254,10 +254,14 @@ struct CandArgs {
   const double* frame;
   double sun[3];      // incident direction, unit
   double sun_alpha;   // largest angle of a sun sample from the sun axis (rad)
+  double shadow_tan, shadow_rise;  // the shadow cone (the same for every heliostat): tan of its half-angle, rise
   double zmax;        // largest |z| of the slope deviate, in units of sigma
   const float4* rect;  // [3n] every heliostat's rectangle record
   float4* cand;        // [n][2][kCandCap][3] the candidates' records, inline
   int* cand_n;        // [n][2]
+  const CandBuckets* buckets;    // centre buckets of the field (header)
+  const int32_t* bucket_start;   // [nbx * nbz + 1]
+  const int32_t* bucket_ids;     // [n]
 };
 
 __device__ __forceinline__ double bound_radius(const float* size, int h) {
@@ -333,51 +337,158 @@ __device__ bool sat_reaches(const float4* rh, const float4* rk, d3 d, double tan
   return true;
 }
 
-__global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int h = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (h >= a.n) return;  // h is uniform across the warp
-  const d3 ch = mk(a.pos[3 * h], a.pos[3 * h + 1], a.pos[3 * h + 2]);
-  const double Rh = bound_radius(a.size, h);
+// The cone of one walk of heliostat h: axis d, tan of its half-angle, and
+// the rise per unit length of its lowest ray, sin(asin(d.y) - alpha) (<= 1e-3:
+// it does not rise).  all: the half-angle is too wide for a cone (slope
+// errors of ~0.13 rad and more); every heliostat is a candidate.
+struct Cone {
+  d3 d;
+  double tan_a, rise;
+  bool all;
+};
+
+__device__ __forceinline__ Cone walk_cone(const CandArgs& a, int h, int walk) {
+  const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
+  if (walk == 0) return Cone{mk(-s.x, -s.y, -s.z), a.shadow_tan, a.shadow_rise, false};
   const double* F = a.frame + 9 * h;
   const d3 nh = mk(F[3], F[4], F[5]);
-  const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
-  const d3 ds = mk(-s.x, -s.y, -s.z);
   const d3 db = s - (2.0 * dot(s, nh)) * nh;
-  const double as = a.sun_alpha + 1e-6, ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
-  const double ts = tan(as), tb = tan(ab);
-  const double ys = sin(asin(fmin(fmax(ds.y, -1.0), 1.0)) - as), yb = sin(asin(fmin(fmax(db.y, -1.0), 1.0)) - ab);
-  float4* Ls = a.cand + (int64_t)2 * h * kCandCap * 3;
-  float4* Lb = Ls + kCandCap * 3;
-  int ns = 0, nb = 0;
-  const unsigned below = (1u << lane) - 1u;
-  for (int k0 = 0; k0 < a.n; k0 += 32) {
-    const int k = k0 + lane;
-    bool rs = false, rb = false;
-    if (k < a.n && k != h) {
-      const d3 ck = mk(a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]);
-      const double Rk = bound_radius(a.size, k);
-      rs = cone_reaches(ch, Rh, ds, ts, ys, ck, Rk) && sat_reaches(a.rect + 3 * h, a.rect + 3 * k, ds, ts);
-      rb = cone_reaches(ch, Rh, db, tb, yb, ck, Rk) && sat_reaches(a.rect + 3 * h, a.rect + 3 * k, db, tb);
-    }
-    const unsigned ms = __ballot_sync(0xffffffffu, rs), mb = __ballot_sync(0xffffffffu, rb);
-    if (rs) {
-      const int slot = ns + __popc(ms & below);
-      if (slot < kCandCap)
-        for (int j = 0; j < 3; ++j) Ls[3 * slot + j] = a.rect[3 * k + j];
-    }
-    if (rb) {
-      const int slot = nb + __popc(mb & below);
-      if (slot < kCandCap)
-        for (int j = 0; j < 3; ++j) Lb[3 * slot + j] = a.rect[3 * k + j];
-    }
-    ns += __popc(ms);
-    nb += __popc(mb);
+  const double ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
+  if (!(ab < 1.2)) return Cone{db, 0.0, 0.0, true};
+  double sa, ca;
+  sincos(ab, &sa, &ca);
+  const double y = fmin(fmax(db.y, -1.0), 1.0);
+  return Cone{db, sa / ca, y * ca - sqrt(fmax(1.0 - y * y, 0.0)) * sa, false};
+}
+
+// Each lane tests its heliostat k (k < 0: none) against heliostat h's cone;
+// the passing ones are appended to list L in lane order.  Returns the updated
+// count, which may pass kCandCap (only the first kCandCap records are kept).
+__device__ __forceinline__ int cand_take(const CandArgs& a, int k, int h, d3 ch, double Rh, const Cone& c, float4* L,
+                                         int cnt) {
+  const int lane = threadIdx.x & 31;
+  bool r = false;
+  if (k >= 0 && k != h) {
+    const d3 ck = mk(a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]);
+    r = c.all || (cone_reaches(ch, Rh, c.d, c.tan_a, c.rise, ck, bound_radius(a.size, k)) &&
+                  sat_reaches(a.rect + 3 * h, a.rect + 3 * k, c.d, c.tan_a));
   }
-  if (lane == 0) {
-    a.cand_n[2 * h] = ns;
-    a.cand_n[2 * h + 1] = nb;
+  const unsigned m = __ballot_sync(0xffffffffu, r);
+  if (r) {
+    const int slot = cnt + __popc(m & ((1u << lane) - 1u));
+    if (slot < kCandCap)
+      for (int j = 0; j < 3; ++j) L[3 * slot + j] = a.rect[3 * k + j];
   }
+  return cnt + __popc(m);
+}
+
+__device__ __forceinline__ int clamp_bucket(double v, int nb) { return (int)fmin(fmax(floor(v), 0.0), nb - 1.0); }
+
+// The candidates of one walk of heliostat h, searched over the centre
+// buckets the cone can reach.  A k accepted by cone_reaches lies at axial
+// distance t in [-(Rh + Rk), Rh + Rk + (ck.y + Rk - ch.y + Rh) / rise] and
+// within Rh + Rk + (t + Rh + Rk) tan_a of the axis, so its centre projects
+// onto (x, z) within rad of the projected axis segment [t0, t1] (bounded
+// with the field's largest Rk and ck.y + Rk; 5 cm added for rounding).  Per
+// bucket row, the part of the segment within rad of the row's z-strip gives
+// the x-range of buckets, one contiguous run of ids.  A cone that does not
+// rise has no axial bound and visits every bucket.  The lanes take one row
+// each (32 rows at a time), and the rows' runs are then tested as one list,
+// 32 ids at a time: each lane finds the row of its id by a binary search over
+// the rows' exclusive prefix sums.
+__device__ int cand_search(const CandArgs& a, const CandBuckets& B, int h, d3 ch, double Rh, const Cone& c,
+                           float4* L) {
+  const int lane = threadIdx.x & 31;
+  const double rr = Rh + B.rmax;
+  const bool bounded = !c.all && c.rise > 1e-3;
+  double rad = 0.0, p0x = 0.0, p0z = 0.0, dx = 0.0, dz = 0.0;
+  int bz0 = 0, bz1 = B.nbz - 1;
+  if (bounded) {
+    const double t0 = -rr, t1 = rr + (B.ytop - ch.y + Rh) / c.rise;
+    rad = rr + (fmax(t1, 0.0) + rr) * c.tan_a + 0.05;
+    p0x = ch.x + t0 * c.d.x;
+    p0z = ch.z + t0 * c.d.z;
+    dx = (t1 - t0) * c.d.x;
+    dz = (t1 - t0) * c.d.z;
+    bz0 = clamp_bucket((fmin(p0z, p0z + dz) - rad - B.z0) * B.inv, B.nbz);
+    bz1 = clamp_bucket((fmax(p0z, p0z + dz) + rad - B.z0) * B.inv, B.nbz);
+  }
+  const double bsz = 1.0 / B.inv;
+  int cnt = 0;
+  for (int rb = bz0; rb <= bz1; rb += 32) {
+    const int bz = rb + lane;
+    int s0 = 0, len = 0;
+    if (bz <= bz1) {
+      int bx0 = 0, bx1 = B.nbx - 1;
+      bool any = true;
+      if (bounded) {
+        const double zs0 = B.z0 + bz * bsz - rad, zs1 = B.z0 + (bz + 1) * bsz + rad;
+        double ta = 0.0, tb = 1.0;
+        if (fabs(dz) > 1e-12) {
+          ta = (zs0 - p0z) / dz;
+          tb = (zs1 - p0z) / dz;
+          if (ta > tb) {
+            const double t = ta;
+            ta = tb;
+            tb = t;
+          }
+          ta = fmax(ta, 0.0);
+          tb = fmin(tb, 1.0);
+          any = ta <= tb;
+        } else {
+          any = p0z >= zs0 && p0z <= zs1;
+        }
+        const double xa = p0x + ta * dx, xb = p0x + tb * dx;
+        bx0 = clamp_bucket((fmin(xa, xb) - rad - B.x0) * B.inv, B.nbx);
+        bx1 = clamp_bucket((fmax(xa, xb) + rad - B.x0) * B.inv, B.nbx);
+      }
+      if (any) {
+        s0 = __ldg(a.bucket_start + bz * B.nbx + bx0);
+        len = __ldg(a.bucket_start + bz * B.nbx + bx1 + 1) - s0;
+      }
+    }
+    int incl = len;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int excl = incl - len, total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int base = 0; base < total; base += 32) {
+      const int idx = base + lane;
+      int r = 0;  // the last row whose exclusive prefix is <= idx
+      for (int step = 16; step > 0; step >>= 1)
+        if (__shfl_sync(0xffffffffu, excl, r + step) <= idx) r += step;
+      const int rs0 = __shfl_sync(0xffffffffu, s0, r), rex = __shfl_sync(0xffffffffu, excl, r);
+      const int k = idx < total ? __ldg(a.bucket_ids + rs0 + idx - rex) : -1;
+      cnt = cand_take(a, k, h, ch, Rh, c, L, cnt);
+    }
+  }
+  return cnt;
+}
+
+// One warp per (heliostat, walk): the shadow (walk 0) or block (walk 1)
+// candidates.  EXHAUSTIVE tests every other heliostat (the O(n^2)
+// definition, kept as the check of the bucket search); otherwise the bucket
+// search, which finds the same set.
+template <bool EXHAUSTIVE>
+__global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
+  const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (w >= 2 * a.n) return;  // w is uniform across the warp
+  const int h = w >> 1, walk = w & 1;
+  const d3 ch = mk(a.pos[3 * h], a.pos[3 * h + 1], a.pos[3 * h + 2]);
+  const double Rh = bound_radius(a.size, h);
+  const Cone c = walk_cone(a, h, walk);
+  float4* L = a.cand + (int64_t)(2 * h + walk) * kCandCap * 3;
+  int cnt = 0;
+  if (EXHAUSTIVE) {
+    for (int b = 0; b < a.n; b += 32) {
+      const int k = b + (int)(threadIdx.x & 31);
+      cnt = cand_take(a, k < a.n ? k : -1, h, ch, Rh, c, L, cnt);
+    }
+  } else {
+    cnt = cand_search(a, *a.buckets, h, ch, Rh, c, L);
+  }
+  if ((threadIdx.x & 31) == 0) a.cand_n[2 * h + walk] = cnt;
 }
 
 // ------------------------------------------------------------ points
@@ -522,6 +633,62 @@ static qmcrt_status check_field(const qmcrt_field* f) {
   return QMCRT_OK;
 }
 
+// Bucket the heliostat centres on a 2D grid over (x, z) for the candidate
+// search: bucket size max(2 R_max, sqrt(area / n)) (about one centre per
+// bucket, never smaller than a mirror), grown until the table fits its
+// capacity; ids ascending within each bucket (a stable counting sort).  The
+// bucket of a centre is floor((x - x0) / size) clamped to the grid, the same
+// double arithmetic the device search uses.
+static qmcrt_status build_buckets(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st) {
+  const int n = f->n;
+  CandBuckets& B = s->h_buckets;
+  double xmin = 1e300, xmax = -1e300, zmin = 1e300, zmax = -1e300, rmax = 0.0, ytop = -1e300;
+  for (int h = 0; h < n; ++h) {
+    const double x = f->pos[3 * h], y = f->pos[3 * h + 1], z = f->pos[3 * h + 2];
+    const double sx = f->size[3 * h], sy = f->size[3 * h + 1], sz = f->size[3 * h + 2];
+    const double r = 0.5 * std::sqrt(sx * sx + sy * sy + sz * sz) + 0.01;  // bound_radius on the device
+    xmin = std::min(xmin, x); xmax = std::max(xmax, x);
+    zmin = std::min(zmin, z); zmax = std::max(zmax, z);
+    rmax = std::max(rmax, r);
+    ytop = std::max(ytop, y + r);
+  }
+  const double area = std::max((xmax - xmin) * (zmax - zmin), 1.0);
+  double size = std::max(2.0 * rmax, std::sqrt(area / n));
+  int64_t nbx = 1, nbz = 1;
+  for (int it = 0; it < 200; ++it, size *= 1.25) {
+    nbx = (int64_t)std::floor((xmax - xmin) / size) + 1;
+    nbz = (int64_t)std::floor((zmax - zmin) / size) + 1;
+    if (nbx * nbz <= s->bucket_cap) break;
+  }
+  if (nbx * nbz > s->bucket_cap) return set_error(QMCRT_ERR_INTERNAL, "candidate bucket grid does not fit");
+  B.x0 = xmin;
+  B.z0 = zmin;
+  B.inv = 1.0 / size;
+  B.nbx = (int)nbx;
+  B.nbz = (int)nbz;
+  B.ytop = ytop + 0.01;
+  B.rmax = rmax + 0.01;
+  const int64_t nb = nbx * nbz;
+  auto bucket_of = [&](int h) {
+    const double bx = std::floor((f->pos[3 * h] - B.x0) * B.inv), bz = std::floor((f->pos[3 * h + 2] - B.z0) * B.inv);
+    const int ix = (int)std::min(std::max(bx, 0.0), (double)(nbx - 1));
+    const int iz = (int)std::min(std::max(bz, 0.0), (double)(nbz - 1));
+    return (int64_t)iz * nbx + ix;
+  };
+  s->h_bucket_start.assign(nb + 1, 0);
+  for (int h = 0; h < n; ++h) s->h_bucket_start[bucket_of(h) + 1]++;
+  for (int64_t b = 0; b < nb; ++b) s->h_bucket_start[b + 1] += s->h_bucket_start[b];
+  std::vector<int32_t> fill(s->h_bucket_start.begin(), s->h_bucket_start.end() - 1);
+  s->h_bucket_ids.assign(n, 0);
+  for (int h = 0; h < n; ++h) s->h_bucket_ids[fill[bucket_of(h)]++] = h;
+  // pageable sources: each copy returns once its source is staged
+  QM_CUDA(cudaMemcpyAsync(s->d_buckets, &s->h_buckets, sizeof(CandBuckets), cudaMemcpyHostToDevice, st));
+  QM_CUDA(cudaMemcpyAsync(s->d_bucket_start, s->h_bucket_start.data(), (nb + 1) * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, st));
+  QM_CUDA(cudaMemcpyAsync(s->d_bucket_ids, s->h_bucket_ids.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  return QMCRT_OK;
+}
+
 qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st) {
   size_t n = (size_t)f->n;
   QM_CUDA(cudaMemcpyAsync(s->d_pos, f->pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -538,12 +705,18 @@ qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st)
   }
   // sample points depend only on the mirror sizes (and the trace parameters)
   bool sizes_changed = s->h_size.size() != 3 * n || std::memcmp(s->h_size.data(), f->size, 3 * n * sizeof(float)) != 0;
+  bool moved = sizes_changed || s->h_pos.size() != 3 * n ||
+               std::memcmp(s->h_pos.data(), f->pos, 3 * n * sizeof(float)) != 0;
   s->h_pos.assign(f->pos, f->pos + 3 * n);
   s->h_size.assign(f->size, f->size + 3 * n);
   s->ytop = -3.0e38f;
   for (size_t h = 0; h < n; ++h) {
     const float* z = f->size + 3 * h;
     s->ytop = std::max(s->ytop, f->pos[3 * h + 1] + 0.5f * std::sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2]));
+  }
+  if (moved) {
+    qmcrt_status e = build_buckets(s, f, st);
+    if (e) return e;
   }
   s->field_version++;
   if (sizes_changed) s->points_key = PointsKey{};
@@ -620,6 +793,38 @@ void free_sun_geom(SunGeom* g) {
   dev_free(g->coarse_yr); dev_free(g->cand); dev_free(g->cand_n); dev_free(g->power);
 }
 
+// Occluder candidates of every heliostat of scene s for the (normalised) sun,
+// from the aimed frames and rectangle records, into cand / cand_n.
+static qmcrt_status launch_cand(const qmcrt_scene* s, const double* frame, const float4* rect, const double sun[3],
+                                bool exhaustive, float4* cand, int* cand_n, cudaStream_t st) {
+  CandArgs ca{};
+  ca.n = s->n;
+  ca.pos = s->d_pos;
+  ca.size = s->d_size;
+  ca.sigma = s->d_sigma;
+  ca.frame = frame;
+  for (int i = 0; i < 3; ++i) ca.sun[i] = sun[i];
+  ca.sun_alpha = kSunAlphaMax;
+  ca.zmax = kSlopeZMax;
+  {
+    const double as = kSunAlphaMax + 1e-6, y = std::min(std::max(-sun[1], -1.0), 1.0);
+    ca.shadow_tan = std::tan(as);
+    ca.shadow_rise = y * std::cos(as) - std::sqrt(std::max(1.0 - y * y, 0.0)) * std::sin(as);
+  }
+  ca.rect = rect;
+  ca.cand = cand;
+  ca.cand_n = cand_n;
+  ca.buckets = s->d_buckets;
+  ca.bucket_start = s->d_bucket_start;
+  ca.bucket_ids = s->d_bucket_ids;
+  if (exhaustive)
+    cand_kernel<true><<<(2 * s->n + 3) / 4, 128, 0, st>>>(ca);
+  else
+    cand_kernel<false><<<(2 * s->n + 3) / 4, 128, 0, st>>>(ca);
+  QM_CUDA(cudaGetLastError());
+  return QMCRT_OK;
+}
+
 // Aim every heliostat for the sun (normalised) and rebuild the grid into g:
 // stream-ordered kernels only, so the sequence can be captured in a graph.
 qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
@@ -647,20 +852,8 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   QM_CUDA(cudaMemsetAsync(g.power, 0, sizeof(double), st));
   aim_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(a);
   QM_CUDA(cudaGetLastError());
-  CandArgs ca{};
-  ca.n = s->n;
-  ca.pos = s->d_pos;
-  ca.size = s->d_size;
-  ca.sigma = s->d_sigma;
-  ca.frame = g.frame;
-  for (int i = 0; i < 3; ++i) ca.sun[i] = sun[i];
-  ca.sun_alpha = kSunAlphaMax;
-  ca.zmax = kSlopeZMax;
-  ca.rect = g.rect;
-  ca.cand = g.cand;
-  ca.cand_n = g.cand_n;
-  cand_kernel<<<(s->n + 3) / 4, 128, 0, st>>>(ca);
-  QM_CUDA(cudaGetLastError());
+  qmcrt_status e = launch_cand(s, g.frame, g.rect, sun, false, g.cand, g.cand_n, st);
+  if (e) return e;
   scan_kernel<<<1, 1024, 0, st>>>(g.cell_count, g.cell_start, s->cells, s->entry_cap, s->d_flag, g.field_yr);
   QM_CUDA(cudaGetLastError());
   fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, g.cellbox, g.cell_start, g.cell_count, g.entries,
@@ -900,6 +1093,10 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   if (s->coarse_cells) ALLOC(s->d_coarse_yr, (size_t)s->coarse_cells);
   ALLOC(s->d_cand, 2 * 3 * kCandCap * n);
   ALLOC(s->d_cand_n, 2 * n);
+  s->bucket_cap = 4 * (int64_t)n + 64;
+  ALLOC(s->d_buckets, 1);
+  ALLOC(s->d_bucket_start, (size_t)s->bucket_cap + 1);
+  ALLOC(s->d_bucket_ids, n);
   ALLOC(s->d_field_yr, 2);
   ALLOC(s->d_helio_weight, n);
   ALLOC(s->d_flag, 1);
@@ -932,7 +1129,8 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_pos); dev_free(s->d_size); dev_free(s->d_aim); dev_free(s->d_normal_in);
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
-  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_cand); dev_free(s->d_cand_n); dev_free(s->d_field_yr); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_cand); dev_free(s->d_cand_n); dev_free(s->d_field_yr);
+  dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)
@@ -1020,6 +1218,50 @@ qmcrt_status qmcrt_scene_read_geometry(qmcrt_scene* s, double* h_normals, double
     }
   }
   QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+static_assert(kCandCap == QMCRT_CAND_CAP, "candidate capacity of the C-ABI");
+
+qmcrt_status qmcrt_scene_read_candidates(qmcrt_scene* s, int32_t exhaustive, int32_t* h_counts, int32_t* h_ids,
+                                         void* stream) {
+  if (!s || !h_counts) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (s->sun_key.field_version != s->field_version)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "no sun set for the current field (qmcrt_scene_set_sun)");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)s->n;
+  float4* cand = s->d_cand;
+  int* cand_n = s->d_cand_n;
+  float4* tc = nullptr;
+  int* tn = nullptr;
+  if (exhaustive) {
+    qmcrt_status e = dev_alloc(&tc, 2 * 3 * kCandCap * n);
+    if (!e) e = dev_alloc(&tn, 2 * n);
+    double sd[3] = {s->sun_key.dir[0], s->sun_key.dir[1], s->sun_key.dir[2]};
+    const double l = std::sqrt(sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]);
+    for (int i = 0; i < 3; ++i) sd[i] /= l;  // as ensure_sun normalised it
+    if (!e) e = launch_cand(s, s->d_frame, s->d_rect, sd, true, tc, tn, st);
+    if (e) {
+      dev_free(tc);
+      dev_free(tn);
+      return e;
+    }
+    cand = tc;
+    cand_n = tn;
+  }
+  std::vector<float4> rec(h_ids ? 2 * 3 * kCandCap * n : 0);
+  cudaError_t ce = cudaMemcpyAsync(h_counts, cand_n, 2 * n * sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess && h_ids)
+    ce = cudaMemcpyAsync(rec.data(), cand, rec.size() * sizeof(float4), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  dev_free(tc);
+  dev_free(tn);
+  if (ce != cudaSuccess) return cuda_error(ce, "qmcrt_scene_read_candidates");
+  if (h_ids)
+    for (size_t l = 0; l < 2 * n; ++l)
+      for (int j = 0; j < kCandCap; ++j)
+        if (j < h_counts[l]) std::memcpy(h_ids + l * kCandCap + j, &rec[(l * kCandCap + j) * 3].w, sizeof(int32_t));
+        else h_ids[l * kCandCap + j] = -1;
   return QMCRT_OK;
 }
 

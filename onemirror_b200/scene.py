@@ -91,6 +91,15 @@ class SolarScene:
         capi.check(capi.lib().qmcrt_scene_read_grid(self.h, capi.as_i32p(start), capi.as_i32p(ent), _stream()))
         return start, ent[: start[-1]]
 
+    def read_candidates(self, exhaustive=False):
+        """Occluder candidates of the current sun: counts [n, 2] (shadow,
+        block) and ids [n, 2, 32] (-1 past the count)."""
+        counts = np.zeros((self.n, 2), np.int32)
+        ids = np.zeros((self.n, 2, capi.CAND_CAP), np.int32)
+        capi.check(capi.lib().qmcrt_scene_read_candidates(self.h, int(bool(exhaustive)), capi.as_i32p(counts),
+                                                          capi.as_i32p(ids), _stream()))
+        return counts, ids
+
     def read_geometry(self):
         nrm = np.zeros((self.n, 3))
         vert = np.zeros((self.n, 9))

@@ -391,6 +391,72 @@ def test_overflowing_candidate_lists_walk_the_grid():
     sc.close()
 
 
+def candidate_field(name):
+    if name == "batch4000":
+        return W.batched(rays_per_item=1 << 16)[0][2]
+    return W.small() if name == "small" else W.BUILDERS[name](rays=1 << 20)
+
+
+@pytest.mark.parametrize("name,elev,az", [("small", 45.0, 200.0), ("small", 0.4, 90.0), ("mid", 30.0, 200.0),
+                                          ("mid", 5.0, 120.0), ("mid", 0.3, 250.0), ("large", 20.0, 200.0),
+                                          ("large", 6.0, 45.0), ("batch4000", 10.0, 250.0)])
+def test_candidate_bucket_search_equals_every_pair(name, elev, az):
+    """The candidate search visits only the centre buckets a cone can reach;
+    its lists hold the same heliostats as testing every pair.  A 0.3-0.4 deg
+    sun makes shadow cones that do not rise, which visit every bucket."""
+    w = candidate_field(name)
+    sc = SolarScene.from_workload(w)
+    sc.set_sun(W.make_sun(elev, az, 1000.0, w.sun.csr))
+    c, ids = sc.read_candidates()
+    ce, ide = sc.read_candidates(exhaustive=True)
+    assert np.array_equal(c, ce)
+    assert c.sum() > 0
+    kept = c <= capi.CAND_CAP  # overflowing lists store only their first records, in search order
+    assert np.array_equal(np.sort(ids, axis=2)[kept], np.sort(ide, axis=2)[kept])
+    # a moved field rebuilds the buckets: move half the mirrors 0.5 m (within
+    # the grid's margin) and compare again
+    sc.pos[0::2, 0] += 0.5
+    sc.pos[1::2, 2] -= 0.5
+    sc.update_field()
+    sc.set_sun(W.make_sun(elev, az, 1000.0, w.sun.csr))
+    c2, ids2 = sc.read_candidates()
+    ce2, ide2 = sc.read_candidates(exhaustive=True)
+    kept = c2 <= capi.CAND_CAP
+    assert np.array_equal(c2, ce2)
+    assert np.array_equal(np.sort(ids2, axis=2)[kept], np.sort(ide2, axis=2)[kept])
+    sc.close()
+
+
+def test_wide_slope_error_takes_every_heliostat():
+    """A slope error so large (0.2 rad: the 6-sigma block cone passes 69
+    degrees) that no cone bounds the block rays: every other heliostat is a
+    block candidate, and a trace through the lists equals the grid walk."""
+    w = W.small()
+    n = 24
+    sc = SolarScene(w.pos[:n].copy(), w.size[:n].copy(), w.receiver, w.grid, sigma=0.2)
+    sun = W.make_sun(30.0, 200.0, 1000.0, w.sun.csr)
+    sc.set_sun(sun)
+    c, _ = sc.read_candidates()
+    assert np.all(c[:, 1] == n - 1)
+    ce, _ = sc.read_candidates(exhaustive=True)
+    assert np.array_equal(c, ce)
+    p = W.params(n * 16 * 256, 256, 0.3)
+    g = sc.trace(sun, p, records=True)
+    f, px, cnt = g["flags"].clone(), g["pixel"].clone(), g["counts"].clone()
+    p.kernel_variant = 5
+    g5 = sc.trace(sun, p, records=True)
+    assert torch.equal(f, g5["flags"]) and torch.equal(px, g5["pixel"]) and torch.equal(cnt, g5["counts"])
+    sc.close()
+
+
+def test_candidates_need_a_sun():
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    with pytest.raises(capi.QmcrtError):
+        sc.read_candidates()
+    sc.close()
+
+
 def test_smoothing_heaps_bit_exact_with_reference_gpu_kernel():
     """QMCRT_TRIM_HEAPS against ImageSmoother::image_smooth's output on a B200."""
     from test_oracle_pins import GV
