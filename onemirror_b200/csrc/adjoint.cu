@@ -259,6 +259,9 @@ __global__ void loss_kernel(LossArgs a) {
 
 __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(s * a.x + b.x, s * a.y + b.y, s * a.z + b.z); }
 
+// Component k (0..3, a compile-time constant after unrolling) of a float4.
+__device__ __forceinline__ float comp(float4 q, int k) { return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w; }
+
 template <bool CULL>
 __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const AdjArgs A) {
   __shared__ float s_tab[1025 + 1025 + 1024];
@@ -277,7 +280,12 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
   for (uint64_t r64 = ch * chunk + threadIdx.x, r1 = min((ch + 1) * chunk, end); r64 < r1; r64 += blockDim.x) {
     float gk[4] = {0.f, 0.f, 0.f, 0.f};
     int h = -1;
-    if (r64 < a.rays) {
+    if (r64 < a.rays && r64 < A.saved && A.tape[r64] == 0) {
+      // a ray the tape marks as lost contributes nothing; its heliostat still
+      // joins the warp's reduction below
+      const uint32_t ray = (uint32_t)r64;
+      h = __ldg(a.point_helio + (a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp));
+    } else if (r64 < a.rays) {
       const uint32_t ray = (uint32_t)r64;
       RaySetup R;
       ray_setup<false>(a, s_tab, s_guide, ray, R);
@@ -285,12 +293,9 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
       bool hit;
       Refl g;
       double u = 0, v = 0, tr = 0;
-      if (r64 < A.saved) {
-        hit = A.tape[r64] != 0;
-        if (hit) {  // rebuild the hit geometry without the traversals
-          g = reflect_ray(R);
-          hit = receiver_uv(a, R.o, g.rd, &u, &v, &tr);
-        }
+      if (r64 < A.saved) {  // the tape says hit: rebuild the geometry without the traversals
+        g = reflect_ray(R);
+        hit = receiver_uv(a, R.o, g.rd, &u, &v, &tr);
       } else {
         hit = ray_hits<CULL>(a, R, fy0, fy1, &g, &u, &v, &tr);
       }
@@ -309,28 +314,34 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         const float gWy = (1.f - fx) * (Gc[2] - Gc[0]) + fx * (Gc[3] - Gc[1]);
         // forward quantities in float
         const float3 npf = to_f(g.np), rdf = to_f(g.rd), wsf = to_f(R.ws);
-        const float lnp = (float)g.lnp, lr = (float)g.lr;
+        const float ilnp = (float)(1.0 / g.lnp), ilr = (float)(1.0 / g.lr);
         const float nws = dot(npf, wsf);
         const float sdn = dot(sd, npf);
         const float e = fabsf(sdn) * R.w, sg = sdn < 0.f ? -1.f : 1.f;
         // t along the reflected ray to the receiver plane (for d(hit) = do + t dr)
         const float3 cr = cross(E2, rdf);
-        const float den = dot(E1, cr);
+        const float iden = 1.f / dot(E1, cr);
         const float t = (float)tr;
-        const float* J = A.jac + 36 * h;
+        // the frame Jacobian, row-major [9][4]: row r holds d(frame component r)
+        // for the 4 parameters, one float4 (144-byte records, 16-byte aligned)
+        const float4* J = reinterpret_cast<const float4*>(A.jac) + 9 * h;
+        float4 Jr[9];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) Jr[r] = __ldg(J + r);
         const float x = R.xz.x, z = R.xz.y, hy = R.hy;
+#pragma unroll
         for (int k = 0; k < 4; ++k) {
-          const float3 du = f3(__ldg(J + 0 * 4 + k), __ldg(J + 1 * 4 + k), __ldg(J + 2 * 4 + k));
-          const float3 dn = f3(__ldg(J + 3 * 4 + k), __ldg(J + 4 * 4 + k), __ldg(J + 5 * 4 + k));
-          const float3 dv = f3(__ldg(J + 6 * 4 + k), __ldg(J + 7 * 4 + k), __ldg(J + 8 * 4 + k));
+          const float3 du = f3(comp(Jr[0], k), comp(Jr[1], k), comp(Jr[2], k));
+          const float3 dn = f3(comp(Jr[3], k), comp(Jr[4], k), comp(Jr[5], k));
+          const float3 dv = f3(comp(Jr[6], k), comp(Jr[7], k), comp(Jr[8], k));
           const float3 dO = fma3(x, du, fma3(hy, dn, z * dv));
           float3 dN = fma3(R.tl.x, du, fma3(R.tl.y, dn, R.tl.z * dv));
-          dN = (1.f / lnp) * (dN - dot(npf, dN) * npf);  // d(normalize)
+          dN = ilnp * (dN - dot(npf, dN) * npf);  // d(normalize)
           float3 dR = -2.f * (dot(dN, wsf) * npf + nws * dN);
-          dR = (1.f / lr) * (dR - dot(rdf, dR) * rdf);
+          dR = ilr * (dR - dot(rdf, dR) * rdf);
           const float3 b = dO + t * dR;  // d(hit point) = du E1 + dv E2 along the plane
-          const float duk = dot(b, cr) / den;
-          const float dvk = dot(E1, cross(b, rdf)) / den;
+          const float duk = dot(b, cr) * iden;
+          const float dvk = dot(E1, cross(b, rdf)) * iden;
           const float dpx = (float)a.res_x * dvk, dpy = (float)a.res_y * duk;
           const float dek = sg * dot(sd, dN) * R.w;
           gk[k] = dek * gW + e * (gWx * dpx + gWy * dpy);
