@@ -27,7 +27,7 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
 void buie_with_guide(float csr, BuieTable* t);
 
 constexpr int kAdjThreads = 256;
-constexpr int kAdjTileMax = 120;  // 57.6 KB of tile + 16 KB of Buie table: 3 CTAs per SM
+constexpr int kAdjTileMax = 112;  // 50.2 KB of tile + 20 KB of Buie table: 3 CTAs per SM
 
 // ------------------------------------------------------------ dual numbers
 // value + derivatives with respect to the 4 parameters of one heliostat
@@ -155,21 +155,30 @@ struct Refl {
   double lnp, lr;
 };
 
+// LENGTHS = false (the forward pass): rd keeps the length of the sun sample
+// (1 to float rounding) and the lengths are not formed; the receiver's
+// (u, v) and the visibility tests are scale-free in rd.
+template <bool LENGTHS = true>
 __device__ __forceinline__ Refl reflect_ray(const RaySetup& R) {
   Refl g;
   const d3 npr = apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z);
   const double q = dot(npr, npr), iq = rsqrt(q);
   g.np = iq * npr;
-  g.lnp = q * iq;
   const d3 rr = R.ws - (2.0 * dot(R.ws, g.np)) * g.np;
-  const double q2 = dot(rr, rr), iq2 = rsqrt(q2);
-  g.rd = iq2 * rr;
-  g.lr = q2 * iq2;
+  if (LENGTHS) {
+    g.lnp = q * iq;
+    const double q2 = dot(rr, rr), iq2 = rsqrt(q2);
+    g.rd = iq2 * rr;
+    g.lr = q2 * iq2;
+  } else {
+    g.rd = rr;
+    g.lnp = g.lr = 1.0;
+  }
   return g;
 }
 
 // Visibility and hit geometry of one ray (shadow, reflection, block, receiver).
-template <bool CULL>
+template <bool CULL, bool LENGTHS = true>
 __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, float fy0, float fy1, Refl* g,
                                          double* u, double* v, double* t) {
   // with CULL (corrected mode) the heliostat's occluder candidates answer the
@@ -180,7 +189,7 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
   if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc)
            : dda_blocked<false, false>(a, of, sd, R.h, fy0, fy1, nt, nc))
     return false;
-  *g = reflect_ray(R);
+  *g = reflect_ray<LENGTHS>(R);
   if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(g->rd), fy0, fy1, nt, nc)
            : dda_blocked<false, false>(a, of, to_f(g->rd), R.h, fy0, fy1, nt, nc))
     return false;
@@ -189,7 +198,7 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
 
 template <bool CULL>
 __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const AdjArgs A) {
-  __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
   // block-private tile of the energy map: many heliostats aim at the same
   // spot, so global atomics on it would queue at the hot pixels
@@ -210,7 +219,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
     ray_setup<false>(a, s_tab, s_guide, ray, R);
     Refl g;
     double u, v, t;
-    const bool hit = ray_hits<CULL>(a, R, fy0, fy1, &g, &u, &v, &t);
+    const bool hit = ray_hits<CULL, false>(a, R, fy0, fy1, &g, &u, &v, &t);
     if (r64 < A.saved) A.tape[r64] = hit ? 1 : 0;
     if (!hit) continue;
     float e = (float)fabs(g.np.x * a.sdir[0] + g.np.y * a.sdir[1] + g.np.z * a.sdir[2]) * R.w;
@@ -264,7 +273,7 @@ __device__ __forceinline__ float comp(float4 q, int k) { return k == 0 ? q.x : k
 
 template <bool CULL>
 __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const AdjArgs A) {
-  __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
   const TraceArgs& a = A.t;
   load_buie(a.buie, s_tab, s_guide);

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
                        int n_items, uint32_t chunk_rays, unsigned long long total_chunks,
                        unsigned long long* counter) {
   __shared__ TraceArgs s_a;
-  __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
   __shared__ unsigned long long s_c;
   __shared__ int s_item, s_anchor[3];

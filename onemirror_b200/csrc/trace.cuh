@@ -98,14 +98,16 @@ __device__ __forceinline__ int max_less_index(const float* cdf_y, float value) {
 // The interval index equals max_less_index's (the largest i with
 // cdf_y[i] <= uu): a guide table over uniform buckets of [0, core) gives a
 // lower bound, then a short forward scan finishes.
-__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float* s_tab, const int* s_guide, float u) {
+// The table is staged as one 16-byte record per interval, {angle, cdf,
+// slope, next interval's cdf}: each step of the scan is one shared load.
+__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float4* s_tab, const int* s_guide, float u) {
   float uu = u * a.b_total;
   if (uu < a.b_core) {
-    const float* cy = s_tab + 1025;
     int b = min((int)(uu * a.b_inv_bucket), kBuieBuckets - 1);
     int id = s_guide[b];
-    while (id < 1023 && cy[id + 1] <= uu) ++id;
-    return (uu - cy[id]) * s_tab[2050 + id] + s_tab[id];
+    float4 q = s_tab[id];
+    while (id < 1023 && q.w <= uu) q = s_tab[++id];
+    return (uu - q.y) * q.z + q.x;
   }
   // the aureole's analytic inverse (a few percent of the rays, but a warp
   // with one of them runs it): the hardware power, relative error ~2^-21,
@@ -373,9 +375,12 @@ struct GlobalDeposit {
   }
 };
 
-// Load the Buie table and its guide into shared memory (all threads).
-__device__ __forceinline__ void load_buie(const float* buie, float* s_tab, int* s_guide) {
-  for (int i = threadIdx.x; i < 3074; i += blockDim.x) s_tab[i] = __ldg(buie + i);
+// Load the Buie table and its guide into shared memory (all threads): the
+// table (angles [1025], cdf [1025], slopes [1024]) as one {angle, cdf, slope,
+// next cdf} record per interval.
+__device__ __forceinline__ void load_buie(const float* buie, float4* s_tab, int* s_guide) {
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x)
+    s_tab[i] = make_float4(__ldg(buie + i), __ldg(buie + 1025 + i), __ldg(buie + 2050 + i), __ldg(buie + 1026 + i));
   for (int i = threadIdx.x; i < kBuieBuckets; i += blockDim.x) s_guide[i] = __float_as_int(__ldg(buie + 3074 + i));
 }
 
@@ -396,7 +401,7 @@ struct RaySetup {
 // Sun sample and slope-error perturbation of ray `ray` from Philox (seed,
 // ray id): theta from the Buie inverse CDF, phi uniform; slope theta
 // Gaussian (Box-Muller), phi uniform (set_samplelights, set_perturbation).
-__device__ __forceinline__ void philox_samples(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
+__device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                                float sigma, float3* sl, float3* tl) {
   uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
   float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
@@ -418,7 +423,7 @@ __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float* 
 
 // Returns false for a ray to skip (table mode with an out-of-range heliostat id).
 template <bool TABLES>
-__device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
+__device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                           RaySetup& R) {
   const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
   const uint32_t j = ray - g * (uint32_t)a.rpp;
@@ -458,7 +463,7 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float* s_tab
 // of a two-level grid, 3 the per-heliostat occluder candidates (Philox
 // sampling only: their cones bound the sampler's directions).
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep>
-__device__ __forceinline__ void trace_ray(const TraceArgs& a, const float* s_tab, const int* s_guide, uint32_t ray,
+__device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit) {
   RaySetup R;
   if (!ray_setup<TABLES>(a, s_tab, s_guide, ray, R)) {
@@ -523,7 +528,7 @@ __device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned lo
 // The plain tracer: one grid-stride pass over the rays of one trace.
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
-  __shared__ float s_tab[1025 + 1025 + 1024];
+  __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   if (!TABLES) {
