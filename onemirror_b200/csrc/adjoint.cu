@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         float4 Jr[9];
 #pragma unroll
         for (int r = 0; r < 9; ++r) Jr[r] = __ldg(J + r);
-        const float x = R.xz.x, z = R.xz.y, hy = R.hy;
+        const float x = R.xz.x, z = R.xz.y, hy = 0.5f * __ldg(a.size + 3 * h + 1);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const float3 du = f3(comp(Jr[0], k), comp(Jr[1], k), comp(Jr[2], k));

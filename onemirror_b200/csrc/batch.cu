@@ -52,14 +52,13 @@ struct TileDeposit {
 __device__ bool chunk_anchor(const TraceArgs& a, uint32_t ray, int T, int* r0, int* c0) {
   const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
   const int h = __ldg(a.point_helio + g);
-  const double* F = a.frame + 9 * h;
+  const double* F = a.frame + kFrameStride * h;
   frame64 fr;
   fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
   fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
   fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
   const float2 xz = __ldg(a.point_xz + g);
-  d3 o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
-         apply(fr, (double)xz.x, 0.5 * __ldg(a.size + 3 * h + 1), (double)xz.y);
+  d3 o = mk(__ldg(F + 9), __ldg(F + 10), __ldg(F + 11)) + (double)xz.x * fr.u + (double)xz.y * fr.v;
   d3 s = mk(a.sdir[0], a.sdir[1], a.sdir[2]);
   d3 rd = s - (2.0 * dot(s, fr.n)) * fr.n;
   int pix = -1;

@@ -37,6 +37,10 @@ QMCRT_HD d3 to_d(float3 a) { return mk(a.x, a.y, a.z); }
 
 // Frame applied to a local vector: out = d.x*u + d.y*n + d.z*v, the matrix of
 // local2world (global_function.cuh:47-49).
+// Doubles per heliostat in the per-sun frame array: the local2world axes
+// u, n, v and the mirror centre c = pos + n * thickness / 2.
+constexpr int kFrameStride = 12;
+
 struct frame64 {
   d3 u, n, v;
 };

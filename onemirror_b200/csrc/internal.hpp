@@ -68,7 +68,7 @@ struct CandBuckets {
 
 struct SunGeom {
   double* normal = nullptr;      // [3n]
-  double* frame = nullptr;       // [9n] u, n, v
+  double* frame = nullptr;       // [kFrameStride n] u, n, v, mirror centre
   float4* rect = nullptr;        // [3n] A(v0)+id, E1, E2
   int4* cellbox = nullptr;       // [2n]
   int32_t* cell_count = nullptr; // [cells]
@@ -134,7 +134,7 @@ struct qmcrt_scene {
   float *d_sigma = nullptr, *d_tilt = nullptr;
   // per-sun geometry
   double* d_normal = nullptr;   // [3n]
-  double* d_frame = nullptr;    // [9n] u, n, v
+  double* d_frame = nullptr;    // [kFrameStride n] u, n, v, mirror centre
   float4* d_rect = nullptr;     // [3n] A(v0)+id, E1, E2 (float)
   int4* d_cellbox = nullptr;    // [2n] lo, hi cell indices per heliostat
   int32_t* d_cell_count = nullptr;  // [cells]

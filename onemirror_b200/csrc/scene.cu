@@ -77,11 +77,13 @@ __global__ void aim_kernel(AimArgs a) {
     a.normal[3 * h] = n.x;
     a.normal[3 * h + 1] = n.y;
     a.normal[3 * h + 2] = n.z;
-    double* fr = a.frame + 9 * h;
+    double* fr = a.frame + kFrameStride * h;
     fr[0] = f.u.x; fr[1] = f.u.y; fr[2] = f.u.z;
     fr[3] = f.n.x; fr[4] = f.n.y; fr[5] = f.n.z;
     fr[6] = f.v.x; fr[7] = f.v.y; fr[8] = f.v.z;
     double sx = a.size[3 * h], sy = a.size[3 * h + 1], sz = a.size[3 * h + 2];
+    const d3 c = p + (sy / 2) * f.n;  // the mirror centre: sample points are c + u x + v z
+    fr[9] = c.x; fr[10] = c.y; fr[11] = c.z;
     // Cset_localvertex + Cset_worldvertex (heliostat.cpp:30-49): v0, v1, v3
     d3 v0 = p + apply(f, -sx / 2, sy / 2, -sz / 2);
     d3 v1 = p + apply(f, -sx / 2, sy / 2, sz / 2);
@@ -350,7 +352,7 @@ struct Cone {
 __device__ __forceinline__ Cone walk_cone(const CandArgs& a, int h, int walk) {
   const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
   if (walk == 0) return Cone{mk(-s.x, -s.y, -s.z), a.shadow_tan, a.shadow_rise, false};
-  const double* F = a.frame + 9 * h;
+  const double* F = a.frame + kFrameStride * h;
   const d3 nh = mk(F[3], F[4], F[5]);
   const d3 db = s - (2.0 * dot(s, nh)) * nh;
   const double ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
@@ -770,7 +772,7 @@ qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g) {
     return e;                           \
   }
   GALLOC(g->normal, 3 * n);
-  GALLOC(g->frame, 9 * n);
+  GALLOC(g->frame, kFrameStride * n);
   GALLOC(g->rect, 3 * n);
   GALLOC(g->cellbox, 2 * n);
   GALLOC(g->cell_count, (size_t)s->cells);
@@ -1082,7 +1084,7 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   if (s->has_tilt) ALLOC(s->d_tilt, 2 * n);
   ALLOC(s->d_sigma, n);
   ALLOC(s->d_normal, 3 * n);
-  ALLOC(s->d_frame, 9 * n);
+  ALLOC(s->d_frame, kFrameStride * n);
   ALLOC(s->d_rect, 3 * n);
   ALLOC(s->d_cellbox, 2 * n);
   ALLOC(s->d_cell_count, (size_t)s->cells);
@@ -1204,11 +1206,11 @@ qmcrt_status qmcrt_scene_read_geometry(qmcrt_scene* s, double* h_normals, double
   cudaStream_t st = (cudaStream_t)stream;
   if (h_normals) QM_CUDA(cudaMemcpyAsync(h_normals, s->d_normal, 3 * (size_t)s->n * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (h_vertices) {
-    std::vector<double> fr(9 * (size_t)s->n);
+    std::vector<double> fr(kFrameStride * (size_t)s->n);
     QM_CUDA(cudaMemcpyAsync(fr.data(), s->d_frame, fr.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     QM_CUDA(cudaStreamSynchronize(st));
     for (int h = 0; h < s->n; ++h) {
-      const double* f = fr.data() + 9 * h;
+      const double* f = fr.data() + kFrameStride * h;
       double sx = s->h_size[3 * h], sy = s->h_size[3 * h + 1], sz = s->h_size[3 * h + 2];
       const double loc[3][3] = {{-sx / 2, sy / 2, -sz / 2}, {-sx / 2, sy / 2, sz / 2}, {sx / 2, sy / 2, -sz / 2}};
       for (int k = 0; k < 3; ++k)

@@ -20,7 +20,7 @@ struct TraceArgs {
   const float* buie;
   float b_total, b_core, b_B, b_C, b_inv, b_inv_bucket;
   // field
-  const double* frame;  // [9n]
+  const double* frame;  // [kFrameStride n] u, n, v, mirror centre
   const float* pos;
   const float* size;
   const float* sigma;
@@ -390,7 +390,6 @@ __device__ __forceinline__ void load_buie(const float* buie, float4* s_tab, int*
 struct RaySetup {
   int h;
   float2 xz;
-  float hy;
   frame64 fr;
   d3 o;
   float3 sl, tl;
@@ -431,13 +430,12 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
   if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
   R.h = h;
   R.xz = __ldg(a.point_xz + g);
-  const double* F = a.frame + 9 * h;
+  const double* F = a.frame + kFrameStride * h;
   R.fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
   R.fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
   R.fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
-  R.hy = 0.5f * __ldg(a.size + 3 * h + 1);
-  R.o = mk(__ldg(a.pos + 3 * h), __ldg(a.pos + 3 * h + 1), __ldg(a.pos + 3 * h + 2)) +
-        apply(R.fr, (double)R.xz.x, (double)R.hy, (double)R.xz.y);
+  // origin: the mirror centre plus the point's in-plane offset
+  R.o = mk(__ldg(F + 9), __ldg(F + 10), __ldg(F + 11)) + (double)R.xz.x * R.fr.u + (double)R.xz.y * R.fr.v;
   R.w = 1.f;
   if (TABLES) {
     // (start + j) mod T, kept in [0, T) for any caller-provided start
