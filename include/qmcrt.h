@@ -519,6 +519,11 @@ qmcrt_status qmcrt_fp32_peak_probe(float* d_sink, int32_t iters, double* flops, 
 qmcrt_status qmcrt_philox_blocks(const uint32_t ctr0[4], const uint32_t key[2], int64_t n,
                                  uint32_t* d_out, void* stream);
 
+/* The tracer's double-precision reciprocal and reciprocal square root (the
+ * receiver determinant, the perturbed normal's length) on n device values
+ * (test hook): d_rcp[i] = 1/x, d_rsqrt[i] = 1/sqrt(x); either may be NULL. */
+qmcrt_status qmcrt_fp64_recip_probe(const double* d_x, int64_t n, double* d_rcp, double* d_rsqrt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -140,6 +140,7 @@ PROTOTYPES = {
     "qmcrt_scene_read_grid": (C.c_int, [C.c_void_p, i32p, i32p, C.c_void_p]),
     "qmcrt_scene_read_geometry": (C.c_int, [C.c_void_p, dp, dp, C.c_void_p]),
     "qmcrt_scene_read_candidates": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, C.c_void_p]),
+    "qmcrt_fp64_recip_probe": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "qmcrt_scene_sample_points": (C.c_int, [C.c_void_p, C.POINTER(TraceParams), C.POINTER(C.c_int64), C.c_void_p]),
     "qmcrt_scene_read_points": (C.c_int, [C.c_void_p, fp, i32p, C.c_void_p]),
     "qmcrt_sample_points_noalloc": (C.c_int, [fp, C.c_int32, C.c_int64, C.c_float, C.c_uint64, C.c_void_p,

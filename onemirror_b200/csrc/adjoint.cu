@@ -136,7 +136,7 @@ __device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, doub
   d3 pv = cross(d, E2);
   double det = dot(E1, pv);
   if (fabs(det) < 1e-6) return false;
-  double inv = 1.0 / det;
+  double inv = rcp_nr(det);
   d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
   *u = dot(T, pv) * inv;
   if (*u < 0 || *u > 1) return false;
@@ -162,12 +162,12 @@ template <bool LENGTHS = true>
 __device__ __forceinline__ Refl reflect_ray(const RaySetup& R) {
   Refl g;
   const d3 npr = apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z);
-  const double q = dot(npr, npr), iq = rsqrt(q);
+  const double q = dot(npr, npr), iq = rsqrt_nr(q);
   g.np = iq * npr;
   const d3 rr = R.ws - (2.0 * dot(R.ws, g.np)) * g.np;
   if (LENGTHS) {
     g.lnp = q * iq;
-    const double q2 = dot(rr, rr), iq2 = rsqrt(q2);
+    const double q2 = dot(rr, rr), iq2 = rsqrt_nr(q2);
     g.rd = iq2 * rr;
     g.lr = q2 * iq2;
   } else {

@@ -26,6 +26,13 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(float* sink, int iters, 
   if (s == 1.2345f) sink[blockIdx.x] = s;  // never true for the probe's inputs; keeps the chains live
 }
 
+__global__ void recip_kernel(const double* x, int64_t n, double* rcp, double* rsq) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (rcp) rcp[i] = rcp_nr(x[i]);
+  if (rsq) rsq[i] = rsqrt_nr(x[i]);
+}
+
 __global__ void philox_kernel(uint4 c0, uint2 key, int64_t n, uint4* out) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -47,6 +54,13 @@ qmcrt_status qmcrt_fp32_peak_probe(float* d_sink, int32_t iters, double* flops, 
   fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d_sink, iters, 0.999999f, 1e-7f);
   QM_CUDA(cudaGetLastError());
   *flops = 2.0 * kChains * (double)iters * 256.0 * blocks;
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_fp64_recip_probe(const double* d_x, int64_t n, double* d_rcp, double* d_rsqrt, void* stream) {
+  if (!d_x || n <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  recip_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_x, n, d_rcp, d_rsqrt);
+  QM_CUDA(cudaGetLastError());
   return QMCRT_OK;
 }
 

@@ -331,7 +331,7 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
     d3 pv = cross(d, E2);
     double det = dot(E1, pv);
     if (fabs(det) < 1e-6) return false;
-    double inv = 1.0 / det;
+    double inv = rcp_nr(det);
     d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
     u = dot(T, pv) * inv;
     if (u < 0 || u > 1) return false;
@@ -357,7 +357,7 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
 }
 
 __device__ __forceinline__ d3 rnorm(d3 a) {
-  double r = rsqrt(dot(a, a));
+  double r = rsqrt_nr(dot(a, a));
   return r * a;
 }
 
