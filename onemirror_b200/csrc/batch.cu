@@ -220,6 +220,11 @@ struct qmcrt_batch {
   qmcrt_batch_tuning tuning{65536, 4, 0, 0.f};
   int sms = 148;
   cudaStream_t cap_stream = nullptr;
+  // the items' geometry is rebuilt on kGeomStreams side streams forked from
+  // the pass's stream and joined before the trace (parallel graph branches)
+  static constexpr int kGeomStreams = 8;
+  cudaStream_t side[kGeomStreams] = {};
+  cudaEvent_t fork = nullptr, join[kGeomStreams] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -262,10 +267,21 @@ static qmcrt_status enqueue_trace(qmcrt_batch* b, int n, cudaStream_t st) {
 
 static qmcrt_status enqueue_pass(qmcrt_batch* b, cudaStream_t st) {
   qmcrt_status e;
-  for (auto& it : b->items) {
-    if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, st))) return e;
-    QM_CUDA(cudaMemsetAsync(it.d_counts, 0, it.res * sizeof(uint32_t), st));
-    QM_CUDA(cudaMemsetAsync(it.d_energy, 0, it.res * sizeof(float), st));
+  // every item's geometry depends only on its own sun and scene: the small
+  // kernels of different items run side by side
+  constexpr int K = qmcrt_batch::kGeomStreams;
+  QM_CUDA(cudaEventRecord(b->fork, st));
+  for (int j = 0; j < K; ++j) QM_CUDA(cudaStreamWaitEvent(b->side[j], b->fork, 0));
+  for (size_t i = 0; i < b->items.size(); ++i) {
+    auto& it = b->items[i];
+    cudaStream_t s = b->side[i % K];
+    if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, s))) return e;
+    QM_CUDA(cudaMemsetAsync(it.d_counts, 0, it.res * sizeof(uint32_t), s));
+    QM_CUDA(cudaMemsetAsync(it.d_energy, 0, it.res * sizeof(float), s));
+  }
+  for (int j = 0; j < K; ++j) {
+    QM_CUDA(cudaEventRecord(b->join[j], b->side[j]));
+    QM_CUDA(cudaStreamWaitEvent(st, b->join[j], 0));
   }
   QM_CUDA(cudaMemsetAsync(b->d_intercepted, 0, b->items.size() * sizeof(double), st));
   if ((e = enqueue_trace(b, -1, st))) return e;
@@ -383,6 +399,11 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     cudaError_t ce = cudaMemcpy(b->d_args, args.data(), n_items * sizeof(TraceArgs), cudaMemcpyHostToDevice);
     if (ce == cudaSuccess) ce = cudaMemcpy(b->d_fin, fin.data(), n_items * sizeof(BatchFinalize), cudaMemcpyHostToDevice);
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    for (int j = 0; j < qmcrt_batch::kGeomStreams && ce == cudaSuccess; ++j) {
+      ce = cudaStreamCreateWithFlags(&b->side[j], cudaStreamNonBlocking);
+      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->join[j], cudaEventDisableTiming);
+    }
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (ce != cudaSuccess) { e = cuda_error(ce, "batch upload"); goto fail; }
   }
   if ((e = upload_chunks(b, nullptr))) goto fail;
@@ -412,6 +433,11 @@ qmcrt_status qmcrt_batch_destroy(qmcrt_batch* b) {
   cudaFree(b->d_counter);
   cudaFree(b->d_intercepted);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  for (int j = 0; j < qmcrt_batch::kGeomStreams; ++j) {
+    if (b->side[j]) cudaStreamDestroy(b->side[j]);
+    if (b->join[j]) cudaEventDestroy(b->join[j]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   delete b;
   return QMCRT_OK;
 }
