@@ -41,8 +41,8 @@ struct TileDeposit {
       atomicAdd(s_cnt + r * T + c, 1u);
       atomicAdd(s_en + r * T + c, e);
     } else {
-      atomicAdd(counts + pix, 1u);
-      atomicAdd(energy + pix, e);
+      red_add(counts + pix, 1u);
+      red_add(energy + pix, e);
     }
   }
 };
@@ -144,8 +144,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
           if (k) {
             int pr = s_anchor[0] + i / T, pc = s_anchor[1] + i % T;
             int pix = pr * s_a.res_x + pc;
-            atomicAdd(s_a.counts + pix, k);
-            atomicAdd(s_a.energy + pix, s_en[i]);
+            red_add(s_a.counts + pix, k);
+            red_add(s_a.energy + pix, s_en[i]);
             s_cnt[i] = 0;
             s_en[i] = 0.f;
           }

@@ -56,6 +56,18 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
   return fma(0.5 * y, fma(-x * y, y, 1.0), y);
 }
 
+// Additions to global memory without a returned value (red.global).  A batch
+// item's map pointers are read from shared memory, where the compiler cannot
+// see that they address global memory and would emit returning atomics.
+__device__ __forceinline__ void red_add(uint32_t* p, uint32_t v) {
+  asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.u32 [g], %1;\n\t}"
+               :: "l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(float* p, float v) {
+  asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f32 [g], %1;\n\t}"
+               :: "l"(p), "f"(v) : "memory");
+}
+
 // Doubles per heliostat in the per-sun frame array: the local2world axes
 // u, n, v and the mirror centre c = pos + n * thickness / 2.
 constexpr int kFrameStride = 12;

@@ -143,6 +143,7 @@ struct qmcrt_scene {
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
   int4* d_cell_info = nullptr;      // [cells] run of each cell's rectangles and their height range
   float2* d_coarse_yr = nullptr;    // [coarse_cells] the same per coarse cell (two-level grid)
+  double2* d_cyl_edge = nullptr;    // cylinder receivers: [res_x] direction of each column's first edge
   float4* d_cand = nullptr;         // [n][2][kCandCap][3] occluder candidates' rectangle records (shadow, block)
   int* d_cand_n = nullptr;          // [n][2]
   int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)

@@ -1100,6 +1100,16 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_bucket_start, (size_t)s->bucket_cap + 1);
   ALLOC(s->d_bucket_ids, n);
   ALLOC(s->d_field_yr, 2);
+  if (recv->type == QMCRT_RECEIVER_CYLINDER) {
+    ALLOC(s->d_cyl_edge, (size_t)recv->res_x);
+    std::vector<double2> edge(recv->res_x);
+    for (int k = 0; k < recv->res_x; ++k) {
+      const double a = 2.0 * 3.141592653589793 * k / recv->res_x;
+      edge[k] = make_double2(std::cos(a), std::sin(a));
+    }
+    cudaError_t ce = cudaMemcpy(s->d_cyl_edge, edge.data(), edge.size() * sizeof(double2), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) { e = cuda_error(ce, "cylinder column edges"); goto fail; }
+  }
   ALLOC(s->d_helio_weight, n);
   ALLOC(s->d_flag, 1);
   ALLOC(s->d_counts, res);
@@ -1132,7 +1142,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
   dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_cand); dev_free(s->d_cand_n); dev_free(s->d_field_yr);
-  dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_cyl_edge); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

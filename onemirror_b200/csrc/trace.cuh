@@ -47,6 +47,7 @@ struct TraceArgs {
   int rtype;
   double rA[3], rE1[3], rE2[3];
   double cyl[5];
+  const double2* cyl_edge;  // cylinder: [res_x] (cos, sin) of each column's first edge, 2 pi k / res_x
   int res_x, res_y;
   // rays
   int n_helio;
@@ -321,11 +322,26 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
       y = o.y + t * d.y - a.cyl[1];
       if (t < 1e-6 || y < 0 || y > H) return false;
     }
-    double phi = atan2(oz + t * d.z, ox + t * d.x);
-    if (phi < 0) phi += 2.0 * 3.141592653589793;
     if (t_out) *t_out = t;
     u = y / H;
-    v = phi / (2.0 * 3.141592653589793);
+    // column = floor(phi / 2 pi * res_x), phi = atan2(Z, X) in [0, 2 pi):
+    // the single-precision angle picks a column within one of the right one;
+    // the signs of the hit's FP64 cross products with that column's edges
+    // (directions at 2 pi k / res_x) settle it.  Both edges lie within two
+    // columns of the hit, where sign(cos a Z - sin a X) = sign(sin(phi - a)).
+    const double X = ox + t * d.x, Z = oz + t * d.z;
+    float pf = atan2f((float)Z, (float)X);
+    if (pf < 0.f) pf += 6.28318531f;
+    int c = min(max((int)(pf * (float)a.res_x * 0.159154943f), 0), a.res_x - 1);
+    const double2 e0 = __ldg(a.cyl_edge + c);
+    if (e0.x * Z - e0.y * X < 0.0) {
+      c = c == 0 ? a.res_x - 1 : c - 1;
+    } else {
+      const int c1 = c + 1 == a.res_x ? 0 : c + 1;
+      const double2 e1 = __ldg(a.cyl_edge + c1);
+      if (e1.x * Z - e1.y * X >= 0.0) c = c1;
+    }
+    v = (c + 0.5) / a.res_x;  // the column's centre: (int)(v * res_x) == c
   } else {
     d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
     d3 pv = cross(d, E2);
@@ -370,8 +386,8 @@ struct GlobalDeposit {
   uint32_t* counts;
   float* energy;
   __device__ __forceinline__ void operator()(int pix, float e) const {
-    atomicAdd(counts + pix, 1u);
-    atomicAdd(energy + pix, e);
+    red_add(counts + pix, 1u);
+    red_add(energy + pix, e);
   }
 };
 
