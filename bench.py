@@ -278,6 +278,32 @@ def batch_section(reps=3):
     e1.record()
     e1.synchronize()
     seq_ms = e0.elapsed_time(e1) / reps
+
+    # The reference's structure (ray_tracing.cu:23-27): one launch and one
+    # device synchronisation per heliostat.  Each heliostat's rays are one
+    # range of the item's rays; timed on the host clock for the day's middle
+    # sun position on all three fields, then scaled to the 45 positions.
+    mid_sun = suns[len(suns) // 2][3]
+    ph_out = [scenes[k]._outputs(0, False) for k in range(len(scenes))]
+    ph = []
+    for k, sc in enumerate(scenes):
+        _, helio = sc.read_points()
+        bounds = np.concatenate([[0], np.cumsum(np.bincount(helio, minlength=sc.n))]) * params.rays_per_point
+        p = W.params(int(params.rays), params.rays_per_point, params.point_spacing, seed=params.seed)
+        p.accumulate = 1
+        ph.append((sc, bounds, p))
+
+    def per_heliostat():
+        for k, (sc, bounds, p) in enumerate(ph):
+            for h in range(sc.n):
+                p.ray_begin, p.ray_end = int(bounds[h]), int(bounds[h + 1])
+                sc.trace(mid_sun, p, stats=False, outputs=ph_out[k])
+                torch.cuda.synchronize()
+
+    per_heliostat()
+    t0 = time.perf_counter()
+    per_heliostat()
+    ph_ms = (time.perf_counter() - t0) * 1e3 * len(suns)
     b.close()
     for s in scenes:
         s.close()
@@ -285,6 +311,11 @@ def batch_section(reps=3):
             "rays_per_item": int(params.rays), "batched_ms": batched_ms, "sequential_ms": seq_ms,
             "batched_rays_per_s": rays / (batched_ms * 1e-3), "sequential_rays_per_s": rays / (seq_ms * 1e-3),
             "speedup_vs_sequential": seq_ms / batched_ms,
+            "per_heliostat_ms": ph_ms, "speedup_vs_per_heliostat": ph_ms / batched_ms,
+            "per_heliostat_launches": sum(f.n for f in fields) * len(suns),
+            "per_heliostat_method": "one qmcrt_trace of a heliostat's ray range + device synchronise per heliostat "
+                                    "(the reference's launch structure), host clock, the middle sun position on all "
+                                    "3 fields x %d positions" % len(suns),
             "tuning": {"chunk_rays": tuning.chunk_rays, "ctas_per_sm": tuning.ctas_per_sm, "tile": tuning.tile}}
 
 

@@ -170,6 +170,13 @@ typedef struct qmcrt_trace_params {
   uint32_t item;           /* Philox stream (counter word 2): distinct items give independent ray sets
                               (shards of one trace, items of a batch) */
   int32_t attenuation;     /* QMCRT_ATTEN_*: atmospheric transmittance of the mirror-to-receiver leg */
+  uint64_t ray_begin;      /* trace only the rays [ray_begin, ray_end) of the full set: the same
+                              rays, points and deposits as the whole trace restricted to them (rays
+                              are numbered point-major and points by heliostat, so one heliostat's
+                              rays are one range: the reference's per-heliostat launches,
+                              ray_tracing.cu:23-27); ray_end = 0: all rays.  Statistics count the
+                              range's rays; total_power stays the whole field's. */
+  uint64_t ray_end;
 } qmcrt_trace_params;
 
 /* Device outputs of a trace.  Any pointer may be NULL. */

@@ -58,7 +58,8 @@ class TraceParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("rays", C.c_uint64), ("rays_per_point", C.c_int32),
                 ("point_mode", C.c_int32), ("point_spacing", C.c_float), ("reflectivity", C.c_float),
                 ("quirks", C.c_uint32), ("deposit", C.c_int32), ("accumulate", C.c_int32),
-                ("kernel_variant", C.c_int32), ("item", C.c_uint32), ("attenuation", C.c_int32)]
+                ("kernel_variant", C.c_int32), ("item", C.c_uint32), ("attenuation", C.c_int32),
+                ("ray_begin", C.c_uint64), ("ray_end", C.c_uint64)]
 
 
 class Outputs(C.Structure):

@@ -437,6 +437,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint traces in corrected mode");
   if (p->attenuation != QMCRT_ATTEN_NONE)
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint has no attenuation term");
+  if (p->ray_end != 0) return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint traces every ray");
   if (!(sun->csr > 0.f && sun->csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   cudaStream_t st = (cudaStream_t)stream;
   // a tape from an earlier call keeps its buffers where they are large enough

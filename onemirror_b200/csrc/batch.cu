@@ -314,6 +314,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "batches trace in corrected mode only");
   if (params->attenuation != QMCRT_ATTEN_NONE && params->attenuation != QMCRT_ATTEN_POLY_EXP)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
+  if (params->ray_end != 0) return set_error(QMCRT_ERR_NOT_SUPPORTED, "batch items trace every ray");
   if (params->point_mode != QMCRT_POINTS_POISSON || params->rays_per_point <= 0 || params->rays == 0 ||
       params->rays > 0xFFFFFFFFull)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "batches need Poisson points and 0 < rays < 2^32");

@@ -73,7 +73,7 @@ static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTraceThreads, 0);
   if (e != cudaSuccess) return e;
   int64_t blocks = (int64_t)std::max(per_sm, 1) * sm_count();
-  int64_t need = ((int64_t)a.rays + kTraceThreads - 1) / kTraceThreads;
+  int64_t need = ((int64_t)a.rays - a.ray0 + kTraceThreads - 1) / kTraceThreads;
   blocks = std::max<int64_t>(1, std::min(blocks, need));
   k<<<(unsigned)blocks, kTraceThreads, 0, st>>>(a);
   return cudaGetLastError();
@@ -236,6 +236,19 @@ static qmcrt_status check_params(const qmcrt_trace_params* p) {
   if (p->kernel_variant < 0 || p->kernel_variant > 5) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "kernel_variant must be 0..5");
   if (p->attenuation != QMCRT_ATTEN_NONE && p->attenuation != QMCRT_ATTEN_POLY_EXP)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
+  if (p->ray_end != 0 && p->ray_begin >= p->ray_end)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray range must have ray_begin < ray_end");
+  return QMCRT_OK;
+}
+
+// The range [ray_begin, ray_end) of a trace of `total` rays (all of them when ray_end is 0).
+static qmcrt_status apply_range(const qmcrt_trace_params* p, uint64_t total, TraceArgs* a) {
+  a->rays = (uint32_t)total;
+  a->ray0 = 0;
+  if (p->ray_end == 0) return QMCRT_OK;
+  if (p->ray_end > total) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray_end is past the trace's last ray");
+  a->ray0 = (uint32_t)p->ray_begin;
+  a->rays = (uint32_t)p->ray_end;
   return QMCRT_OK;
 }
 
@@ -324,7 +337,7 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   TraceArgs a{};
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
   a.atten = p->attenuation;
-  a.rays = (uint32_t)(s->points * (int64_t)p->rays_per_point);
+  if ((e = apply_range(p, (uint64_t)s->points * (uint64_t)p->rays_per_point, &a))) return e;
   a.rpp = p->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);
   a.key = make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32));
@@ -351,7 +364,7 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcr
   TraceArgs a{};
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
   a.atten = p->attenuation;
-  a.rays = (uint32_t)(t->points * t->rays_per_point);
+  if ((e = apply_range(p, (uint64_t)t->points * (uint64_t)t->rays_per_point, &a))) return e;
   a.rpp = t->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);
   a.point_xz = (const float2*)t->d_point_xz;

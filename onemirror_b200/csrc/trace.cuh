@@ -51,7 +51,8 @@ struct TraceArgs {
   int res_x, res_y;
   // rays
   int n_helio;
-  uint32_t rays;
+  uint32_t rays;  // one past the last ray traced
+  uint32_t ray0;  // the first ray traced (a range of the full set; 0 for whole traces)
   int rpp;
   int rpp_shift;  // log2(rpp) when rpp is a power of two, else -1
   uint2 key;
@@ -555,10 +556,11 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   // rays per point) taken grid-stride: a CTA stays on one heliostat for most
   // of a chunk, so its frame and candidates stay in L1, and the chunks are
   // small enough to keep the SMs evenly loaded
-  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = ((uint64_t)a.rays + chunk - 1) / chunk;
+  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x,
+                 nch = ((uint64_t)a.rays - a.ray0 + chunk - 1) / chunk;
   for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-    const uint64_t r1 = min((ch + 1) * chunk, (uint64_t)a.rays);
-    for (uint64_t r64 = ch * chunk + threadIdx.x; r64 < r1; r64 += blockDim.x)
+    const uint64_t r0 = a.ray0 + ch * chunk, r1 = min(r0 + chunk, (uint64_t)a.rays);
+    for (uint64_t r64 = r0 + threadIdx.x; r64 < r1; r64 += blockDim.x)
       trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep);
   }
   if (STATS) flush_counters(c, a.stats);

@@ -196,3 +196,44 @@ def test_fp64_reciprocals_within_bound():
     q = rsq.cpu().numpy()
     assert np.max(np.abs(r * x - 1.0)) < 3e-12
     assert np.max(np.abs(q * np.sqrt(x[pos]) - 1.0)) < 3e-12
+
+
+def test_ray_range_traces_the_same_rays():
+    """qmcrt_trace_params.ray_begin/ray_end: one heliostat's rays (one range,
+    as the reference launches them) give the whole trace's flags and pixels
+    for those rays, count maps that add up to the whole trace's, and
+    statistics of the range alone."""
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    g = sc.trace(w.sun, p, records=True)
+    f_all, px_all = g["flags"].cpu().numpy(), g["pixel"].cpu().numpy()
+    c_all = g["counts"].cpu().numpy().astype(np.int64)
+    _, helio = sc.read_points()
+    bounds = np.concatenate([[0], np.cumsum(np.bincount(helio, minlength=w.n))]) * p.rays_per_point
+    total = np.zeros_like(c_all)
+    for h in (0, 1, w.n // 2, w.n - 1):
+        p.ray_begin, p.ray_end = int(bounds[h]), int(bounds[h + 1])
+        r = sc.trace(w.sun, p, records=True)
+        b, e = p.ray_begin, p.ray_end
+        assert np.array_equal(r["flags"].cpu().numpy()[b:e], f_all[b:e])
+        assert np.array_equal(r["pixel"].cpu().numpy()[b:e], px_all[b:e])
+        assert r["stats"].rays == e - b
+        pix = px_all[b:e]
+        want = np.bincount(pix[pix >= 0], minlength=c_all.size).reshape(c_all.shape)
+        assert np.array_equal(r["counts"].cpu().numpy().astype(np.int64), want)
+    # every heliostat's range, accumulated, is the whole trace
+    p.accumulate = 1
+    outs = sc._outputs(int(p.rays), False)
+    for h in range(w.n):
+        p.ray_begin, p.ray_end = int(bounds[h]), int(bounds[h + 1])
+        sc.trace(w.sun, p, stats=False, outputs=outs)
+    total = outs[1]["counts"].cpu().numpy().astype(np.int64)
+    assert np.array_equal(total, c_all)
+    p.accumulate = 0
+    for bad in ((5, 5), (10, int(p.rays) + 1)):
+        p.ray_begin, p.ray_end = bad
+        with pytest.raises(capi.QmcrtError):
+            sc.trace(w.sun, p)
+    p.ray_begin = p.ray_end = 0
+    sc.close()
