@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work budget of the oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling runs; multiple of 256)")
     ap.add_argument("--variant", type=int, default=0, help="trace kernel variant (qmcrt_trace_params.kernel_variant)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-versus-sequential section")
