@@ -449,12 +449,15 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
   if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
   R.h = h;
   R.xz = __ldg(a.point_xz + g);
-  const double* F = a.frame + kFrameStride * h;
-  R.fr.u = mk(__ldg(F + 0), __ldg(F + 1), __ldg(F + 2));
-  R.fr.n = mk(__ldg(F + 3), __ldg(F + 4), __ldg(F + 5));
-  R.fr.v = mk(__ldg(F + 6), __ldg(F + 7), __ldg(F + 8));
+  // the 96-byte frame record (16-byte aligned) as six 16-byte loads
+  const double2* F = reinterpret_cast<const double2*>(a.frame + kFrameStride * h);
+  const double2 q0 = __ldg(F), q1 = __ldg(F + 1), q2 = __ldg(F + 2), q3 = __ldg(F + 3), q4 = __ldg(F + 4),
+                q5 = __ldg(F + 5);
+  R.fr.u = mk(q0.x, q0.y, q1.x);
+  R.fr.n = mk(q1.y, q2.x, q2.y);
+  R.fr.v = mk(q3.x, q3.y, q4.x);
   // origin: the mirror centre plus the point's in-plane offset
-  R.o = mk(__ldg(F + 9), __ldg(F + 10), __ldg(F + 11)) + (double)R.xz.x * R.fr.u + (double)R.xz.y * R.fr.v;
+  R.o = mk(q4.y, q5.x, q5.y) + (double)R.xz.x * R.fr.u + (double)R.xz.y * R.fr.v;
   R.w = 1.f;
   if (TABLES) {
     // (start + j) mod T, kept in [0, T) for any caller-provided start
