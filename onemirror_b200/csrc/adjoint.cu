@@ -495,7 +495,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.t.rays = (uint32_t)p->rays;
   A.t.rpp = p->rays_per_point;
   A.t.rpp_shift = (A.t.rpp & (A.t.rpp - 1)) ? -1 : __builtin_ctz((unsigned)A.t.rpp);
-  A.t.key = make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32));
+  philox_round_keys(make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32)), A.t.rk);
   A.t.item = p->item;
   A.t.point_xz = s->d_point_xz;
   A.t.point_helio = s->d_point_helio;
@@ -560,7 +560,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   A.t.rays = t->args.t.rays;
   A.t.rpp = t->args.t.rpp;
   A.t.rpp_shift = t->args.t.rpp_shift;
-  A.t.key = t->args.t.key;
+  std::memcpy(A.t.rk, t->args.t.rk, sizeof(A.t.rk));
   A.t.item = t->args.t.item;
   A.t.point_xz = s->d_point_xz;
   A.t.point_helio = s->d_point_helio;

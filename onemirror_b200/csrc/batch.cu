@@ -383,7 +383,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     a.atten = params->attenuation;
     a.rpp = params->rays_per_point;
     a.rpp_shift = (a.rpp & (a.rpp - 1)) ? -1 : __builtin_ctz((unsigned)a.rpp);
-    a.key = make_uint2((uint32_t)params->seed, (uint32_t)(params->seed >> 32));
+    philox_round_keys(make_uint2((uint32_t)params->seed, (uint32_t)(params->seed >> 32)), a.rk);
     a.item = (uint32_t)i;
     a.point_xz = b->pts[items[i].scene];
     a.point_helio = b->pts_helio[items[i].scene];

@@ -83,6 +83,7 @@ QMCRT_HD d3 apply(const frame64& f, double x, double y, double z) {
 // --------------------------------------------------------------- Philox
 // Philox4x32 with 10 rounds; multipliers and Weyl increments from the
 // published algorithm (Random123 paper, SC'11).
+constexpr uint32_t kPhiloxW0 = 0x9E3779B9u, kPhiloxW1 = 0xBB67AE85u;
 QMCRT_HD uint4 philox4x32_10(uint4 c, uint2 k) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
@@ -95,8 +96,26 @@ QMCRT_HD uint4 philox4x32_10(uint4 c, uint2 k) {
     uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
 #endif
     c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-    k.x += 0x9E3779B9u;
-    k.y += 0xBB67AE85u;
+    k.x += kPhiloxW0;
+    k.y += kPhiloxW1;
+  }
+  return c;
+}
+
+// The key schedule of philox4x32_10 for `key`: rk[r] = key + r (W0, W1).
+QMCRT_HD void philox_round_keys(uint2 key, uint2* rk) {
+  for (int r = 0; r < 10; ++r) rk[r] = make_uint2(key.x + r * kPhiloxW0, key.y + r * kPhiloxW1);
+}
+
+// philox4x32_10 from precomputed round keys: a kernel that receives them as
+// launch parameters reads each one from the constant bank as an operand
+// instead of stepping the key in registers.
+__device__ __forceinline__ uint4 philox4x32_10_rk(uint4 c, const uint2* rk) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ rk[r].x, lo1, hi0 ^ c.w ^ rk[r].y, lo0);
   }
   return c;
 }

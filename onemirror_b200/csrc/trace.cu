@@ -340,7 +340,7 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   if ((e = apply_range(p, (uint64_t)s->points * (uint64_t)p->rays_per_point, &a))) return e;
   a.rpp = p->rays_per_point;
   a.rpp_shift = pow2_shift(a.rpp);
-  a.key = make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32));
+  philox_round_keys(make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32)), a.rk);
   a.item = p->item;
   a.point_xz = s->d_point_xz;
   a.point_helio = s->d_point_helio;

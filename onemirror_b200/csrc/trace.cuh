@@ -55,7 +55,7 @@ struct TraceArgs {
   uint32_t ray0;  // the first ray traced (a range of the full set; 0 for whole traces)
   int rpp;
   int rpp_shift;  // log2(rpp) when rpp is a power of two, else -1
-  uint2 key;
+  uint2 rk[10];  // Philox round keys of the seed (philox_round_keys)
   uint32_t item;
   uint32_t quirks;
   const float2* point_xz;
@@ -421,7 +421,7 @@ struct RaySetup {
 // Gaussian (Box-Muller), phi uniform (set_samplelights, set_perturbation).
 __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                                float sigma, float3* sl, float3* tl) {
-  uint4 r = philox4x32_10(make_uint4(ray, 0u, a.item, kTagTrace), a.key);
+  uint4 r = philox4x32_10_rk(make_uint4(ray, 0u, a.item, kTagTrace), a.rk);
   float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
   float st, ct, sp, cp;
   // The azimuths and the Box-Muller log use the hardware approximations
