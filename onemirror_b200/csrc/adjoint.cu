@@ -282,19 +282,49 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
   const float3 E1 = f3((float)a.rE1[0], (float)a.rE1[1], (float)a.rE1[2]);
   const float3 E2 = f3((float)a.rE2[0], (float)a.rE2[1], (float)a.rE2[2]);
   const float3 sd = f3((float)a.sdir[0], (float)a.sdir[1], (float)a.sdir[2]);
-  const uint64_t end = ((uint64_t)a.rays + 31) / 32 * 32;  // whole warps keep the shuffles converged
-  // chunks of consecutive rays (a multiple of 32) taken grid-stride
-  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = (end + chunk - 1) / chunk;
-  for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x)
-  for (uint64_t r64 = ch * chunk + threadIdx.x, r1 = min((ch + 1) * chunk, end); r64 < r1; r64 += blockDim.x) {
+  // Each warp takes segments of 256 consecutive rays (grid-stride over all
+  // warps) and works only on the rays that contribute: those the tape marks
+  // as hits, and every ray past the saved part of the tape (their visibility
+  // is recomputed).  Lane i reads the tape bytes of rays 8i..8i+7 of the
+  // segment; the selected rays are then handed out 32 per pass, lane j taking
+  // the j-th one (a binary search over the lanes' prefix counts finds the lane
+  // that owns it).  Lost rays cost nothing, and a segment's rays mostly share
+  // a heliostat, so the warp reduction below stays uniform.
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const uint64_t nseg = ((uint64_t)a.rays + 255) / 256;
+  for (uint64_t sg = (uint64_t)blockIdx.x * nwarps + (threadIdx.x >> 5); sg < nseg;
+       sg += (uint64_t)gridDim.x * nwarps) {
+    const uint64_t b0 = sg * 256 + 8 * lane;  // this lane's first ray (a multiple of 8)
+    uint32_t m = 0;  // bit k: ray b0 + k is worked on
+    if (b0 + 8 <= A.saved && b0 + 8 <= a.rays) {
+      const uint2 t8 = *reinterpret_cast<const uint2*>(A.tape + b0);  // 8-byte aligned
+#pragma unroll
+      for (int k = 0; k < 8; ++k) m |= (((k < 4 ? t8.x >> (8 * k) : t8.y >> (8 * (k - 4))) & 0xFFu) != 0u) << k;
+    } else {
+      for (int k = 0; k < 8; ++k) {
+        const uint64_t r = b0 + k;
+        if (r < a.rays && (r >= A.saved || A.tape[r] != 0)) m |= 1u << k;
+      }
+    }
+    const int cnt = __popc(m);
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int excl = incl - cnt, total = __shfl_sync(0xffffffffu, incl, 31);
+  for (int base = 0; base < total; base += 32) {
+    const int q = base + lane;
+    int own = 0;  // the last lane whose prefix count is <= q
+    for (int step = 16; step > 0; step >>= 1)
+      if (__shfl_sync(0xffffffffu, excl, own + step) <= q) own += step;
+    uint32_t mo = __shfl_sync(0xffffffffu, m, own);
+    const int skip = q - __shfl_sync(0xffffffffu, excl, own);
     float gk[4] = {0.f, 0.f, 0.f, 0.f};
     int h = -1;
-    if (r64 < a.rays && r64 < A.saved && A.tape[r64] == 0) {
-      // a ray the tape marks as lost contributes nothing; its heliostat still
-      // joins the warp's reduction below
-      const uint32_t ray = (uint32_t)r64;
-      h = __ldg(a.point_helio + (a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp));
-    } else if (r64 < a.rays) {
+    if (q < total) {
+      for (int i = 0; i < skip; ++i) mo &= mo - 1u;  // drop the lower selected rays
+      const uint64_t r64 = sg * 256 + 8 * own + (__ffs(mo) - 1);
       const uint32_t ray = (uint32_t)r64;
       RaySetup R;
       ray_setup<false>(a, s_tab, s_guide, ray, R);
@@ -376,6 +406,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
       atomicAdd(A.grad_tilt + 2 * h, gk[2]);
       atomicAdd(A.grad_tilt + 2 * h + 1, gk[3]);
     }
+  }
   }
 }
 
