@@ -227,6 +227,15 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
     int i0 = (int)floorf(px), j0 = (int)floorf(py);
     float fx = px - (float)i0, fy = py - (float)j0;
     const float wgt[4] = {(1.f - fx) * (1.f - fy), fx * (1.f - fy), (1.f - fx) * fy, fx * fy};
+    if ((unsigned)(j0 - r0) < (unsigned)(T - 1) && (unsigned)(i0 - c0) < (unsigned)(T - 1)) {
+      // all four corners in the tile (which lies inside the map): one check
+      float* q = s_tile + (j0 - r0) * T + (i0 - c0);
+      atomicAdd(q, e * wgt[0]);
+      atomicAdd(q + 1, e * wgt[1]);
+      atomicAdd(q + T, e * wgt[2]);
+      atomicAdd(q + T + 1, e * wgt[3]);
+      continue;
+    }
     for (int k = 0; k < 4; ++k) {
       int ci = i0 + (k & 1), cj = j0 + (k >> 1);
       if (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) continue;
