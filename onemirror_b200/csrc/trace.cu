@@ -209,6 +209,7 @@ void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, u
     a->rE2[i] = s->rg.v3[i] - s->rg.v0[i];
   }
   for (int i = 0; i < 5; ++i) a->cyl[i] = s->rg.cyl[i];
+  a->cyl[5] = s->rg.cyl[4] > 0 ? 1.0 / s->rg.cyl[4] : 0.0;
   a->cyl_edge = s->d_cyl_edge;
   a->res_x = s->rg.res_x;
   a->res_y = s->rg.res_y;

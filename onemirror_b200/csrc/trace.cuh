@@ -46,7 +46,7 @@ struct TraceArgs {
   // receiver
   int rtype;
   double rA[3], rE1[3], rE2[3];
-  double cyl[5];
+  double cyl[6];  // cylinder: bottom centre x, y, z, radius, height, 1 / height
   const double2* cyl_edge;  // cylinder: [res_x] (cos, sin) of each column's first edge, 2 pi k / res_x
   int res_x, res_y;
   // rays
@@ -307,7 +307,8 @@ __device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int whic
 // Receiver intersection in FP64; returns true on a hit and the pixel index
 // (-1 when the hit falls outside the map, QMCRT_QUIRK_PIXEL_EDGE only).
 __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int& pix, double* t_out = nullptr) {
-  double u, v;
+  double u, v = 0.0;
+  int col = -1;  // set directly by the cylinder
   if (a.rtype == QMCRT_RECEIVER_CYLINDER) {
     double ox = o.x - a.cyl[0], oz = o.z - a.cyl[2], R = a.cyl[3], H = a.cyl[4];
     double qa = d.x * d.x + d.z * d.z;
@@ -326,7 +327,7 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
       if (t < 1e-6 || y < 0 || y > H) return false;
     }
     if (t_out) *t_out = t;
-    u = y / H;
+    u = y * a.cyl[5];
     // column = floor(phi / 2 pi * res_x), phi = atan2(Z, X) in [0, 2 pi):
     // the single-precision angle picks a column within one of the right one;
     // the signs of the hit's FP64 cross products with that column's edges
@@ -344,7 +345,7 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
       const double2 e1 = __ldg(a.cyl_edge + c1);
       if (e1.x * Z - e1.y * X >= 0.0) c = c1;
     }
-    v = (c + 0.5) / a.res_x;  // the column's centre: (int)(v * res_x) == c
+    col = c;
   } else {
     d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
     d3 pv = cross(d, E2);
@@ -361,7 +362,8 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
     if (t < 1e-6) return false;
     if (t_out) *t_out = t;
   }
-  int row = (int)(u * a.res_y), col = (int)(v * a.res_x);  // rectgrid_raytracing.cu:144
+  int row = (int)(u * a.res_y);  // rectgrid_raytracing.cu:144
+  if (col < 0) col = (int)(v * a.res_x);
   if (a.quirks & QMCRT_QUIRK_PIXEL_EDGE) {
     if (row >= a.res_y || col >= a.res_x) {
       pix = -1;
