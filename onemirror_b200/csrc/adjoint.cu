@@ -362,13 +362,14 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         const float gWy = (1.f - fx) * (Gc[2] - Gc[0]) + fx * (Gc[3] - Gc[1]);
         // forward quantities in float
         const float3 npf = to_f(g.np), rdf = to_f(g.rd), wsf = to_f(R.ws);
-        const float ilnp = (float)(1.0 / g.lnp), ilr = (float)(1.0 / g.lr);
+        // the tangents are FP32: reciprocals to ~1e-12 (and 2 ulp below) suffice
+        const float ilnp = (float)rcp_nr(g.lnp), ilr = (float)rcp_nr(g.lr);
         const float nws = dot(npf, wsf);
         const float sdn = dot(sd, npf);
         const float e = fabsf(sdn) * R.w, sg = sdn < 0.f ? -1.f : 1.f;
         // t along the reflected ray to the receiver plane (for d(hit) = do + t dr)
         const float3 cr = cross(E2, rdf);
-        const float iden = 1.f / dot(E1, cr);
+        const float iden = __fdividef(1.f, dot(E1, cr));
         const float t = (float)tr;
         // the frame Jacobian, row-major [9][4]: row r holds d(frame component r)
         // for the 4 parameters, one float4 (144-byte records, 16-byte aligned)
