@@ -63,6 +63,30 @@ def test_buie_sample_density_matches_the_tabulated_profile():
     assert np.max(np.abs(hist - expect) / np.sqrt(expect)) < 5
 
 
+@pytest.mark.parametrize("csr", [0.05, 0.1, 0.2])
+def test_buie_cdf_equals_the_integrated_profile(csr):
+    """The table's cumulative values are the integral of the core profile
+    cos(0.326 t)/cos(0.308 t) (t in mrad, no sin t Jacobian) from 0 to each
+    node (1024 trapezoids to 4.65 mrad: exact to the trapezoid error), the
+    aureole mass is the integral of e^k t^gamma from 4.65 to 9.3 mrad, and
+    the analytic aureole inverse lands where the integrated CDF reaches u."""
+    from scipy.integrate import quad
+    x, y, s, p = O.buie_table(csr)
+    k, gamma, core, total = (float(v) for v in p[:4])
+    prof = lambda t: np.cos(0.326 * t) / np.cos(0.308 * t)
+    for i in (1, 100, 512, 900, 1024):
+        exact = quad(prof, 0.0, float(x[i]), epsabs=1e-13)[0]
+        assert abs(float(y[i]) - exact) <= 1e-4 * exact, (i, y[i], exact)
+    aur = lambda t: np.exp(k) * t ** gamma
+    assert abs((total - core) - quad(aur, 4.65, 9.3, epsabs=1e-13)[0]) <= 1e-4 * (total - core)
+    L = O.lib()
+    for frac in (0.2, 0.5, 0.9):
+        u = (core + frac * (total - core)) / total
+        th = L.orc_buie_sample(u, O._p(x, O.fp), O._p(y, O.fp), O._p(s, O.fp), O._p(p, O.fp))
+        reached = core + quad(aur, 4.65, th, epsabs=1e-13)[0]
+        assert abs(reached - u * total) <= 1e-4 * total, (frac, th)
+
+
 def test_local2world_frame():
     L = O.lib()
     rng = np.random.default_rng(3)
