@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
        r64 += blockDim.x) {
     const uint32_t ray = (uint32_t)r64;
     RaySetup R;
-    ray_setup<false>(a, s_tab, s_guide, ray, R);
+    ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
     Refl g;
     double u, v, t;
     const bool hit = ray_hits<CULL, false>(a, R, fy0, fy1, &g, &u, &v, &t);
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
       const uint64_t r64 = sg * 256 + 8 * own + (__ffs(mo) - 1);
       const uint32_t ray = (uint32_t)r64;
       RaySetup R;
-      ray_setup<false>(a, s_tab, s_guide, ray, R);
+      ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
       h = R.h;
       bool hit;
       Refl g;

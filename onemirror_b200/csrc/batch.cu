@@ -68,11 +68,18 @@ __device__ bool chunk_anchor(const TraceArgs& a, uint32_t ray, int T, int* r0, i
   return true;
 }
 
+// The Philox round keys of a batch's seed (every item shares it), passed as
+// a launch parameter so that the rounds read them from the constant bank
+// rather than from the shared-memory copy of the item's arguments.
+struct PhiloxKeys {
+  uint2 rk[10];
+};
+
 template <int T>
 __global__ void __launch_bounds__(kBatchThreads, 4)
     batch_trace_kernel(const TraceArgs* __restrict__ items, const unsigned long long* __restrict__ chunk_begin,
                        int n_items, uint32_t chunk_rays, unsigned long long total_chunks,
-                       unsigned long long* counter) {
+                       unsigned long long* counter, const __grid_constant__ PhiloxKeys keys) {
   __shared__ TraceArgs s_a;
   __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
@@ -136,7 +143,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
       const TileDeposit<T> dep{s_cnt, s_en, s_anchor[2] ? s_anchor[0] : -(1 << 30), s_anchor[1], s_a.res_x,
                                s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep);
+        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
       __syncthreads();
       if (s_anchor[2]) {  // flush the tile's non-zero pixels, then clear it
         for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
     } else {
       const GlobalDeposit dep{s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep);
+        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
     }
     __syncthreads();  // everyone is done with s_c / s_a / the tile before the next chunk
   }
@@ -219,6 +226,7 @@ struct qmcrt_batch {
   std::vector<unsigned long long> chunk_begin;  // host copy [items+1]
   qmcrt_batch_tuning tuning{65536, 4, 0, 0.f};
   int sms = 148;
+  qm::PhiloxKeys keys{};  // round keys of params.seed
   cudaStream_t cap_stream = nullptr;
   // the items' geometry is rebuilt on kGeomStreams side streams forked from
   // the pass's stream and joined before the trace (parallel graph branches)
@@ -251,15 +259,15 @@ static qmcrt_status enqueue_trace(qmcrt_batch* b, int n, cudaStream_t st) {
   switch (b->tuning.tile) {
     case 32:
       batch_trace_kernel<32><<<ctas, kBatchThreads, 0, st>>>(b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays,
-                                                              total, b->d_counter);
+                                                              total, b->d_counter, b->keys);
       break;
     case 48:
       batch_trace_kernel<48><<<ctas, kBatchThreads, 0, st>>>(b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays,
-                                                              total, b->d_counter);
+                                                              total, b->d_counter, b->keys);
       break;
     default:
       batch_trace_kernel<0><<<ctas, kBatchThreads, 0, st>>>(b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays,
-                                                             total, b->d_counter);
+                                                             total, b->d_counter, b->keys);
   }
   QM_CUDA(cudaGetLastError());
   return QMCRT_OK;
@@ -384,6 +392,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     a.rpp = params->rays_per_point;
     a.rpp_shift = (a.rpp & (a.rpp - 1)) ? -1 : __builtin_ctz((unsigned)a.rpp);
     philox_round_keys(make_uint2((uint32_t)params->seed, (uint32_t)(params->seed >> 32)), a.rk);
+    std::memcpy(b->keys.rk, a.rk, sizeof(b->keys.rk));
     a.item = (uint32_t)i;
     a.point_xz = b->pts[items[i].scene];
     a.point_helio = b->pts_helio[items[i].scene];

@@ -421,9 +421,11 @@ struct RaySetup {
 // Sun sample and slope-error perturbation of ray `ray` from Philox (seed,
 // ray id): theta from the Buie inverse CDF, phi uniform; slope theta
 // Gaussian (Box-Muller), phi uniform (set_samplelights, set_perturbation).
+// rk: the seed's Philox round keys (a.rk, or a copy the caller holds in
+// faster memory).
 __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
-                                               float sigma, float3* sl, float3* tl) {
-  uint4 r = philox4x32_10_rk(make_uint4(ray, 0u, a.item, kTagTrace), a.rk);
+                                               float sigma, float3* sl, float3* tl, const uint2* rk) {
+  uint4 r = philox4x32_10_rk(make_uint4(ray, 0u, a.item, kTagTrace), rk);
   float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
   float st, ct, sp, cp;
   // The azimuths and the Box-Muller log use the hardware approximations
@@ -444,7 +446,7 @@ __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4*
 // Returns false for a ray to skip (table mode with an out-of-range heliostat id).
 template <bool TABLES>
 __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
-                                          RaySetup& R) {
+                                          RaySetup& R, const uint2* rk) {
   const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
   const uint32_t j = ray - g * (uint32_t)a.rpp;
   const int h = __ldg(a.point_helio + g);
@@ -470,7 +472,7 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
     R.sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
     R.tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
   } else {
-    philox_samples(a, s_tab, s_guide, ray, __ldg(a.sigma + h), &R.sl, &R.tl);
+    philox_samples(a, s_tab, s_guide, ray, __ldg(a.sigma + h), &R.sl, &R.tl, rk);
     R.w = a.weight ? __ldg(a.weight + h) : 1.f;
   }
   // world sample (local2world(sample, sun_dir)), incident direction
@@ -486,9 +488,10 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
 // sampling only: their cones bound the sampler's directions).
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep>
 __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
-                                          float fy0, float fy1, RayCounters& c, const Dep& deposit) {
+                                          float fy0, float fy1, RayCounters& c, const Dep& deposit,
+                                          const uint2* rk) {
   RaySetup R;
-  if (!ray_setup<TABLES>(a, s_tab, s_guide, ray, R)) {
+  if (!ray_setup<TABLES>(a, s_tab, s_guide, ray, R, rk)) {
     if (RECORDS) {
       if (a.flags) a.flags[ray] = 0;
       if (a.pixel) a.pixel[ray] = -1;
@@ -568,7 +571,7 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
     const uint64_t r0 = a.ray0 + ch * chunk, r1 = min(r0 + chunk, (uint64_t)a.rays);
     for (uint64_t r64 = r0 + threadIdx.x; r64 < r1; r64 += blockDim.x)
-      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep);
+      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep, a.rk);
   }
   if (STATS) flush_counters(c, a.stats);
 }
