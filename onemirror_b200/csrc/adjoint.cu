@@ -186,11 +186,11 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
   uint32_t nt = 0, nc = 0;
   const float3 of = to_f(R.o);
   const float3 sd = f3((float)-R.ws.x, (float)-R.ws.y, (float)-R.ws.z);
-  if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc)
+  if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc, R.reach.x)
            : dda_blocked<false, false>(a, of, sd, R.h, fy0, fy1, nt, nc))
     return false;
   *g = reflect_ray<LENGTHS>(R);
-  if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(g->rd), fy0, fy1, nt, nc)
+  if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(g->rd), fy0, fy1, nt, nc, R.reach.y)
            : dda_blocked<false, false>(a, of, to_f(g->rd), R.h, fy0, fy1, nt, nc))
     return false;
   return receiver_uv(a, R.o, g->rd, u, v, t);
@@ -459,6 +459,7 @@ static qmcrt_status tape_geometry(qmcrt_tape* t, cudaStream_t st) {
   qmcrt_status e;
   if ((e = ensure_sun(s, &t->sun, t->params.quirks, st))) return e;
   if ((e = ensure_points(s, &t->params, st))) return e;
+  if ((e = ensure_masks(s, st))) return e;
   return QMCRT_OK;
 }
 }  // namespace qm
@@ -540,6 +541,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.t.item = p->item;
   A.t.point_xz = s->d_point_xz;
   A.t.point_helio = s->d_point_helio;
+  A.t.point_mask = s->d_point_mask;
   A.t.energy = t->d_energy;
   double l1 = 0, l2 = 0;
   for (int i = 0; i < 3; ++i) {
@@ -605,6 +607,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   A.t.item = t->args.t.item;
   A.t.point_xz = s->d_point_xz;
   A.t.point_helio = s->d_point_helio;
+  A.t.point_mask = s->d_point_mask;
   A.t.energy = t->d_energy;
   A.grad_aim = d_grad_aim;
   A.grad_tilt = d_grad_tilt;

@@ -152,6 +152,11 @@ struct qmcrt_scene {
   // points
   qm::PointsKey points_key;
   int64_t points = 0, points_cap = 0;
+  // per-point candidate masks, rebuilt when the sun geometry or the points change
+  uint64_t geom_version = 0, points_version = 0, mask_geom = ~0ull, mask_points = ~0ull;
+  double sun_unit[3] = {0, 0, 0};   // the normalised sun direction of the current geometry
+  int64_t mask_cap = 0;
+  uint2* d_point_mask = nullptr;     // [points] (shadow, block) candidate bits
   float2* d_point_xz = nullptr;
   int32_t* d_point_helio = nullptr;
   float* d_helio_weight = nullptr;  // [n] mirror area per point
@@ -182,4 +187,10 @@ void free_sun_geom(SunGeom* g);
 qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
                              cudaStream_t st);
 qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
+// Per-point candidate masks of `points` points (xz, helio) for geometry g of
+// scene s and the (normalised) sun, into mask.
+qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
+                                const int32_t* helio, int64_t points, uint2* mask, cudaStream_t st);
+// The scene's masks for its current sun and points (rebuilt when stale).
+qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st);
 }  // namespace qm

@@ -493,6 +493,101 @@ __global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
   if ((threadIdx.x & 31) == 0) a.cand_n[2 * h + walk] = cnt;
 }
 
+// ---------------------------------------------------- per-point candidate masks
+// A heliostat's candidate list holds every heliostat that some ray of ANY of
+// its sample points can reach.  From one point the rays leave within the same
+// cone (the apex now the point itself), so most of the list is out of reach:
+// bit j of a point's mask is set when candidate j of its heliostat's list can
+// be reached from that point, and its rays test only those candidates.
+struct MaskArgs {
+  int64_t points;
+  const float2* point_xz;
+  const int32_t* point_helio;
+  const double* frame;  // [kFrameStride n] u, n, v, mirror centre
+  const float4* cand;
+  const int* cand_n;
+  const float* sigma;
+  double sun[3];
+  double shadow_tan, sun_alpha, zmax;
+  uint2* mask;  // [points] (shadow bits, block bits)
+};
+
+// Can a ray from point p, leaving within atan(tan_a) of the unit axis d, meet
+// the parallelogram of rectangle record r?  The hit q satisfies (q - p).d >= 0
+// and lies at most (q - p).d tan_a across the axis from p, so the
+// parallelogram's projection across d must come within (largest axial
+// distance) tan_a of p's; a projected edge normal that separates them by more
+// rules the pair out.  2 cm of slack covers the FP32 rounding of the ray's
+// origin, direction and rectangle test.
+__device__ bool point_reaches(d3 p, const float4* r, d3 d, double tan_a) {
+  const double mu = 0.02;
+  d3 e1 = fabs(d.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
+  e1 = e1 - dot(e1, d) * d;
+  e1 = (1.0 / sqrt(dot(e1, e1))) * e1;
+  const d3 e2 = cross(d, e1);
+  const d3 A = mk(r[0].x, r[0].y, r[0].z) - p, E1 = mk(r[1].x, r[1].y, r[1].z), E2 = mk(r[2].x, r[2].y, r[2].z);
+  const d3 c[4] = {A, A + E1, A + E2, A + E1 + E2};
+  double amax = -1e300, px[4], py[4];
+  for (int i = 0; i < 4; ++i) {
+    amax = fmax(amax, dot(c[i], d));
+    px[i] = dot(c[i], e1);
+    py[i] = dot(c[i], e2);
+  }
+  if (amax < -mu) return false;  // wholly behind the point
+  const double rho = (fmax(amax, 0.0) + mu) * tan_a + mu;
+  const double ex[2] = {dot(E1, e1), dot(E2, e1)}, ey[2] = {dot(E1, e2), dot(E2, e2)};
+  for (int j = 0; j < 2; ++j) {
+    const double l = sqrt(ex[j] * ex[j] + ey[j] * ey[j]);
+    if (!(l > 1e-9)) continue;
+    const double nx = -ey[j] / l, ny = ex[j] / l;
+    double lo = 1e300, hi = -1e300;
+    for (int i = 0; i < 4; ++i) {
+      const double v = px[i] * nx + py[i] * ny;
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
+    if (lo > rho || hi < -rho) return false;  // the point projects to 0
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= a.points) return;
+  const int h = a.point_helio[g];
+  const float2 xz = a.point_xz[g];
+  const double* F = a.frame + kFrameStride * h;
+  const d3 u = mk(F[0], F[1], F[2]), n = mk(F[3], F[4], F[5]), v = mk(F[6], F[7], F[8]);
+  const d3 p = mk(F[9], F[10], F[11]) + (double)xz.x * u + (double)xz.y * v;
+  const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
+  uint32_t bits[2] = {0u, 0u};
+  for (int w = 0; w < 2; ++w) {
+    const int m = a.cand_n[2 * h + w];
+    if (m > kCandCap) {  // the rays walk the grid
+      bits[w] = 0xffffffffu;
+      continue;
+    }
+    d3 d;
+    double tan_a;
+    if (w == 0) {
+      d = mk(-s.x, -s.y, -s.z);
+      tan_a = a.shadow_tan;
+    } else {
+      d = s - (2.0 * dot(s, n)) * n;
+      const double ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
+      if (!(ab < 1.2)) {  // no cone bounds the block rays: every candidate
+        bits[w] = m == 32 ? 0xffffffffu : (1u << m) - 1u;
+        continue;
+      }
+      tan_a = tan(ab);
+    }
+    const float4* L = a.cand + (int64_t)(2 * h + w) * kCandCap * 3;
+    for (int j = 0; j < m; ++j)
+      if (point_reaches(p, L + 3 * j, d, tan_a)) bits[w] |= 1u << j;
+  }
+  a.mask[g] = make_uint2(bits[0], bits[1]);
+}
+
 // ------------------------------------------------------------ points
 struct PoissonArgs {
   int n;
@@ -741,6 +836,46 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
   QM_CUDA(cudaEventRecord(s->ev[1], st));
   s->setup_timed = true;
   s->sun_key = k;
+  std::memcpy(s->sun_unit, sd, sizeof(sd));
+  s->geom_version++;
+  return QMCRT_OK;
+}
+
+qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
+                                const int32_t* helio, int64_t points, uint2* mask, cudaStream_t st) {
+  if (points <= 0) return QMCRT_OK;
+  MaskArgs m{};
+  m.points = points;
+  m.point_xz = xz;
+  m.point_helio = helio;
+  m.frame = g.frame;
+  m.cand = g.cand;
+  m.cand_n = g.cand_n;
+  m.sigma = s->d_sigma;
+  for (int i = 0; i < 3; ++i) m.sun[i] = sun[i];
+  m.shadow_tan = std::tan(kSunAlphaMax + 1e-6);
+  m.sun_alpha = kSunAlphaMax;
+  m.zmax = kSlopeZMax;
+  m.mask = mask;
+  point_mask_kernel<<<(unsigned)((points + 255) / 256), 256, 0, st>>>(m);
+  QM_CUDA(cudaGetLastError());
+  return QMCRT_OK;
+}
+
+qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st) {
+  if (s->mask_geom == s->geom_version && s->mask_points == s->points_version) return QMCRT_OK;
+  if (s->mask_cap < s->points) {
+    dev_free(s->d_point_mask);
+    s->mask_cap = 0;
+    qmcrt_status e = dev_alloc(&s->d_point_mask, (size_t)s->points);
+    if (e) return e;
+    s->mask_cap = s->points;
+  }
+  qmcrt_status e = launch_point_masks(s, scene_geom(s), s->sun_unit, s->d_point_xz, s->d_point_helio, s->points,
+                                      s->d_point_mask, st);
+  if (e) return e;
+  s->mask_geom = s->geom_version;
+  s->mask_points = s->points_version;
   return QMCRT_OK;
 }
 
@@ -975,6 +1110,7 @@ qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStre
   QM_CUDA(cudaGetLastError());
   s->points = total;
   s->points_key = k;
+  s->points_version++;
   return QMCRT_OK;
 }
 
@@ -1142,7 +1278,8 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_sigma); dev_free(s->d_tilt); dev_free(s->d_normal); dev_free(s->d_frame);
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
   dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_cand); dev_free(s->d_cand_n); dev_free(s->d_field_yr);
-  dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_cyl_edge); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_cyl_edge);
+  dev_free(s->d_point_mask); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

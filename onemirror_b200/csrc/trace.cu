@@ -345,6 +345,8 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   a.item = p->item;
   a.point_xz = s->d_point_xz;
   a.point_helio = s->d_point_helio;
+  if ((e = ensure_masks(s, st))) return e;
+  a.point_mask = s->d_point_mask;
   return run_and_finish(s, sun, p, a, false, 1.0, out, stats, st);
 }
 

@@ -33,6 +33,7 @@ struct TraceArgs {
   // (> kCandCap: the list overflowed); NULL: walk the grid
   const float4* cand;   // [n][2][kCandCap][3]
   const int* cand_n;    // [n][2]
+  const uint2* point_mask;  // [points] candidates reachable from each point (shadow, block bits); NULL: all
   const float4* rect;   // [3n] every heliostat's own rectangle record
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
@@ -291,13 +292,18 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
 // meet is in the list, so the answer is the grid walk's; all lanes of a warp
 // share h, so they run the same candidates with broadcast loads.  A list that
 // overflowed, or no lists (cand_n NULL), falls back to the grid walk.
+// reach: the candidates the ray's point can reach (bit j: list entry j), from
+// the per-point masks; every bit set when there are none.
 template <bool STATS>
 __device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int which, float3 o, float3 d, float fy0,
-                                             float fy1, uint32_t& ntest, uint32_t& ncell) {
+                                             float fy1, uint32_t& ntest, uint32_t& ncell, uint32_t reach) {
   const int m = a.cand_n ? __ldg(a.cand_n + 2 * h + which) : kCandCap + 1;  // no lists: walk
   if (m > kCandCap) return dda_blocked<STATS, true>(a, o, d, h, fy0, fy1, ntest, ncell);
   const float4* L = a.cand + (size_t)(2 * h + which) * (kCandCap * 3);
-  for (int i = 0; i < m; ++i) {
+  uint32_t bits = reach & (m == 32 ? 0xffffffffu : (1u << m) - 1u);
+  while (bits) {  // the same bits on every lane of a warp (one point)
+    const int i = __ffs(bits) - 1;
+    bits &= bits - 1u;
     if (STATS) ++ntest;
     if (rect_hit(__ldg(L + 3 * i), __ldg(L + 3 * i + 1), __ldg(L + 3 * i + 2), o, d)) return true;
   }
@@ -411,6 +417,7 @@ __device__ __forceinline__ void load_buie(const float* buie, float4* s_tab, int*
 struct RaySetup {
   int h;
   float2 xz;
+  uint2 reach;  // candidate masks of the ray's point (shadow, block)
   frame64 fr;
   d3 o;
   float3 sl, tl;
@@ -453,6 +460,7 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
   if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
   R.h = h;
   R.xz = __ldg(a.point_xz + g);
+  R.reach = a.point_mask ? __ldg(a.point_mask + g) : make_uint2(0xffffffffu, 0xffffffffu);
   // the 96-byte frame record (16-byte aligned) as six 16-byte loads
   const double2* F = reinterpret_cast<const double2*>(a.frame + kFrameStride * h);
   const double2 q0 = __ldg(F), q1 = __ldg(F + 1), q2 = __ldg(F + 2), q3 = __ldg(F + 3), q4 = __ldg(F + 4),
@@ -515,10 +523,10 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_ta
   int pix = -1;
   double th = 0.0;
   const float3 sdir = f3((float)-ws.x, (float)-ws.y, (float)-ws.z);
-  if (CULL == 3 ? list_blocked<STATS>(a, h, 0, of, sdir, fy0, fy1, c.test, c.cell)
+  if (CULL == 3 ? list_blocked<STATS>(a, h, 0, of, sdir, fy0, fy1, c.test, c.cell, R.reach.x)
                 : dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, sdir, h, fy0, fy1, c.test, c.cell)) {
     flag = QMCRT_RAY_SHADOWED;
-  } else if (CULL == 3 ? list_blocked<STATS>(a, h, 1, of, to_f(rd), fy0, fy1, c.test, c.cell)
+  } else if (CULL == 3 ? list_blocked<STATS>(a, h, 1, of, to_f(rd), fy0, fy1, c.test, c.cell, R.reach.y)
                        : dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
     flag = QMCRT_RAY_BLOCKED;
   } else if (receiver_hit(a, o, rd, pix, &th)) {
