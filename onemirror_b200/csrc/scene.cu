@@ -517,35 +517,31 @@ struct MaskArgs {
 // and lies at most (q - p).d tan_a across the axis from p, so the
 // parallelogram's projection across d must come within (largest axial
 // distance) tan_a of p's; a projected edge normal that separates them by more
-// rules the pair out.  2 cm of slack covers the FP32 rounding of the ray's
-// origin, direction and rectangle test.
-__device__ bool point_reaches(d3 p, const float4* r, d3 d, double tan_a) {
-  const double mu = 0.02;
-  d3 e1 = fabs(d.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
-  e1 = e1 - dot(e1, d) * d;
-  e1 = (1.0 / sqrt(dot(e1, e1))) * e1;
-  const d3 e2 = cross(d, e1);
-  const d3 A = mk(r[0].x, r[0].y, r[0].z) - p, E1 = mk(r[1].x, r[1].y, r[1].z), E2 = mk(r[2].x, r[2].y, r[2].z);
-  const d3 c[4] = {A, A + E1, A + E2, A + E1 + E2};
-  double amax = -1e300, px[4], py[4];
-  for (int i = 0; i < 4; ++i) {
-    amax = fmax(amax, dot(c[i], d));
-    px[i] = dot(c[i], e1);
-    py[i] = dot(c[i], e2);
-  }
+// rules the pair out.  The corner is taken relative to p in FP64 and the rest
+// runs in FP32 (lengths of at most a few hundred metres: ~1e-5 m of rounding);
+// 2 cm of slack covers that and the FP32 rounding of the ray's origin,
+// direction and rectangle test.  e1, e2: unit vectors across d.
+__device__ bool point_reaches(d3 p, const float4* r, float3 d, float3 e1, float3 e2, float tan_a) {
+  const float mu = 0.02f;
+  const float4 r0 = r[0], r1 = r[1], r2 = r[2];
+  const float3 A = f3((float)((double)r0.x - p.x), (float)((double)r0.y - p.y), (float)((double)r0.z - p.z));
+  const float3 E1 = f3(r1.x, r1.y, r1.z), E2 = f3(r2.x, r2.y, r2.z);
+  // axial and cross-axis coordinates of A, E1, E2 (the corners are A, A + E1, A + E2, A + E1 + E2)
+  const float aA = dot(A, d), a1 = dot(E1, d), a2 = dot(E2, d);
+  const float amax = aA + fmaxf(a1, 0.f) + fmaxf(a2, 0.f);
   if (amax < -mu) return false;  // wholly behind the point
-  const double rho = (fmax(amax, 0.0) + mu) * tan_a + mu;
-  const double ex[2] = {dot(E1, e1), dot(E2, e1)}, ey[2] = {dot(E1, e2), dot(E2, e2)};
+  const float rho = (fmaxf(amax, 0.f) + mu) * tan_a + mu;
+  const float xA = dot(A, e1), x1 = dot(E1, e1), x2 = dot(E2, e1);
+  const float yA = dot(A, e2), y1 = dot(E1, e2), y2 = dot(E2, e2);
+#pragma unroll
   for (int j = 0; j < 2; ++j) {
-    const double l = sqrt(ex[j] * ex[j] + ey[j] * ey[j]);
-    if (!(l > 1e-9)) continue;
-    const double nx = -ey[j] / l, ny = ex[j] / l;
-    double lo = 1e300, hi = -1e300;
-    for (int i = 0; i < 4; ++i) {
-      const double v = px[i] * nx + py[i] * ny;
-      lo = fmin(lo, v);
-      hi = fmax(hi, v);
-    }
+    const float ex = j ? x2 : x1, ey = j ? y2 : y1;
+    const float l2 = ex * ex + ey * ey;
+    if (!(l2 > 1e-12f)) continue;
+    const float il = rsqrtf(l2), nx = -ey * il, ny = ex * il;
+    // the corners' coordinates along (nx, ny): A's plus either edge's or both
+    const float c0 = xA * nx + yA * ny, d1 = x1 * nx + y1 * ny, d2 = x2 * nx + y2 * ny;
+    const float lo = c0 + fminf(d1, 0.f) + fminf(d2, 0.f), hi = c0 + fmaxf(d1, 0.f) + fmaxf(d2, 0.f);
     if (lo > rho || hi < -rho) return false;  // the point projects to 0
   }
   return true;
@@ -567,13 +563,13 @@ __global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
       bits[w] = 0xffffffffu;
       continue;
     }
-    d3 d;
+    d3 dd;
     double tan_a;
     if (w == 0) {
-      d = mk(-s.x, -s.y, -s.z);
+      dd = mk(-s.x, -s.y, -s.z);
       tan_a = a.shadow_tan;
     } else {
-      d = s - (2.0 * dot(s, n)) * n;
+      dd = s - (2.0 * dot(s, n)) * n;
       const double ab = a.sun_alpha + 2.0 * a.zmax * (double)a.sigma[h] + 1e-6;
       if (!(ab < 1.2)) {  // no cone bounds the block rays: every candidate
         bits[w] = m == 32 ? 0xffffffffu : (1u << m) - 1u;
@@ -581,9 +577,16 @@ __global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
       }
       tan_a = tan(ab);
     }
+    dd = rsqrt_nr(dot(dd, dd)) * dd;
+    const float3 d = f3((float)dd.x, (float)dd.y, (float)dd.z);
+    float3 e1 = fabsf(d.x) < 0.9f ? f3(1.f, 0.f, 0.f) : f3(0.f, 1.f, 0.f);
+    e1 = e1 - dot(e1, d) * d;
+    e1 = rsqrtf(dot(e1, e1)) * e1;
+    const float3 e2 = cross(d, e1);
+    const float ta = (float)tan_a * 1.0001f;  // rounded up
     const float4* L = a.cand + (int64_t)(2 * h + w) * kCandCap * 3;
     for (int j = 0; j < m; ++j)
-      if (point_reaches(p, L + 3 * j, d, tan_a)) bits[w] |= 1u << j;
+      if (point_reaches(p, L + 3 * j, d, e1, e2, ta)) bits[w] |= 1u << j;
   }
   a.mask[g] = make_uint2(bits[0], bits[1]);
 }
