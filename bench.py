@@ -3,8 +3,8 @@
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload mid|small|large] [--impl b200|reference]
 
 One step = one pass of the hot path over one batch: aim the field for the
-step's sun position, rebuild the grid and the per-heliostat occluder
-candidates on the GPU, trace 2^28 rays (Buie sampling, shadow and block tests,
+step's sun position, rebuild the grid, the per-heliostat occluder
+candidates and the per-point candidate masks on the GPU, trace 2^28 rays (Buie sampling, shadow and block tests,
 receiver deposition), scale the flux map and smooth the count map (trimmed
 mean).  Every step uses a fresh Philox stream
 and a slightly moved sun, so no output or geometry is reused.  Under torchrun
@@ -554,8 +554,8 @@ def b200_arm(a, rank, world, local):
             "hbm_peak_gbs_of_measured": peaks.get("hbm_gbs")}
     if traffic is not None:
         roof["hbm_achieved_gbs"] = traffic / kern_s / 1e9
-    per_step = {"aim": 1, "candidates": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "trace": 1, "finalize": 1,
-                "smooth": 1}
+    per_step = {"aim": 1, "candidates": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "point_masks": 1,
+                "trace": 1, "finalize": 1, "smooth": 1}
     if w.grid.fine_div > 1:
         per_step["grid_coarse"] = 1
     launches = sum(per_step.values())
@@ -566,7 +566,7 @@ def b200_arm(a, rank, world, local):
                        "parallelism": "ray shards per GPU + NCCL all-reduce of maps" if world > 1 else "1 GPU",
                        "l2": "flushed between timed steps (256 MB write)",
                        "grid": grid_name(w.grid),
-                       "step": "aim + occluder candidates + grid build + trace + flux scaling + trimmed-mean smoothing"},
+                       "step": "aim + occluder candidates + grid build + point masks + trace + flux scaling + trimmed-mean smoothing"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "flux_rmse": accuracy,
             "gpu_launches": launches * a.steps,
             "launches_per_step": per_step,
