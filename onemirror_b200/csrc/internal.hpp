@@ -52,7 +52,7 @@ qmcrt_status receiver_setup(const qmcrt_receiver& r, ReceiverGeom* g);
 // ends at 9.3 mrad for every CSR; the host checks each table against it.
 constexpr double kSunAlphaMax = 9.31e-3;
 // Largest |z| of the slope-error deviate sqrt(-2 ln u1) cos(2 pi u2) with
-// 24-bit uniforms (u1 >= 2^-25): 5.89, in units of sigma.
+// 23-bit uniforms (u1 >= 2^-24): 5.77, in units of sigma.
 constexpr double kSlopeZMax = 6.0;
 
 // Heliostat centres bucketed on a 2D grid over (x, z), rebuilt on the host

@@ -433,20 +433,20 @@ struct RaySetup {
 __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                                float sigma, float3* sl, float3* tl, const uint2* rk) {
   uint4 r = philox4x32_10_rk(make_uint4(ray, 0u, a.item, kTagTrace), rk);
-  float th = buie_theta_mrad(a, s_tab, s_guide, u24f(r.x)) * 1e-3f;
+  float th = buie_theta_mrad(a, s_tab, s_guide, u23f(r.x)) * 1e-3f;
   float st, ct, sp, cp;
   // The azimuths and the Box-Muller log use the hardware approximations
   // (__sincosf, __logf: absolute errors near 2^-21): they scale milliradian
   // polar angles, so a direction moves by ~1e-9 rad, far below FP32 rounding
   // of the geometry that follows.
   sincos_small(th, &st, &ct);  // th <= 9.3 mrad
-  __sincosf(6.28318531f * u24f(r.y), &sp, &cp);
+  __sincosf(6.28318531f * u23f(r.y), &sp, &cp);
   *sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
-  float z = sqrtf(-2.f * __logf(u24f(r.z))) * __cosf(6.28318531f * u24f(r.w));
+  float z = sqrtf(-2.f * __logf(u23f(r.z))) * __cosf(6.28318531f * u23f(r.w));
   float ths = sigma * z;
   uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
   sincos_small(ths, &st, &ct);
-  __sincosf(6.28318531f * u24f(extra), &sp, &cp);
+  __sincosf(6.28318531f * u23f(extra), &sp, &cp);
   *tl = f3(st * cp, ct, st * sp);
 }
 

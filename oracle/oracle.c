@@ -37,7 +37,8 @@ void orc_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint3
   out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-static inline double u24(uint32_t w) { return ((double)(w >> 8) + 0.5) * (1.0 / 16777216.0); }
+/* the tracer's uniform: (k + 0.5) 2^-23, k the top 23 bits of the Philox word */
+static inline double u23(uint32_t w) { return ((double)(w >> 9) + 0.5) * (1.0 / 8388608.0); }
 
 /* ------------------------------------------------------------ Buie */
 static float buie_core(float theta) {
@@ -498,11 +499,11 @@ void orc_ray_samples(const orc_trace_cfg* c, double sigma, uint64_t ray, double 
   uint32_t key[2] = {(uint32_t)c->seed, (uint32_t)(c->seed >> 32)};
   uint32_t w[4];
   orc_philox4x32_10(ctr, key, w);
-  double th = orc_buie_sample(u24(w[0]), c->cdf_x, c->cdf_y, c->slope, c->bparams) / 1000.0;
-  angle2xyz(th, 2.0 * M_PI * u24(w[1]), sun_local);
-  double z = sqrt(-2.0 * log(u24(w[2]))) * cos(2.0 * M_PI * u24(w[3]));
+  double th = orc_buie_sample(u23(w[0]), c->cdf_x, c->cdf_y, c->slope, c->bparams) / 1000.0;
+  angle2xyz(th, 2.0 * M_PI * u23(w[1]), sun_local);
+  double z = sqrt(-2.0 * log(u23(w[2]))) * cos(2.0 * M_PI * u23(w[3]));
   uint32_t extra = (w[0] & 0xFFu) | ((w[1] & 0xFFu) << 8) | ((w[2] & 0xFFu) << 16) | ((w[3] & 0xFFu) << 24);
-  angle2xyz(sigma * z, 2.0 * M_PI * u24(extra), turb_local);
+  angle2xyz(sigma * z, 2.0 * M_PI * u23(extra), turb_local);
 }
 
 /* one ray given its local samples; the body of map_tracing
