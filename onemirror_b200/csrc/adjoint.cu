@@ -542,6 +542,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.t.point_xz = s->d_point_xz;
   A.t.point_helio = s->d_point_helio;
   A.t.point_mask = s->d_point_mask;
+  A.t.point_origin = s->d_point_origin;
   A.t.energy = t->d_energy;
   double l1 = 0, l2 = 0;
   for (int i = 0; i < 3; ++i) {
@@ -608,6 +609,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   A.t.point_xz = s->d_point_xz;
   A.t.point_helio = s->d_point_helio;
   A.t.point_mask = s->d_point_mask;
+  A.t.point_origin = s->d_point_origin;
   A.t.energy = t->d_energy;
   A.grad_aim = d_grad_aim;
   A.grad_tilt = d_grad_tilt;

@@ -207,6 +207,7 @@ struct qmcrt_batch {
     float* d_energy = nullptr;
     float* d_flux = nullptr;
     uint2* d_mask = nullptr;  // per-point candidate masks for this item's sun
+    double4* d_origin = nullptr;  // the points in world coordinates for this item's sun
     const float2* pts = nullptr;
     const int32_t* pts_helio = nullptr;
     int64_t points = 0;
@@ -288,7 +289,8 @@ static qmcrt_status enqueue_pass(qmcrt_batch* b, cudaStream_t st) {
     auto& it = b->items[i];
     cudaStream_t s = b->side[i % K];
     if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, s))) return e;
-    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.points, it.d_mask, s))) return e;
+    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.points, it.d_mask, it.d_origin, s)))
+      return e;
     QM_CUDA(cudaMemsetAsync(it.d_counts, 0, it.res * sizeof(uint32_t), s));
     QM_CUDA(cudaMemsetAsync(it.d_energy, 0, it.res * sizeof(float), s));
   }
@@ -404,13 +406,14 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     it.pts = a.point_xz;
     it.pts_helio = a.point_helio;
     it.points = scenes[items[i].scene]->points;
-    if ((e = balloc(&it.d_mask, it.points))) goto fail;
+    if ((e = balloc(&it.d_mask, it.points)) || (e = balloc(&it.d_origin, it.points))) goto fail;
     // every candidate until a pass builds the masks for the item's sun
     if (cudaMemset(it.d_mask, 0xFF, it.points * sizeof(uint2)) != cudaSuccess) {
       e = set_error(QMCRT_ERR_CUDA, "batch mask initialisation");
       goto fail;
     }
     a.point_mask = it.d_mask;
+    a.point_origin = it.d_origin;
     a.weight = b->weights[items[i].scene];
     a.counts = it.d_counts;
     a.energy = it.d_energy;
@@ -445,6 +448,7 @@ qmcrt_status qmcrt_batch_destroy(qmcrt_batch* b) {
   for (auto& it : b->items) {
     free_sun_geom(&it.geo);
     cudaFree(it.d_mask);
+    cudaFree(it.d_origin);
     cudaFree(it.d_counts);
     cudaFree(it.d_energy);
     cudaFree(it.d_flux);
@@ -487,7 +491,8 @@ qmcrt_status qmcrt_batch_autotune(qmcrt_batch* b, qmcrt_batch_tuning* chosen, vo
   for (int i = 0; i < n; ++i) {
     auto& it = b->items[i];
     if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, st))) return e;
-    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.points, it.d_mask, st))) return e;
+    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.points, it.d_mask, it.d_origin, st)))
+      return e;
   }
   cudaEvent_t e0, e1;
   QM_CUDA(cudaEventCreate(&e0));

@@ -157,6 +157,7 @@ struct qmcrt_scene {
   double sun_unit[3] = {0, 0, 0};   // the normalised sun direction of the current geometry
   int64_t mask_cap = 0;
   uint2* d_point_mask = nullptr;     // [points] (shadow, block) candidate bits
+  double4* d_point_origin = nullptr; // [points] the points in world coordinates for the current sun
   float2* d_point_xz = nullptr;
   int32_t* d_point_helio = nullptr;
   float* d_helio_weight = nullptr;  // [n] mirror area per point
@@ -188,9 +189,11 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
                              cudaStream_t st);
 qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
 // Per-point candidate masks of `points` points (xz, helio) for geometry g of
-// scene s and the (normalised) sun, into mask.
+// scene s and the (normalised) sun, into mask, and the points' world
+// coordinates (the rays' origins) into origin.
 qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
-                                const int32_t* helio, int64_t points, uint2* mask, cudaStream_t st);
+                                const int32_t* helio, int64_t points, uint2* mask, double4* origin,
+                                cudaStream_t st);
 // The scene's masks for its current sun and points (rebuilt when stale).
 qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st);
 }  // namespace qm

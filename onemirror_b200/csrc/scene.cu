@@ -509,7 +509,8 @@ struct MaskArgs {
   const float* sigma;
   double sun[3];
   double shadow_tan, sun_alpha, zmax;
-  uint2* mask;  // [points] (shadow bits, block bits)
+  uint2* mask;      // [points] (shadow bits, block bits)
+  double4* origin;  // [points] the point in world coordinates (the rays' origin)
 };
 
 // Can a ray from point p, leaving within atan(tan_a) of the unit axis d, meet
@@ -555,6 +556,7 @@ __global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
   const double* F = a.frame + kFrameStride * h;
   const d3 u = mk(F[0], F[1], F[2]), n = mk(F[3], F[4], F[5]), v = mk(F[6], F[7], F[8]);
   const d3 p = mk(F[9], F[10], F[11]) + (double)xz.x * u + (double)xz.y * v;
+  a.origin[g] = make_double4(p.x, p.y, p.z, 0.0);
   const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
   uint32_t bits[2] = {0u, 0u};
   for (int w = 0; w < 2; ++w) {
@@ -845,7 +847,8 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
 }
 
 qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
-                                const int32_t* helio, int64_t points, uint2* mask, cudaStream_t st) {
+                                const int32_t* helio, int64_t points, uint2* mask, double4* origin,
+                                cudaStream_t st) {
   if (points <= 0) return QMCRT_OK;
   MaskArgs m{};
   m.points = points;
@@ -860,6 +863,7 @@ qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const do
   m.sun_alpha = kSunAlphaMax;
   m.zmax = kSlopeZMax;
   m.mask = mask;
+  m.origin = origin;
   point_mask_kernel<<<(unsigned)((points + 255) / 256), 256, 0, st>>>(m);
   QM_CUDA(cudaGetLastError());
   return QMCRT_OK;
@@ -869,13 +873,15 @@ qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st) {
   if (s->mask_geom == s->geom_version && s->mask_points == s->points_version) return QMCRT_OK;
   if (s->mask_cap < s->points) {
     dev_free(s->d_point_mask);
+    dev_free(s->d_point_origin);
     s->mask_cap = 0;
     qmcrt_status e = dev_alloc(&s->d_point_mask, (size_t)s->points);
+    if (!e) e = dev_alloc(&s->d_point_origin, (size_t)s->points);
     if (e) return e;
     s->mask_cap = s->points;
   }
   qmcrt_status e = launch_point_masks(s, scene_geom(s), s->sun_unit, s->d_point_xz, s->d_point_helio, s->points,
-                                      s->d_point_mask, st);
+                                      s->d_point_mask, s->d_point_origin, st);
   if (e) return e;
   s->mask_geom = s->geom_version;
   s->mask_points = s->points_version;
@@ -1282,7 +1288,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_rect); dev_free(s->d_cellbox); dev_free(s->d_cell_count); dev_free(s->d_cell_start);
   dev_free(s->d_entries); dev_free(s->d_cell_rect); dev_free(s->d_cell_info); dev_free(s->d_coarse_yr); dev_free(s->d_cand); dev_free(s->d_cand_n); dev_free(s->d_field_yr);
   dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_cyl_edge);
-  dev_free(s->d_point_mask); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
+  dev_free(s->d_point_mask); dev_free(s->d_point_origin); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
   dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)

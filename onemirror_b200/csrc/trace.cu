@@ -347,6 +347,7 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   a.point_helio = s->d_point_helio;
   if ((e = ensure_masks(s, st))) return e;
   a.point_mask = s->d_point_mask;
+  a.point_origin = s->d_point_origin;
   return run_and_finish(s, sun, p, a, false, 1.0, out, stats, st);
 }
 

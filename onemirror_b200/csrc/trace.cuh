@@ -34,6 +34,7 @@ struct TraceArgs {
   const float4* cand;   // [n][2][kCandCap][3]
   const int* cand_n;    // [n][2]
   const uint2* point_mask;  // [points] candidates reachable from each point (shadow, block bits); NULL: all
+  const double4* point_origin;  // [points] world coordinates of each point (Philox traces; table mode computes them)
   const float4* rect;   // [3n] every heliostat's own rectangle record
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
@@ -461,15 +462,20 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
   R.h = h;
   R.xz = __ldg(a.point_xz + g);
   R.reach = a.point_mask ? __ldg(a.point_mask + g) : make_uint2(0xffffffffu, 0xffffffffu);
-  // the 96-byte frame record (16-byte aligned) as six 16-byte loads
+  // the frame axes (16-byte aligned record) as 16-byte loads
   const double2* F = reinterpret_cast<const double2*>(a.frame + kFrameStride * h);
-  const double2 q0 = __ldg(F), q1 = __ldg(F + 1), q2 = __ldg(F + 2), q3 = __ldg(F + 3), q4 = __ldg(F + 4),
-                q5 = __ldg(F + 5);
+  const double2 q0 = __ldg(F), q1 = __ldg(F + 1), q2 = __ldg(F + 2), q3 = __ldg(F + 3), q4 = __ldg(F + 4);
   R.fr.u = mk(q0.x, q0.y, q1.x);
   R.fr.n = mk(q1.y, q2.x, q2.y);
   R.fr.v = mk(q3.x, q3.y, q4.x);
-  // origin: the mirror centre plus the point's in-plane offset
-  R.o = mk(q4.y, q5.x, q5.y) + (double)R.xz.x * R.fr.u + (double)R.xz.y * R.fr.v;
+  if (TABLES) {  // origin: the mirror centre plus the point's in-plane offset
+    const double2 q5 = __ldg(F + 5);
+    R.o = mk(q4.y, q5.x, q5.y) + (double)R.xz.x * R.fr.u + (double)R.xz.y * R.fr.v;
+  } else {  // the same, computed once per point and sun by the mask pass
+    const double2* O = reinterpret_cast<const double2*>(a.point_origin + g);  // 32-byte records
+    const double2 oa = __ldg(O), ob = __ldg(O + 1);
+    R.o = mk(oa.x, oa.y, ob.x);
+  }
   R.w = 1.f;
   if (TABLES) {
     // (start + j) mod T, kept in [0, T) for any caller-provided start
