@@ -551,9 +551,11 @@ def b200_arm(a, rank, world, local):
             "executed_flops_per_ray": exe, "executed_tflops": rays * exe / kern_s / 1e12,
             "executed_frac": rays * exe / kern_s / 1e12 / best,
             "rect_tests_per_ray": gpu_stats[5] / gpu_stats[0], "dda_cells_per_ray": gpu_stats[6] / gpu_stats[0],
-            "hbm_peak_gbs_of_measured": peaks.get("hbm_gbs")}
+            "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0),
+            "hbm_peak_source": "measured copy" if "hbm_gbs" in peaks else "fallback (6.65 TB/s, earlier copy on B200)"}
     if traffic is not None:
         roof["hbm_achieved_gbs"] = traffic / kern_s / 1e9
+        roof["hbm_frac"] = roof["hbm_achieved_gbs"] / roof["hbm_peak_gbs"]
     per_step = {"aim": 1, "candidates": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "point_masks": 1,
                 "trace": 1, "finalize": 1, "smooth": 1}
     if w.grid.fine_div > 1:
