@@ -2,7 +2,8 @@
 test_gpu_parity): one heliostat, rays-per-point that is not a power of two,
 regular grid points through the full trace, given normals / tilts /
 per-heliostat slope errors, a sun below the horizon, zero DNI, accumulation,
-the largest ray count, and the arguments that must be rejected."""
+one scene across suns and point sets, the largest ray count, and the
+arguments that must be rejected."""
 import numpy as np
 import pytest
 
@@ -113,6 +114,32 @@ def test_zero_dni_and_accumulation():
     sc.trace(w.sun, p, stats=False, outputs=out)
     assert torch.equal(out[1]["counts"], 2 * counts)
     assert torch.allclose(out[1]["flux"], 2 * flux, rtol=1e-6, atol=1e-3)
+    sc.close()
+
+
+def test_one_scene_across_suns_and_point_sets_equals_fresh_scenes():
+    """A scene keeps its per-sun passes (aiming, occluder candidates, the
+    points' candidate masks and world coordinates) and its points between
+    traces, and rebuilds them when the sun or the point set changes: one
+    scene traced under sun A, sun B, a second point set, and sun A again
+    gives, ray for ray, what a fresh scene gives for each trace."""
+    w = W.small()
+    sun_b = W.make_sun(25.0, 120.0)
+    p_other = W.params(int(w.params.rays), 128, 0.2)  # 32 points per mirror
+    steps = [(w.sun, w.params), (sun_b, w.params), (w.sun, p_other), (w.sun, w.params)]
+    sc = SolarScene.from_workload(w)
+    for sun, params in steps:
+        h = sc.trace(sun, params)  # the production kernel meets the change first
+        counts = h["counts"].clone()
+        g = sc.trace(sun, params, records=True)
+        fresh = SolarScene.from_workload(w)
+        f = fresh.trace(sun, params, records=True)
+        torch.cuda.synchronize()
+        assert torch.equal(g["flags"], f["flags"]) and torch.equal(g["pixel"], f["pixel"])
+        assert torch.equal(counts, f["counts"]) and torch.equal(g["counts"], f["counts"])
+        assert (g["stats"].hit, g["stats"].shadowed, g["stats"].blocked) == (f["stats"].hit, f["stats"].shadowed,
+                                                                             f["stats"].blocked)
+        fresh.close()
     sc.close()
 
 
