@@ -37,7 +37,7 @@ UNIT = "rays/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="mid", choices=["small", "mid", "large"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
@@ -168,7 +168,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu_id)], stdout=subprocess.PIPE,
+                                          "-lms", "50", "-i", str(self.gpu_id)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -177,9 +177,11 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
-    def stop(self):
+    def stop(self, window=None):
+        """Summary of the samples that arrived within window = (t0, t1) (host
+        clock; all samples when none arrived there or no window is given)."""
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -187,9 +189,20 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        return self.summarise(self.lines, window)
+
+    @staticmethod
+    def summarise(lines, window=None):
+        """Median SM clock, max clock and the throttle reasons seen in
+        (arrival time, csv line) samples of FIELDS, keeping those that arrived
+        in window (a sample arrives at most one interval after it was taken)."""
+        inside = [ln for ts, ln in lines if window is None or window[0] <= ts <= window[1] + 0.05]
+        scope = "timed region"
+        if not inside:
+            inside, scope = [ln for _, ln in lines], "whole run (no sample inside the timed region)"
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -202,7 +215,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "scope": scope}
 
 
 # ------------------------------------------------------------------ arms
@@ -454,7 +467,8 @@ def b200_arm(a, rank, world, local):
     clk = ClockSampler(local if "CUDA_VISIBLE_DEVICES" not in os.environ else
                        os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local])
     clk.start()
-    time.sleep(0.3)
+    time.sleep(0.3)  # nvidia-smi's first samples; the summary keeps only the timed region's
+    t_begin = time.time()
     step_ms, kern_ms, setup_ms = [], [], []
     for k in range(a.steps):
         flush.zero_()
@@ -470,7 +484,7 @@ def b200_arm(a, rank, world, local):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = clk.stop()
+    clocks = clk.stop((t_begin, time.time()))
     total_ms = float(sum(step_ms))
     if world > 1:
         tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
