@@ -108,22 +108,32 @@ void buie_with_guide(float csr, BuieTable* t) {
   t->host.resize(1025 + 1025 + 1024 + kBuieBuckets);
   float* h = t->host.data();
   buie_build(csr, h, h + 1025, h + 2050, t->params);
-  // guide table: for each uniform bucket of [0, core), a lower bound of the
-  // interval index of every value the kernel maps to that bucket (one below
-  // the index at the bucket's lower edge, which absorbs float rounding of the
-  // bucket computation; CDF intervals are far wider than that rounding)
+  // guide table: for each uniform bucket of [0, core), the interval index of
+  // the smallest float the kernel maps to that bucket ((int)(uu * inv_bucket),
+  // one float multiply: the same rounding here), so a lower bound of the
+  // index of every value in the bucket, and the index itself unless an
+  // interval boundary falls inside the bucket (a warp then scans 1.2 steps on
+  // average at csr 0.1 instead of 2.2 with a bound one below)
   const float* cy = h + 1025;
-  float inv_bucket = (float)kBuieBuckets / t->params[2];
+  const float inv_bucket = (float)kBuieBuckets / t->params[2];
+  auto bucket_of = [inv_bucket](float x) {
+    volatile float p = x * inv_bucket;  // rounded to float, as the kernel's FMUL
+    return (int)p;
+  };
   for (int b = 0; b < kBuieBuckets; ++b) {
-    float edge = (float)b / inv_bucket;
+    float edge = 0.f;
+    if (b > 0) {
+      edge = (float)b / inv_bucket;
+      while (bucket_of(edge) < b) edge = std::nextafter(edge, HUGE_VALF);
+      while (bucket_of(std::nextafter(edge, 0.f)) >= b) edge = std::nextafter(edge, 0.f);
+    }
     int lo = 0, hi = 1024;
     while (lo < hi) {  // largest i with cy[i] <= edge
       int mid = (lo + hi + 1) >> 1;
       if (cy[mid] <= edge) lo = mid;
       else hi = mid - 1;
     }
-    int g = std::max(lo - 1, 0);
-    std::memcpy(h + 3074 + b, &g, sizeof(int));
+    std::memcpy(h + 3074 + b, &lo, sizeof(int));
   }
   t->inv_bucket = inv_bucket;
   t->csr = csr;
