@@ -184,7 +184,7 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
   // with CULL (corrected mode) the heliostat's occluder candidates answer the
   // visibility questions (the grid walk where there are none)
   uint32_t nt = 0, nc = 0;
-  const float3 of = to_f(R.o);
+  const float3 of = R.of;
   const float3 sd = f3((float)-R.ws.x, (float)-R.ws.y, (float)-R.ws.z);
   if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc, R.reach.x)
            : dda_blocked<false, false>(a, of, sd, R.h, fy0, fy1, nt, nc))

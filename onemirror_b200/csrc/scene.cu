@@ -510,7 +510,7 @@ struct MaskArgs {
   double sun[3];
   double shadow_tan, sun_alpha, zmax;
   uint2* mask;      // [points] (shadow bits, block bits)
-  double4* origin;  // [points] the point in world coordinates (the rays' origin)
+  double4* origin;  // [points] the point in world coordinates (the rays' origin); w: float x, y
 };
 
 // Can a ray from point p, leaving within atan(tan_a) of the unit axis d, meet
@@ -556,7 +556,8 @@ __global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
   const double* F = a.frame + kFrameStride * h;
   const d3 u = mk(F[0], F[1], F[2]), n = mk(F[3], F[4], F[5]), v = mk(F[6], F[7], F[8]);
   const d3 p = mk(F[9], F[10], F[11]) + (double)xz.x * u + (double)xz.y * v;
-  a.origin[g] = make_double4(p.x, p.y, p.z, 0.0);
+  // the spare 8 bytes carry the float x and y the walks use (low, high word)
+  a.origin[g] = make_double4(p.x, p.y, p.z, __hiloint2double(__float_as_int((float)p.y), __float_as_int((float)p.x)));
   const d3 s = mk(a.sun[0], a.sun[1], a.sun[2]);
   uint32_t bits[2] = {0u, 0u};
   for (int w = 0; w < 2; ++w) {

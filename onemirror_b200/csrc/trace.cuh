@@ -34,7 +34,9 @@ struct TraceArgs {
   const float4* cand;   // [n][2][kCandCap][3]
   const int* cand_n;    // [n][2]
   const uint2* point_mask;  // [points] candidates reachable from each point (shadow, block bits); NULL: all
-  const double4* point_origin;  // [points] world coordinates of each point (Philox traces; table mode computes them)
+  // [points] world coordinates of each point, w holding their float x and y
+  // (Philox traces; table mode computes them)
+  const double4* point_origin;
   const float4* rect;   // [3n] every heliostat's own rectangle record
   const int* field_yr;    // [2] height range of the field (order-preserving ints)
   float gpos[3], gcell[3], ginv[3];  // ginv = 1 / gcell
@@ -421,6 +423,7 @@ struct RaySetup {
   uint2 reach;  // candidate masks of the ray's point (shadow, block)
   frame64 fr;
   d3 o;
+  float3 of;  // o rounded to float
   float3 sl, tl;
   d3 ws;
   float w;
@@ -471,10 +474,12 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
   if (TABLES) {  // origin: the mirror centre plus the point's in-plane offset
     const double2 q5 = __ldg(F + 5);
     R.o = mk(q4.y, q5.x, q5.y) + (double)R.xz.x * R.fr.u + (double)R.xz.y * R.fr.v;
+    R.of = to_f(R.o);
   } else {  // the same, computed once per point and sun by the mask pass
     const double2* O = reinterpret_cast<const double2*>(a.point_origin + g);  // 32-byte records
     const double2 oa = __ldg(O), ob = __ldg(O + 1);
     R.o = mk(oa.x, oa.y, ob.x);
+    R.of = f3(__int_as_float(__double2loint(ob.y)), __int_as_float(__double2hiint(ob.y)), (float)ob.x);
   }
   R.w = 1.f;
   if (TABLES) {
@@ -514,7 +519,7 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_ta
   }
   const int h = R.h;
   const d3 o = R.o, ws = R.ws;
-  const float3 of = to_f(o);
+  const float3 of = R.of;
   // perturbed normal, reflected direction (i - 2 n (n.i)) and energy first,
   // so that the mirror frame is dead before the walks.  The reflection keeps
   // the length of ws (1 to float rounding of the sample), and nothing that
