@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--cell", type=float, default=0.0, help="override the grid cell size (m; the coarse cell of a two-level grid)")
     ap.add_argument("--fine-div", type=int, default=-1, help="override the two-level grid split (1 = one level)")
     ap.add_argument("--sun-elev", type=float, default=None, help="override the sun elevation (degrees)")
+    ap.add_argument("--no-fields", action="store_true", help="skip the small- and large-field sub-blocks")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip the timing of the reference's CUDA build")
+    ap.add_argument("--ref-cuda-child", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-cuda-reps", type=int, default=3, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -219,6 +223,19 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ arms
+STEP = ("aim + occluder candidates + grid build + point masks + trace + flux scaling + all-reduce of the maps "
+        "(N > 1) + trimmed-mean smoothing of the summed count map; the Poisson sample points depend only on the "
+        "mirror sizes and are sampled once per scene, before the timed steps")
+SUN_ELEV = {"small": 45.0, "mid": 30.0, "large": 20.0}
+
+
+def bench_config(w, world):
+    """The `config` of both arms' lines (identical for the same workload)."""
+    return {"workload": workload_name(w), "rays_per_step_per_gpu": int(w.params.rays), "heliostats": w.n,
+            "parallelism": "ray shards per GPU + NCCL all-reduce of maps" if world > 1 else "1 GPU",
+            "l2": "flushed between timed steps (256 MB write)", "grid": grid_name(w.grid), "step": STEP}
+
+
 def reference_arm(a, rank, world):
     if rank != 0:
         return
@@ -239,7 +256,7 @@ def reference_arm(a, rank, world):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * secs / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(w), "rays_per_step": int(w.params.rays)},
+            "config": bench_config(w, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -399,11 +416,267 @@ def read_traffic(name):
     return None
 
 
+class FieldRun:
+    """One workload traced step after step on this rank's GPU: the timed
+    device step, and the same step end to end on host buffers."""
+
+    def __init__(self, w, rank, world, dev, flush, sun_elev=None, variant=0):
+        from onemirror_b200.scene import SolarScene
+        self.w, self.rank, self.world, self.dev, self.flush = w, rank, world, dev, flush
+        self.sc = SolarScene.from_workload(w)
+        self.p = w.params
+        self.p.kernel_variant = variant
+        self.rays = int(self.p.rays)
+        self.sun_elev = SUN_ELEV[w.name] if sun_elev is None else sun_elev
+        self.base_az = 180.0
+        self.outs = self.sc._outputs(self.rays, False)
+
+    def sun(self, k):
+        from onemirror_b200 import workloads as W
+        return W.make_sun(self.sun_elev, self.base_az + 0.01 * k, self.w.sun.dni, self.w.sun.csr)
+
+    def smooth(self, counts):
+        from onemirror_b200 import capi
+        from onemirror_b200.scene import image_smooth
+        return image_smooth(counts, self.w.smooth_radius, self.w.smooth_ratio, capi.TRIM_SORTED)
+
+    def step(self, k, item, want_stats=False):
+        """Trace with a sun moved by 0.01 deg per step, exchange the maps
+        (N > 1), smooth the summed count map."""
+        from onemirror_b200 import dist as D
+        self.p.item = item
+        r = self.sc.trace(self.sun(k), self.p, stats=want_stats, outputs=self.outs)
+        _, _, sm = D.step_maps(r["counts"], r["energy"], self.smooth)
+        return r, sm
+
+    def timed(self, steps, k0):
+        """`steps` device-timed steps, L2 flushed before each (outside the
+        events); returns per-step ms, trace-kernel ms and setup ms."""
+        import torch
+        from onemirror_b200 import dist as D
+        step_ms, kern_ms, setup_ms = [], [], []
+        for k in range(steps):
+            self.flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.step(k0 + k, D.shard_item(self.rank, k))
+            e1.record()
+            t = self.sc.timing()
+            kern_ms.append(t.trace_kernel_ms)
+            setup_ms.append(t.setup_ms)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        return step_ms, kern_ms, setup_ms
+
+    def e2e(self, steps):
+        """The same step end to end on pinned host buffers, L2 flushed before
+        each call (outside the timed span).  One GPU: one qmcrt_results_host
+        call (field upload, trace, scaling, smoothing, download of counts,
+        flux and smoothed map).  N GPUs: the field upload, qmcrt_trace, the
+        map exchange and smoothing, then the download of the summed maps.
+        Host clock per step, the slowest rank's total."""
+        import torch
+        from onemirror_b200 import capi
+        from onemirror_b200 import dist as D
+        sc, w = self.sc, self.w
+        for name in ("pos", "size", "aim"):  # the field the call uploads, from pinned memory
+            v = getattr(sc, name)
+            if v is not None:
+                setattr(sc, name, torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy())
+        h2d = sum(getattr(sc, nm).nbytes for nm in ("pos", "size", "aim") if getattr(sc, nm) is not None)
+        res = w.res
+        if self.world == 1:
+            out = {"counts": torch.zeros(res, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                   "flux": torch.zeros(res, dtype=torch.float32).pin_memory().numpy(),
+                   "smoothed": torch.zeros(res, dtype=torch.float32).pin_memory().numpy()}
+            d2h = sum(v.nbytes for v in out.values())
+            call = "qmcrt_results_host (field upload, trace, flux scaling, smoothing, map downloads)"
+        else:
+            hc = torch.zeros(res, dtype=torch.int64).pin_memory()
+            he = torch.zeros(res, dtype=torch.float64).pin_memory()
+            hs = torch.zeros(res, dtype=torch.float32).pin_memory()
+            d2h = hc.numel() * 8 + he.numel() * 8 + hs.numel() * 4
+            call = "qmcrt_scene_set_field + qmcrt_trace + NCCL all-reduce + qmcrt_smooth_trimmed_u32 + map downloads"
+        total = 0.0
+        for k in range(steps + 1):
+            self.flush.zero_()
+            torch.cuda.synchronize()
+            if self.world > 1:
+                import torch.distributed as dist
+                dist.barrier()
+            t0 = time.perf_counter()
+            self.p.item = D.shard_item(self.rank, 9000 + k)
+            sun = self.sun(-(k + 1))
+            if self.world == 1:
+                sc.results_host(sun, self.p, w.smooth_radius, w.smooth_ratio, capi.TRIM_SORTED, capi.SMOOTH_COUNTS,
+                                out=out)
+            else:
+                sc.update_field()
+                r = sc.trace(sun, self.p, stats=False, outputs=self.outs)
+                c, e, sm = D.step_maps(r["counts"], r["energy"], self.smooth)
+                hc.copy_(c, non_blocking=True)
+                he.copy_(e, non_blocking=True)
+                hs.copy_(sm, non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+            if k:
+                total += time.perf_counter() - t0
+        if self.world > 1:
+            total = D.max_over_ranks(total, self.dev)
+        return {"value": self.rays * self.world * steps / total, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "call": call, "ms_per_step": 1e3 * total / steps,
+                "l2": "flushed before each step, outside the timed span"}
+
+    def close(self):
+        self.sc.close()
+
+
+def field_block(name, rank, world, dev, flush, steps, e2e_steps, warmup=3):
+    """Throughput of another field at its own configuration (a sub-block of
+    the default line): device-timed steps and the end-to-end call."""
+    import statistics as S
+    from onemirror_b200 import workloads as W
+    w = W.BUILDERS[name]()
+    run = FieldRun(w, rank, world, dev, flush)
+    for k in range(warmup):
+        run.step(k, 60000 + k)
+    step_ms, kern_ms, _ = run.timed(steps, warmup)
+    e2e = run.e2e(e2e_steps)
+    run.close()
+    total = sum(step_ms)
+    return {"value": run.rays * steps / (total * 1e-3), "unit": UNIT, "steps": steps, "warmup": warmup,
+            "ms_per_step": total / steps, "trace_kernel_ms": S.mean(kern_ms), "e2e": e2e,
+            "config": bench_config(w, world)}
+
+
+# ----------------------------------------------- the reference's CUDA build
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+
+
+def aimed_normals(pos, aim, sun):
+    """Unit bisectors of the reversed incident sun direction and the direction
+    to each aim point (the reference's CRotate(focus, sun), heliostat.cpp:16-21)."""
+    to_t = aim.astype(np.float64) - pos
+    to_t /= np.linalg.norm(to_t, axis=1, keepdims=True)
+    n = to_t - np.asarray(sun, np.float64)[None, :] / np.linalg.norm(sun)
+    return (n / np.linalg.norm(n, axis=1, keepdims=True)).astype(np.float32)
+
+
+def ref_cuda_scene(name):
+    """Inputs of the reference's own pass (positions, sizes, normals, grid,
+    receiver, sunshape), and the CPU checks that keep its out-of-range
+    accesses from happening (see ref_cuda_child)."""
+    from onemirror_b200 import workloads as W
+    if name == "nine":
+        g = np.load(os.path.join(ROOT, "tests", "golden", "ref_gpu_vectors.npz"))
+        sc = dict(pos=g["trace_pos"], size=g["trace_size"], normal=g["trace_normal"], gpos=g["trace_gpos"],
+                  gsize=g["trace_gsize"], inter=g["trace_inter"], rpos=g["trace_rpos"], rsize=g["trace_rsize"],
+                  rnorm=g["trace_rnorm"], face=0, ginfo=16, pixel=float(g["trace_pl"]), sun=g["trace_sun"],
+                  dni=1000.0, csr=0.1, sigma=0.002,
+                  desc="the 9-heliostat scene of the reference's own GPU pin (2x2 m mirrors, 8x8 m receiver at 128x128)")
+    else:
+        w = W.mid()
+        pos, size = w.pos, w.size
+        hd = 0.5 * np.linalg.norm(size[:, [0, 2]], axis=1) + 1.0
+        lo = np.array([(pos[:, 0] - hd).min(), (pos[:, 1] - hd).min(), (pos[:, 2] - hd).min()], np.float32)
+        hi = np.array([(pos[:, 0] + hd).max(), (pos[:, 1] + hd).max(), (pos[:, 2] + hd).max()], np.float32)
+        inter = np.full(3, 25.0, np.float32)
+        sc = dict(pos=pos, size=size, normal=aimed_normals(pos, w.aim, np.asarray(w.sun.dir[:], np.float32)),
+                  gpos=lo, gsize=(hi - lo).astype(np.float32), inter=inter, rpos=np.array(w.receiver.pos[:], np.float32),
+                  rsize=np.array(w.receiver.size[:], np.float32), rnorm=np.array(w.receiver.normal[:], np.float32),
+                  face=0, ginfo=21, pixel=10.0 / 11.0, sun=np.asarray(w.sun.dir[:], np.float32), dni=1000.0,
+                  csr=float(w.sun.csr), sigma=float(w.sigma),
+                  desc="the mid field (1000 heliostats 10x10 m, aim offsets, 25 m cells), 11x11 grid micro-points "
+                       "per heliostat x 2048 rays, receiver 12x12 m at 21 px/m = 252x252 (the reference's integer "
+                       "pixels per metre)")
+    return sc
+
+
+def ref_cuda_checks(sc):
+    """CPU checks on the exact inputs: every registration cube of
+    CGridHelioMatch (half-side sqrt(|size|)/2, grid.cpp:49-59) and every
+    micro-point (on the mirror, within its half-diagonal of the centre) lies
+    inside the grid, so boxIntersect and NotCollision index in range."""
+    pos, size, gpos, gsize, inter = (np.asarray(sc[k], np.float64) for k in ("pos", "size", "gpos", "gsize", "inter"))
+    dims = np.ceil(gsize / inter).astype(int)
+    rad = np.sqrt(np.linalg.norm(size, axis=1)) / 2
+    lo = ((pos - rad[:, None]) - gpos) / inter
+    hi = ((pos + rad[:, None]) - gpos) / inter
+    if lo.min() < 0 or np.any(hi.astype(int) > dims - 1):
+        return "a registration cube leaves the grid"
+    hd = 0.5 * np.linalg.norm(size, axis=1)
+    if np.any(pos - hd[:, None] < gpos) or np.any(pos + hd[:, None] > gpos + gsize):
+        return "a micro-point may lie outside the grid"
+    return None
+
+
+def ref_cuda_child(name, reps):
+    """Run in a child process (the reference exits the process on any CUDA
+    error, utils.h:13-22): the reference's pass over one sun position on the
+    given scene, `reps` times; prints one JSON line."""
+    import torch  # noqa: F401  (CUDA context set-up on the same device as the parent)
+    sc = ref_cuda_scene(name)
+    why = ref_cuda_checks(sc)
+    if why:
+        print(json.dumps({"scene": name, "skipped": why}))
+        return
+    L = C.CDLL(REF_LIB)
+    fp = C.POINTER(C.c_float)
+    P = lambda a: np.ascontiguousarray(a, np.float32).ctypes.data_as(fp)  # noqa: E731
+    keep = {k: np.ascontiguousarray(sc[k], np.float32) for k in ("pos", "size", "normal", "gpos", "gsize", "inter",
+                                                                  "rpos", "rsize", "rnorm", "sun")}
+    n = keep["pos"].shape[0]
+    res = np.zeros(2, np.int32)
+    rays = C.c_longlong()
+    pass_ms = np.zeros(reps, np.float64)
+    trace_ms = np.zeros(reps, np.float32)
+    spill = C.c_int()
+    L.ref_run_field.restype = C.c_int
+    rc = L.ref_run_field(n, *(P(keep[k]) for k in ("pos", "size", "normal", "gpos", "gsize", "inter", "rpos", "rsize",
+                                                 "rnorm")), sc["face"], sc["ginfo"], C.c_float(sc["pixel"]),
+                         P(keep["sun"]), C.c_float(sc["dni"]), C.c_float(sc["csr"]), C.c_float(sc["sigma"]), 128, 2048,
+                         C.c_ulonglong(2018), reps, None, res.ctypes.data_as(C.POINTER(C.c_int)), C.byref(rays),
+                         pass_ms.ctypes.data_as(C.POINTER(C.c_double)), trace_ms.ctypes.data_as(fp), C.byref(spill))
+    if rc != 0:
+        print(json.dumps({"scene": name, "skipped": "reference pass returned %d" % rc}))
+        return
+    best = int(np.argmin(pass_ms[1:])) + 1 if reps > 1 else 0
+    print(json.dumps({"scene": name, "desc": sc["desc"], "heliostats": n, "rays": int(rays.value),
+                      "res": [int(res[0]), int(res[1])], "passes": reps, "pass_ms": float(np.median(pass_ms[1:] if reps > 1 else pass_ms)),
+                      "map_tracing_ms": float(np.median(trace_ms[1:] if reps > 1 else trace_ms)),
+                      "rays_per_s": float(rays.value / (np.median(pass_ms[1:] if reps > 1 else pass_ms) * 1e-3)),
+                      "map_tracing_rays_per_s": float(rays.value / (np.median(trace_ms[1:] if reps > 1 else trace_ms) * 1e-3)),
+                      "wrote_past_image": bool(spill.value), "best_pass": best}))
+
+
+def reference_cuda_section(local, reps=3):
+    """The reference's own CUDA build (oracle/_ref/libref.so, compiled from
+    its sources by oracle/ref.mk) on its per-heliostat structure: per
+    heliostat a cuRAND sun table, micro-points, vertices, groups and one
+    map_tracing launch followed by a device synchronisation (Gtest.cu:21-35,
+    recthelio_tracing.cpp:46-80, ray_tracing.cu:12-27).  A baseline, not the
+    measured product; each scene runs in a child process."""
+    if not os.path.exists(REF_LIB):
+        return {"unavailable": "oracle/_ref/libref.so is not built (the reference sources were absent at build time)"}
+    out = {}
+    env = dict(os.environ)
+    visible = env.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = visible.split(",")[local] if visible else str(local)
+    for name in ("nine", "mid"):
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-cuda-child", name,
+                                "--ref-cuda-reps", str(reps)], capture_output=True, text=True, timeout=900, env=env)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            out[name] = json.loads(lines[-1]) if r.returncode == 0 and lines else \
+                {"skipped": "child exited %d: %s" % (r.returncode, (r.stderr or r.stdout)[-300:])}
+        except subprocess.TimeoutExpired:
+            out[name] = {"skipped": "child timed out"}
+    return out
+
+
 def b200_arm(a, rank, world, local):
     import torch
     from onemirror_b200 import capi, workloads as W
     from onemirror_b200 import dist as D
-    from onemirror_b200.scene import SolarScene, image_smooth
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -416,14 +689,8 @@ def b200_arm(a, rank, world, local):
         w.grid.cell[:] = [a.cell] * 3
     if a.fine_div >= 0:
         w.grid.fine_div = a.fine_div
-    sc = SolarScene.from_workload(w)
-    p = w.params
-    p.kernel_variant = a.variant
-    rays = int(p.rays)
-    base_az = 180.0
-    sun_elev = a.sun_elev if a.sun_elev is not None else {"small": 45.0, "mid": 30.0, "large": 20.0}[a.workload]
     if a.sun_elev is not None:  # the oracle sample follows the same sun
-        w.sun = W.make_sun(sun_elev, base_az, w.sun.dni, w.sun.csr)
+        w.sun = W.make_sun(a.sun_elev, 180.0, w.sun.dni, w.sun.csr)
 
     # FP32 issue-rate peak, measured live (best of 5 bursts)
     sink = torch.zeros(8192, device=dev)
@@ -439,22 +706,12 @@ def b200_arm(a, rank, world, local):
         if it:
             best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
 
-    outs = sc._outputs(rays, False)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
-
-    def one(k, item, want_stats=False):
-        el, az = sun_elev, base_az + 0.01 * k
-        sun = W.make_sun(el, az, w.sun.dni, w.sun.csr)
-        p.item = item
-        r = sc.trace(sun, p, stats=want_stats, outputs=outs)
-        sm = image_smooth(r["counts"], w.smooth_radius, w.smooth_ratio, capi.TRIM_SORTED)
-        if world > 1:
-            D.reduce_maps(r["counts"], r["energy"])  # the one exchange: sum of the ranks' maps
-        return r, sm
-
+    run = FieldRun(w, rank, world, dev, flush, sun_elev=a.sun_elev, variant=a.variant)
+    sc, p, rays = run.sc, run.p, run.rays
     for k in range(a.warmup):
-        one(k, D.shard_item(rank, 1000 + k))
-    r, _ = one(a.warmup, D.shard_item(rank, 5000), want_stats=True)
+        run.step(k, D.shard_item(rank, 1000 + k))
+    r, _ = run.step(a.warmup, D.shard_item(rank, 5000), want_stats=True)
     gst = r["stats"]
     gpu_stats = [gst.rays, gst.shadowed, gst.blocked, gst.hit, gst.offmap, gst.rect_tests, gst.dda_cells]
     torch.cuda.synchronize()
@@ -469,68 +726,29 @@ def b200_arm(a, rank, world, local):
     clk.start()
     time.sleep(0.3)  # nvidia-smi's first samples; the summary keeps only the timed region's
     t_begin = time.time()
-    step_ms, kern_ms, setup_ms = [], [], []
-    for k in range(a.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        one(a.warmup + 1 + k, D.shard_item(rank, k))
-        e1.record()
-        t = sc.timing()
-        kern_ms.append(t.trace_kernel_ms)
-        setup_ms.append(t.setup_ms)
-        e1.synchronize()
-        step_ms.append(e0.elapsed_time(e1))
+    step_ms, kern_ms, setup_ms = run.timed(a.steps, a.warmup + 1)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clocks = clk.stop((t_begin, time.time()))
     total_ms = float(sum(step_ms))
     if world > 1:
-        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+        total_ms = D.max_over_ranks(total_ms, dev)
     value = rays * world * a.steps / (total_ms * 1e-3)
 
-    # end to end through the host-buffer entry point (pinned host memory)
-    e2e = None
-    if a.e2e_steps > 0:
-        pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
-               for k, v in (("pos", w.pos), ("size", w.size), ("aim", w.aim)) if v is not None}
-        counts = torch.zeros(w.res, dtype=torch.int32).pin_memory().numpy()
-        flux = torch.zeros(w.res, dtype=torch.float32).pin_memory().numpy()
-        f = capi.Field()
-        f.n = w.n
-        f.pos, f.size = capi.as_fp(pin["pos"]), capi.as_fp(pin["size"])
-        f.aim = capi.as_fp(pin["aim"]) if "aim" in pin else None
-        f.sigma = w.sigma
-        h2d = sum(v.nbytes for v in pin.values())
-        d2h = counts.nbytes + flux.nbytes
-        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-        for k in range(a.e2e_steps + 1):
-            if k == 1:
-                if world > 1:
-                    dist.barrier()
-                t0 = time.perf_counter()
-            sun = W.make_sun(sun_elev, base_az - 0.01 * (k + 1),
-                             w.sun.dni, w.sun.csr)
-            p.item = D.shard_item(rank, 9000 + k)
-            capi.check(capi.lib().qmcrt_trace_host(sc.h, C.byref(f), C.byref(sun), C.byref(p),
-                                                   counts.ctypes.data_as(capi.u32p), capi.as_fp(flux), None, stream))
-        dt = time.perf_counter() - t0
-        if world > 1:
-            tt = torch.tensor([dt], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            dt = float(tt.item())
-        e2e = {"value": rays * world * a.e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "call": "qmcrt_trace_host"}
+    e2e = run.e2e(a.e2e_steps) if a.e2e_steps > 0 else None
 
-    batch = adj = None
-    if rank == 0 and world == 1 and a.workload == "mid" and not a.rays:
+    batch = adj = refcuda = None
+    fields = {}
+    default_run = rank == 0 and world == 1 and a.workload == "mid" and not a.rays
+    if default_run:
         if not a.no_batch:
             batch = batch_section()
         if not a.no_adjoint:
             adj = adjoint_section()
+        if not a.no_fields:
+            fields["small"] = field_block("small", rank, world, dev, flush, steps=100, e2e_steps=20)
+            fields["large"] = field_block("large", rank, world, dev, flush, steps=10, e2e_steps=3)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         ob = oracle_sample(w, a.cpu_seconds)
@@ -542,6 +760,10 @@ def b200_arm(a, rank, world, local):
     else:
         ref_stats = None
         accuracy = None
+    if default_run and not a.no_ref_cuda:
+        refcuda = reference_cuda_section(local)
+        if "mid" in refcuda and "rays_per_s" in refcuda["mid"]:
+            refcuda["value_over_reference_mid"] = value / refcuda["mid"]["rays_per_s"]
     # Algorithmic flops per ray: the per-ray figure of the reference algorithm
     # (fixed work + traversal set-ups + 54 per rectangle test + 4 per DDA cell)
     # with the oracle's counts of rectangle tests and cells on a sample of the
@@ -565,6 +787,7 @@ def b200_arm(a, rank, world, local):
             "executed_flops_per_ray": exe, "executed_tflops": rays * exe / kern_s / 1e12,
             "executed_frac": rays * exe / kern_s / 1e12 / best,
             "rect_tests_per_ray": gpu_stats[5] / gpu_stats[0], "dda_cells_per_ray": gpu_stats[6] / gpu_stats[0],
+            "traffic_source": "committed ncu summary profiles/trace_kernel_%s.md (dram bytes of one launch)" % a.workload,
             "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0),
             "hbm_peak_source": "measured copy" if "hbm_gbs" in peaks else "fallback (6.65 TB/s, earlier copy on B200)"}
     if traffic is not None:
@@ -578,23 +801,21 @@ def b200_arm(a, rank, world, local):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(w), "rays_per_step_per_gpu": rays, "heliostats": w.n,
-                       "parallelism": "ray shards per GPU + NCCL all-reduce of maps" if world > 1 else "1 GPU",
-                       "l2": "flushed between timed steps (256 MB write)",
-                       "grid": grid_name(w.grid),
-                       "step": "aim + occluder candidates + grid build + point masks + trace + flux scaling + trimmed-mean smoothing"},
+            "config": bench_config(w, world),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "flux_rmse": accuracy,
             "gpu_launches": launches * a.steps,
             "launches_per_step": per_step,
             "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
             "clocks": clocks,
+            "fields": fields or None,
+            "reference_cuda": refcuda,
             "batched": batch,
             "adjoint": adj,
             "stats": {"shadowed": gst.shadowed / gst.rays, "blocked": gst.blocked / gst.rays,
                       "hit": gst.hit / gst.rays, "intercept_ratio": gst.intercept_ratio}}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sc.close()
+    run.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -602,6 +823,9 @@ def b200_arm(a, rank, world, local):
 def main():
     a = parse()
     rank, world, local = dist_env()
+    if a.ref_cuda_child:
+        ref_cuda_child(a.ref_cuda_child, a.ref_cuda_reps)
+        return
     if a.impl == "reference":
         reference_arm(a, rank, world)
         return

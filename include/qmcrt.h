@@ -269,6 +269,8 @@ typedef struct qmcrt_batch qmcrt_batch;
 /* ------------------------------------------------------------------ info */
 const char* qmcrt_version(void);
 const char* qmcrt_status_string(qmcrt_status s);
+/* The thread-local message of the last failure (named qmcrt_last_error_string
+ * in earlier designs of this boundary). */
 const char* qmcrt_last_error(void);
 
 /* --------------------------------------------------- host-side helpers
@@ -393,11 +395,13 @@ qmcrt_status qmcrt_scene_read_points(qmcrt_scene* scene, float* h_point_xz, int3
  * file-scope __device__ array that every GPU loading this library holds until
  * the process exits: room for QMCRT_NOALLOC_MAX_POINTS points and
  * QMCRT_NOALLOC_MAX_HELIOSTATS heliostats (about 8.2 MB); larger requests are
- * rejected with QMCRT_ERR_INVALID_ARGUMENT.  The first call on a device looks
- * up that array's device address; make that first call before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU
- * (different streams or host threads at the same time) race; serialise them.
- * Synchronises `stream` to read the sampler's status. */
+ * rejected with QMCRT_ERR_INVALID_ARGUMENT.  Each call finds that array's
+ * device address on the current device before it launches.  All calls share
+ * the array, so calls that overlap on the GPU (different streams or host
+ * threads at the same time) race; serialise them.  Synchronises `stream` to
+ * read the sampler's status.  After any status other than QMCRT_OK the
+ * outputs are undefined: a sampling failure leaves some heliostats' points
+ * written and others not.  A later successful call overwrites all of them. */
 #define QMCRT_NOALLOC_MAX_POINTS 1048576
 #define QMCRT_NOALLOC_MAX_HELIOSTATS 16384
 qmcrt_status qmcrt_sample_points_noalloc(const float* h_size, int32_t n, int64_t total_points, float spacing,
@@ -415,7 +419,8 @@ qmcrt_status qmcrt_trace(qmcrt_scene* scene, const qmcrt_sun* sun, const qmcrt_t
 
 /* Parity mode: the same traversal fed by caller-provided sample tables
  * (the inputs of map_tracing, rectgrid_raytracing.cu:155-162).  Rays are
- * numbered point-major (ray = point*rays_per_point + j). */
+ * numbered point-major (ray = point*rays_per_point + j).  Named
+ * qmcrt_trace_records in earlier designs of this boundary. */
 qmcrt_status qmcrt_trace_tables(qmcrt_scene* scene, const qmcrt_sun* sun,
                                 const qmcrt_table_inputs* tables, const qmcrt_trace_params* params,
                                 const qmcrt_outputs* out, qmcrt_trace_stats* stats, void* stream);
@@ -425,6 +430,33 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* scene, const qmcrt_sun* sun,
 qmcrt_status qmcrt_trace_host(qmcrt_scene* scene, const qmcrt_field* field, const qmcrt_sun* sun,
                               const qmcrt_trace_params* params, uint32_t* h_counts, float* h_flux,
                               qmcrt_trace_stats* stats, void* stream);
+
+/* Which map qmcrt_results_host smooths. */
+enum {
+  QMCRT_SMOOTH_COUNTS = 0, /* the integer count map (exact with QMCRT_TRIM_SORTED) */
+  QMCRT_SMOOTH_ENERGY = 1  /* the raw energy image, then scaled to W/m^2, as Gtest.cu:49-57 does */
+};
+
+/* Trimmed-mean smoothing of one result map (ImageSmoother::image_smooth
+ * arguments, image_smooth.cuh:20-22). */
+typedef struct qmcrt_smooth_params {
+  int32_t radius; /* window half-size, 0..7 (Gtest.cu:50 uses 5) */
+  float ratio;    /* fraction dropped at each end, [0, 0.5) (Gtest.cu:51 uses 0.02) */
+  int32_t method; /* QMCRT_TRIM_* */
+  int32_t source; /* QMCRT_SMOOTH_* */
+} qmcrt_smooth_params;
+
+/* One sun position end to end on host buffers: the work of
+ * results_with_given_normal (Gtest.cu:10-63) without its file output.
+ * Uploads the field (NULL: keep the scene's), traces, scales the flux map,
+ * smooths the map `smooth` names (NULL: no smoothing) and downloads the
+ * results: h_counts [res] counts, h_flux [res] W/m^2 (the non-smoothed
+ * result), h_smoothed [res] the smoothed map (smoothed counts, or W/m^2 for
+ * QMCRT_SMOOTH_ENERGY).  Any output pointer may be NULL.  Synchronises. */
+qmcrt_status qmcrt_results_host(qmcrt_scene* scene, const qmcrt_field* field, const qmcrt_sun* sun,
+                                const qmcrt_trace_params* params, const qmcrt_smooth_params* smooth,
+                                uint32_t* h_counts, float* h_flux, float* h_smoothed, qmcrt_trace_stats* stats,
+                                void* stream);
 
 /* ------------------------------------------------------------ batching
  * No counterpart in the reference (it launches and synchronises once per
@@ -446,7 +478,9 @@ typedef struct qmcrt_batch_tuning {
 } qmcrt_batch_tuning;
 
 /* Items must use corrected-mode traversal (no SKIP_ORIGIN_CELL / AABB_RADIUS
- * quirks) and nearest deposition; every item traces params->rays rays. */
+ * quirks) and nearest deposition; every item traces params->rays rays.
+ * qmcrt_batch_create is the qmcrt_batch_plan of earlier designs of this
+ * boundary. */
 qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, const qmcrt_batch_item* items,
                                 int32_t n_items, const qmcrt_trace_params* params, qmcrt_batch** out);
 qmcrt_status qmcrt_batch_destroy(qmcrt_batch* batch);
@@ -495,7 +529,9 @@ qmcrt_status qmcrt_tape_free(qmcrt_tape* tape);
 /* ----------------------------------------------------------- smoothing
  * Trimmed-mean smoothing over a (2r+1)^2 window clipped at the border,
  * k = int(cnt * ratio) values dropped at each end (ImageSmoother::image_smooth,
- * image_smooth.cu:60-115).  d_in and d_out must not overlap. */
+ * image_smooth.cu:60-115).  d_in and d_out must not overlap.  One entry point
+ * per map type (the single qmcrt_smooth_trimmed of earlier designs of this
+ * boundary). */
 qmcrt_status qmcrt_smooth_trimmed_u32(const uint32_t* d_in, float* d_out, int32_t width,
                                       int32_t height, int32_t radius, float ratio, int32_t method,
                                       void* stream);

@@ -27,6 +27,7 @@ DEPOSIT_NEAREST, DEPOSIT_BILINEAR = 0, 1
 ATTEN_NONE, ATTEN_POLY_EXP = 0, 1
 CAND_CAP = 32  # QMCRT_CAND_CAP: occluder candidates kept per heliostat and walk
 TRIM_SORTED, TRIM_HEAPS = 0, 1
+SMOOTH_COUNTS, SMOOTH_ENERGY = 0, 1
 RAY_SHADOWED, RAY_BLOCKED, RAY_HIT, RAY_OFFMAP = 1, 2, 4, 8
 
 fp = C.POINTER(C.c_float)
@@ -92,6 +93,10 @@ class BatchTuning(C.Structure):
     _fields_ = [("chunk_rays", C.c_int32), ("ctas_per_sm", C.c_int32), ("tile", C.c_int32), ("ms", C.c_float)]
 
 
+class SmoothParams(C.Structure):
+    _fields_ = [("radius", C.c_int32), ("ratio", C.c_float), ("method", C.c_int32), ("source", C.c_int32)]
+
+
 class Timing(C.Structure):
     _fields_ = [("setup_ms", C.c_float), ("trace_kernel_ms", C.c_float), ("finalize_ms", C.c_float)]
 
@@ -152,6 +157,8 @@ PROTOTYPES = {
                                      C.POINTER(Outputs), C.POINTER(TraceStats), C.c_void_p]),
     "qmcrt_trace_host": (C.c_int, [C.c_void_p, C.POINTER(Field), C.POINTER(Sun), C.POINTER(TraceParams), u32p, fp,
                                    C.POINTER(TraceStats), C.c_void_p]),
+    "qmcrt_results_host": (C.c_int, [C.c_void_p, C.POINTER(Field), C.POINTER(Sun), C.POINTER(TraceParams),
+                                     C.POINTER(SmoothParams), u32p, fp, fp, C.POINTER(TraceStats), C.c_void_p]),
     "qmcrt_smooth_trimmed_u32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                            C.c_int32, C.c_void_p]),
     "qmcrt_smooth_trimmed_f32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,

@@ -166,6 +166,8 @@ struct qmcrt_scene {
   // maps and statistics
   uint32_t* d_counts = nullptr;
   float* d_energy = nullptr;
+  float* d_map_flux = nullptr;    // [res] qmcrt_results_host: the flux map
+  float* d_map_smooth = nullptr;  // [res] qmcrt_results_host: the smoothed map
   unsigned long long* d_stats = nullptr;  // [16]
 
   // sunshape

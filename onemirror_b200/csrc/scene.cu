@@ -1260,6 +1260,8 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_flag, 1);
   ALLOC(s->d_counts, res);
   ALLOC(s->d_energy, res);
+  ALLOC(s->d_map_flux, res);
+  ALLOC(s->d_map_smooth, res);
   ALLOC(s->d_stats, 16);
   ALLOC(s->d_buie, 1025 + 1025 + 1024 + 1024);  // table + guide
 #undef ALLOC
@@ -1291,7 +1293,7 @@ qmcrt_status qmcrt_scene_destroy(qmcrt_scene* s) {
   dev_free(s->d_buckets); dev_free(s->d_bucket_start); dev_free(s->d_bucket_ids); dev_free(s->d_cyl_edge);
   dev_free(s->d_point_mask); dev_free(s->d_point_origin); dev_free(s->d_point_xz); dev_free(s->d_point_helio);
   dev_free(s->d_helio_weight); dev_free(s->d_flag); dev_free(s->d_counts); dev_free(s->d_energy);
-  dev_free(s->d_stats); dev_free(s->d_buie);
+  dev_free(s->d_map_flux); dev_free(s->d_map_smooth); dev_free(s->d_stats); dev_free(s->d_buie);
   for (int i = 0; i < 5; ++i)
     if (s->ev[i]) cudaEventDestroy(s->ev[i]);
   delete s;
@@ -1458,21 +1460,15 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-constexpr int kMaxDevices = 64;
-static NoAllocScratch* g_noalloc_ptr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch on the current device; looked up once per
-// device (host code cannot use the symbol itself as a device address).
+// Device address of the scratch on the current device.  Host code cannot use
+// the symbol itself as a device address, so every call asks the runtime for
+// it (cudaGetSymbolAddress, cheap next to the call's synchronisation): no
+// process-wide cache that could go stale when a context is torn down and
+// re-created (cudaDeviceReset) or race between host threads.
 static qmcrt_status noalloc_scratch(NoAllocScratch** out) {
-  int dev = 0;
-  QM_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return set_error(QMCRT_ERR_NOT_SUPPORTED, "device index above 63");
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    QM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_ptr[dev] = (NoAllocScratch*)p;
-  }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  QM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  *out = (NoAllocScratch*)p;
   return QMCRT_OK;
 }
 

@@ -263,6 +263,19 @@ static qmcrt_status apply_range(const qmcrt_trace_params* p, uint64_t total, Tra
   return QMCRT_OK;
 }
 
+// W/m^2 per unit of the raw energy map: DNI * S_sub * rho / N_c / S_rec
+// (Gtest.cu:40-46); S_sub is folded into the per-point weights of Philox
+// traces (weight_scale 1) and is point_spacing^2 for table traces.
+static double flux_scale(const qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace_params* p,
+                         double weight_scale) {
+  return (double)sun->dni * p->reflectivity * weight_scale / ((double)p->rays_per_point * s->rg.pixel_area);
+}
+
+__global__ void scale_kernel(float* m, int64_t n, float k) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m[i] *= k;
+}
+
 static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace_params* p, TraceArgs& a,
                                    bool tables, double weight_scale, const qmcrt_outputs* out,
                                    qmcrt_trace_stats* stats, cudaStream_t st) {
@@ -290,7 +303,7 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
     cull = 3;
   QM_CUDA(dispatch(a, tables, records, stats != nullptr, cull, p->kernel_variant, st));
   QM_CUDA(cudaEventRecord(s->ev[3], st));
-  double scale = (double)sun->dni * p->reflectivity * weight_scale / ((double)p->rays_per_point * s->rg.pixel_area);
+  const double scale = flux_scale(s, sun, p, weight_scale);
   FinalizeArgs f{};
   f.res = res;
   f.counts = s->d_counts;
@@ -408,6 +421,49 @@ qmcrt_status qmcrt_trace_host(qmcrt_scene* s, const qmcrt_field* field, const qm
   int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
   if (h_counts) QM_CUDA(cudaMemcpyAsync(h_counts, s->d_counts, res * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   if (h_flux) QM_CUDA(cudaMemcpyAsync(h_flux, s->d_energy, res * sizeof(float), cudaMemcpyDeviceToHost, st));
+  QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_results_host(qmcrt_scene* s, const qmcrt_field* field, const qmcrt_sun* sun,
+                                const qmcrt_trace_params* p, const qmcrt_smooth_params* sm, uint32_t* h_counts,
+                                float* h_flux, float* h_smoothed, qmcrt_trace_stats* stats, void* stream) {
+  if (!s || !sun || !p) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (sm && sm->source != QMCRT_SMOOTH_COUNTS && sm->source != QMCRT_SMOOTH_ENERGY)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown smoothing source");
+  if (!sm && h_smoothed) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "h_smoothed needs smoothing parameters");
+  cudaStream_t st = (cudaStream_t)stream;
+  qmcrt_status e;
+  if (field && (e = qmcrt_scene_set_field(s, field, stream))) return e;
+  // the trace leaves the raw counts and energy in the scene's maps and the
+  // scaled flux in d_map_flux
+  qmcrt_outputs out{};
+  out.d_flux = s->d_map_flux;
+  qmcrt_trace_params pp = *p;
+  pp.accumulate = 0;
+  // (with `stats` the trace counts its events and synchronises)
+  if ((e = qmcrt_trace(s, sun, &pp, &out, stats, stream))) return e;
+  const int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
+  if (sm) {
+    if (sm->source == QMCRT_SMOOTH_COUNTS) {
+      e = qmcrt_smooth_trimmed_u32(s->d_counts, s->d_map_smooth, s->rg.res_x, s->rg.res_y, sm->radius, sm->ratio,
+                                   sm->method, stream);
+    } else {
+      // the reference smooths its raw image, then scales it (Gtest.cu:52-57)
+      e = qmcrt_smooth_trimmed_f32(s->d_energy, s->d_map_smooth, s->rg.res_x, s->rg.res_y, sm->radius, sm->ratio,
+                                   sm->method, stream);
+      if (!e) {
+        const int blocks = (int)std::min<int64_t>((res + 255) / 256, 4 * sm_count());
+        scale_kernel<<<blocks, 256, 0, st>>>(s->d_map_smooth, res, (float)flux_scale(s, sun, p, 1.0));
+        QM_CUDA(cudaGetLastError());
+      }
+    }
+    if (e) return e;
+  }
+  if (h_counts) QM_CUDA(cudaMemcpyAsync(h_counts, s->d_counts, res * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (h_flux) QM_CUDA(cudaMemcpyAsync(h_flux, s->d_map_flux, res * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (h_smoothed)
+    QM_CUDA(cudaMemcpyAsync(h_smoothed, s->d_map_smooth, res * sizeof(float), cudaMemcpyDeviceToHost, st));
   QM_CUDA(cudaStreamSynchronize(st));
   return QMCRT_OK;
 }

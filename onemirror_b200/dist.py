@@ -5,6 +5,9 @@ field (the stream id is the trace's `item`), and the per-rank flux maps are
 summed with one all-reduce -- the only exchange the path has.  Counts are
 integers (exact in any order); energies are summed in float64 on the wire so
 the result does not depend on the reduction order beyond float64 rounding.
+The smoothing of a step (ImageSmoother::image_smooth, image_smooth.cu:60-115)
+runs on the summed count map, after the exchange: a trimmed mean of per-rank
+maps is not the trimmed mean of their sum.
 """
 import torch
 import torch.distributed as dist
@@ -20,17 +23,33 @@ def shard_item(rank, step):
 
 
 def reduce_maps(counts, energy, group=None):
-    """Sum count and energy maps over the process group, in place.
+    """Sum count and energy maps over the process group.
 
-    counts: int32/int64 tensor; energy: float32/float64 tensor.  Returns the
-    reduced tensors (energy as float64)."""
-    if not dist.is_initialized() or dist.get_world_size(group) == 1:
-        return counts, energy.double()
-    c = counts.to(torch.int64)
-    e = energy.to(torch.float64)
-    dist.all_reduce(c, group=group)
-    dist.all_reduce(e, group=group)
+    counts: integer tensor; energy: float32/float64 tensor.  Returns NEW
+    tensors holding the sums, counts as int64 and energy as float64; the
+    inputs are left as they were.  With one rank (or no process group) the
+    returned tensors are converted copies of the inputs."""
+    c = counts.to(torch.int64, copy=True)
+    e = energy.to(torch.float64, copy=True)
+    if dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(c, group=group)
+        dist.all_reduce(e, group=group)
     return c, e
+
+
+def step_maps(counts, energy, smooth, group=None):
+    """The exchange and smoothing of one step: sum the ranks' maps, then smooth
+    the summed count map with `smooth` (a function of an int32 count map).
+    Returns (summed counts int64, summed energy float64, smoothed map).  Every
+    rank runs the same collectives in the same order and gets the same maps.
+    The int64 sums go to the smoother as 32-bit words, which hold the uint32
+    count of any pixel below 2^32 rays (the conversion keeps the low 32 bits).
+    With one rank nothing is exchanged or converted: the inputs are returned
+    with the smoothing of `counts` itself."""
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return counts, energy, smooth(counts)
+    c, e = reduce_maps(counts, energy, group)
+    return c, e, smooth(c.to(torch.int32))
 
 
 def max_over_ranks(value, device=None):

@@ -214,6 +214,25 @@ class SolarScene:
         return counts, flux, st
 
 
+    def results_host(self, sun, params, radius=2, ratio=0.2, method=capi.TRIM_SORTED, source=capi.SMOOTH_COUNTS,
+                     stats=False, upload=True, out=None):
+        """One sun position end to end on host buffers (qmcrt_results_host,
+        the work of results_with_given_normal, Gtest.cu:10-63): upload the
+        field, trace, scale, smooth, download counts, flux and the smoothed
+        map.  `out` may hold preallocated (pinned) host arrays."""
+        if out is None:
+            out = {"counts": np.zeros(self.res, np.uint32), "flux": np.zeros(self.res, np.float32),
+                   "smoothed": np.zeros(self.res, np.float32)}
+        sm = capi.SmoothParams(radius, ratio, method, source)
+        st = capi.TraceStats() if stats else None
+        capi.check(capi.lib().qmcrt_results_host(self.h, C.byref(self.field()) if upload else None, C.byref(sun),
+                                                 C.byref(params), C.byref(sm), out["counts"].ctypes.data_as(capi.u32p),
+                                                 capi.as_fp(out["flux"]), capi.as_fp(out["smoothed"]),
+                                                 C.byref(st) if stats else None, _stream()))
+        out["stats"] = st
+        return out
+
+
 class Batch:
     """Many (field, sun) items traced in one persistent launch (qmcrt_batch_*)."""
 

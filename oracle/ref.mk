@@ -1,5 +1,8 @@
 # Builds oracle/_ref/libref.so: the reference's own sources compiled where
 # they lie under /root/reference (read-only), plus oracle/ref_harness.cu.
+# Also oracle/_ref/libdropin.so: the drop-in results_with_given_normal of
+# tests/dropin/ compiled against the reference's headers and linked with
+# libref.so and this repository's libqmcrt.so (when that is built).
 # Test infrastructure only; outputs go to oracle/_ref/ (git-ignored).
 #
 # Portability shims, all in _ref/shim (generated, never edited sources):
@@ -25,7 +28,11 @@ SRCS_CPP := scene_instance_process.cpp random_generator.cpp common_var.cpp helio
 OBJS := $(addprefix $(OUT)/obj/,$(SRCS_CU:.cu=.cu.o) $(SRCS_CPP:.cpp=.cpp.o))
 SHIMS := device_ptr copy host_vector device_vector
 
-all: $(OUT)/libref.so
+DROPIN := ../tests/dropin
+LIBQMCRT := ../onemirror_b200/lib/libqmcrt.so
+DROPIN_LIB := $(if $(wildcard $(LIBQMCRT)),$(OUT)/libdropin.so)
+
+all: $(OUT)/libref.so $(DROPIN_LIB)
 
 $(OUT)/shim/.done:
 	mkdir -p $(OUT)/shim $(OUT)/obj
@@ -43,6 +50,13 @@ $(OUT)/obj/ref_harness.o: ref_harness.cu $(OUT)/shim/.done
 
 $(OUT)/libref.so: $(OBJS) $(OUT)/obj/ref_harness.o
 	$(NVCC) -shared -gencode arch=compute_100a,code=sm_100a -o $@ $^ -lcurand
+
+$(OUT)/obj/dropin_%.o: $(DROPIN)/%.cu $(OUT)/shim/.done ../include/qmcrt.h
+	$(NVCC) $(FLAGS) -I../include -c $< -o $@
+
+$(OUT)/libdropin.so: $(OUT)/obj/dropin_results_with_given_normal.o $(OUT)/obj/dropin_harness.o $(OUT)/libref.so $(LIBQMCRT)
+	$(NVCC) -shared -gencode arch=compute_100a,code=sm_100a -o $@ $(filter %.o,$^) -L$(OUT) -lref \
+	    -L../onemirror_b200/lib -lqmcrt -Xlinker -rpath,'$$ORIGIN' -Xlinker -rpath,'$$ORIGIN/../../onemirror_b200/lib'
 
 clean:
 	rm -rf $(OUT)

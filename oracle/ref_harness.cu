@@ -13,6 +13,7 @@
 // map_tracing through ray_tracing (ray_tracing.cu) with caller-given tables.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -274,6 +275,98 @@ int ref_trace_tables(int n, const float* pos, const float* size, const float* no
   *ms_out = total_ms;
   if (cudaDeviceSynchronize() != cudaSuccess && rc == 0) rc = 2;
   sun.CClear();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  free_ref_scene(s);
+  return rc;
+}
+
+// The reference's own pass over one sun position, timed: per heliostat of the
+// field, as results_with_given_normal (Gtest.cu:21-35) does, regenerate the
+// sun and perturbation tables with cuRAND (SceneProcessor::set_sunray_content,
+// scene_instance_process.cu:6-11), then recthelio_ray_tracing's steps
+// (recthelio_tracing.cpp:46-80: micro-points, all vertices, groups,
+// ray_tracing = one map_tracing launch + cudaDeviceSynchronize, frees) with
+// CUDA events around ray_tracing.  `reps` passes; per pass the host-clock
+// time of the whole pass and the summed event time of its map_tracing
+// launches.  The receiver image is replaced by one with a spare row and
+// element after it, zeroed, so the one write the reference can make past its
+// image (u == 1 gives row res_y, rectgrid_raytracing.cu:144; v == 1 in the
+// last row gives index res) lands in memory this harness owns; *spill_out
+// reports whether any did.  Writes the raw image of the last pass.
+// Returns 0 on success.
+int ref_run_field(int n, const float* pos, const float* size, const float* normal, const float* gpos,
+                  const float* gsize, const float* ginter, const float* rpos, const float* rsize, const float* rnorm,
+                  int rface, int geometry_info, float helio_pixel, const float* sun_dir, float dni, float csr,
+                  float disturb_std, int groups, int lights, unsigned long long seed, int reps, float* image,
+                  int* res_out, long long* rays_out, double* pass_ms, float* trace_ms, int* spill_out) {
+  RefScene* s = make_ref_scene(n, pos, size, normal, gpos, gsize, ginter, rpos, rsize, rnorm, rface, geometry_info,
+                               helio_pixel);
+  const size_t res = (size_t)s->recv.resolution_.x * s->recv.resolution_.y;
+  const size_t pad = (size_t)s->recv.resolution_.x + 1;
+  float* padded = nullptr;
+  if (cudaMalloc(&padded, sizeof(float) * (res + pad)) != cudaSuccess) {
+    free_ref_scene(s);
+    return 4;
+  }
+  cudaMemset(padded, 0, sizeof(float) * (res + pad));
+  cudaFree(s->recv.d_image_);
+  s->recv.d_image_ = padded;
+  curandGenerator_t gen;
+  curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT);
+  curandSetPseudoRandomGeneratorSeed(gen, seed);
+  RandomGenerator::gen = &gen;
+  solarenergy::disturb_std = disturb_std;
+  SunRay sun(normalize(f3p(sun_dir)), groups, lights, dni, csr);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  long long rays = 0;
+  int rc = 0;
+  for (int r = 0; r < reps && rc == 0; ++r) {
+    float kms = 0;
+    rays = 0;
+    cudaDeviceSynchronize();
+    auto t0 = std::chrono::steady_clock::now();
+    s->recv.Cclean_image_content();
+    for (int i = 0; i < n; ++i) {
+      RectangleHelio* rh = dynamic_cast<RectangleHelio*>(s->helios[i]);
+      SceneProcessor::set_sunray_content(sun);
+      size_t m = 0;
+      float3 *d_c = nullptr, *d_n = nullptr, *d_v = nullptr;
+      int* d_g = nullptr;
+      recthelio_ray_tracing_init(*rh, s->grid, s->helios, sun.num_sunshape_groups_ * sun.num_sunshape_lights_per_group_,
+                                 m, d_c, d_n, d_v, d_g);
+      cudaEventRecord(e0);
+      ray_tracing(sun, s->grid, s->recv, d_v, d_n, d_c, d_g, (int)m);
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      kms += ms;
+      rays += (long long)m * sun.num_sunshape_lights_per_group_;
+      cudaFree(d_c);
+      cudaFree(d_n);
+      cudaFree(d_v);
+      cudaFree(d_g);
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = 2;
+    auto t1 = std::chrono::steady_clock::now();
+    pass_ms[r] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    trace_ms[r] = kms;
+  }
+  res_out[0] = s->recv.resolution_.x;
+  res_out[1] = s->recv.resolution_.y;
+  *rays_out = rays;
+  std::vector<float> tail(pad);
+  if (rc == 0 && image) cudaMemcpy(image, padded, sizeof(float) * res, cudaMemcpyDeviceToHost);
+  cudaMemcpy(tail.data(), padded + res, sizeof(float) * pad, cudaMemcpyDeviceToHost);
+  *spill_out = 0;
+  for (float v : tail) *spill_out |= v != 0.0f;
+  if (cudaDeviceSynchronize() != cudaSuccess && rc == 0) rc = 2;
+  sun.CClear();
+  curandDestroyGenerator(gen);
+  RandomGenerator::gen = nullptr;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   free_ref_scene(s);

@@ -4,6 +4,7 @@ summaries, and the algorithmic flops per ray."""
 import os
 import sys
 
+import numpy as np
 import pytest
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -40,3 +41,27 @@ def test_traffic_of_the_committed_summaries_covers_the_point_data(name, points):
 def test_flops_per_ray_of_the_reference_algorithm():
     # 1000 rays, 100 shadowed, 12 760 rectangle tests, 5 140 DDA cells
     assert bench.flops_per_ray([1000, 100, 0, 0, 0, 12760, 5140]) == pytest.approx(192 + 30 * 1.9 + 54 * 12.76 + 4 * 5.14)
+
+
+def test_both_arms_quote_the_same_config():
+    from onemirror_b200 import workloads as W
+    for name in ("small", "mid", "large"):
+        w = W.BUILDERS[name]()
+        a, b = bench.bench_config(w, 1), bench.bench_config(W.BUILDERS[name](), 1)
+        assert a == b and "Poisson sample points" in a["step"] and "smoothing" in a["step"]
+        assert "flushed" in a["l2"]
+
+
+@pytest.mark.parametrize("name", ["nine", "mid"])
+def test_reference_cuda_scenes_pass_the_range_checks(name):
+    # the CPU checks that gate every run of the reference's own CUDA pass
+    sc = bench.ref_cuda_scene(name)
+    assert bench.ref_cuda_checks(sc) is None
+    assert np.allclose(np.linalg.norm(sc["normal"], axis=1), 1.0, atol=1e-5)
+
+
+def test_reference_cuda_checks_catch_a_cube_outside_the_grid():
+    sc = dict(bench.ref_cuda_scene("nine"))
+    sc["pos"] = np.array(sc["pos"], np.float32)
+    sc["pos"][0, 0] = sc["gpos"][0] + 0.2  # registration cube reaches below the grid origin
+    assert bench.ref_cuda_checks(sc) is not None

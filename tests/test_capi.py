@@ -130,7 +130,8 @@ def test_scn_parser_reads_the_reference_format():
 
 
 def test_scn_parser_reference_sample_if_present():
-    path = "/root/reference/Hu_smooth/userData/face2face_shadow.scn"
+    path = os.path.join(os.environ.get("QMCRT_REFERENCE_ROOT", "/root/reference"), "Hu_smooth", "userData",
+                        "face2face_shadow.scn")
     if not os.path.exists(path):
         pytest.skip("reference tree not mounted")
     rv, gp, pos, size = _parse(path)

@@ -3,7 +3,9 @@
 Checked against (1) the FP64 CPU adjoint (per-ray central differences of each
 ray's deposit under fixed random numbers and visibility), and (2) central
 finite differences of the GPU loss itself under common random numbers
-(h = 1e-3 m for aims, 1e-5 rad for tilts).
+(h = 1e-3 m for aims, 1e-5 rad for tilts), on a reduced field (150
+heliostats, 2^20 rays) and on the differentiable configuration at its own
+size (2000 heliostats, 128 x 128, 2^26 rays).
 """
 import ctypes as C
 
@@ -53,59 +55,71 @@ def oracle_grad(sc, w):
                   grid_csr=sc.read_grid(), grid_bounds=(list(gi.origin), list(gi.cell), list(gi.dims)))
     xz, helio = sc.points(w.params)  # the cached points of this trace's parameters
     weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
-    cfg = ref.cfg(w.sun.csr, w.params.seed, RAYS, 256, xz, helio, weight)
+    cfg = ref.cfg(w.sun.csr, w.params.seed, int(w.params.rays), 256, xz, helio, weight)
     return ref.adjoint(cfg, w.extra["target"], scale_of(w))
+
+
+def compare_with_oracle(g, og, loss, oloss, flux, oflux):
+    """Errors of the GPU adjoint against the FP64 one: relative loss error,
+    flux error over the map maximum, per-column gradient error over the
+    column's largest gradient, and the relative error of all gradients."""
+    cols = [float(np.abs(g[:, k] - og[:, k]).max() / np.abs(og[:, k]).max()) for k in range(4)]
+    return {"loss": abs(loss - oloss) / oloss, "flux": float(np.abs(flux - oflux).max() / oflux.max()),
+            "columns": cols, "all": float(np.linalg.norm(g - og) / np.linalg.norm(og))}
 
 
 def test_forward_and_gradients_match_fp64_adjoint(case):
     w, sc, target = case
     loss, flux, g = gpu_grad(sc, w, target)
     oloss, oenergy, og = oracle_grad(sc, w)
-    oflux = oenergy * scale_of(w)
-    assert abs(loss - oloss) / oloss < 1e-4
-    assert np.abs(flux - oflux).max() <= 1e-3 * oflux.max()
+    err = compare_with_oracle(g, og, loss, oloss, flux, oenergy * scale_of(w))
+    assert err["loss"] < 1e-4 and err["flux"] <= 1e-3, err
     assert np.abs(g).max() > 0
     # per column (aim w, aim h, tilt u, tilt v): error against the largest
     # gradient of that kind; a ray whose visibility differs between the FP32
     # traversal and the FP64 oracle (edge cases, <= 0.01 %) moves one
     # heliostat's gradient by up to ~0.5 % of that maximum
-    for k in range(4):
-        err = np.abs(g[:, k] - og[:, k])
-        assert err.max() <= 1e-2 * np.abs(og[:, k]).max(), (k, err.max() / np.abs(og[:, k]).max())
-    rel = np.linalg.norm(g - og) / np.linalg.norm(og)
-    assert rel < 5e-3, rel
+    assert max(err["columns"]) <= 1e-2, err
+    assert err["all"] < 5e-3, err
+
+
+# receiver axes of the flat receiver facing -z: width (v3 - v0) and height (v1 - v0)
+EW = np.array([-1.0, 0.0, 0.0])
+EH = np.array([0.0, 1.0, 0.0])
+
+
+def central_differences(sc, w, target, pairs):
+    """Central differences of the GPU loss for (heliostat, parameter) pairs
+    under common random numbers: h = 1e-3 m for aims, 1e-5 rad for tilts."""
+    base_aim, base_tilt = sc.aim.copy(), sc.tilt.copy()
+    out = []
+    for h, k in pairs:
+        step = 1e-3 if k < 2 else 1e-5
+        vals = []
+        for sgn in (1.0, -1.0):
+            sc.aim[:] = base_aim
+            sc.tilt[:] = base_tilt
+            if k < 2:
+                sc.aim[h] += (sgn * step * (EW if k == 0 else EH)).astype(np.float32)
+            else:
+                sc.tilt[h, k - 2] += np.float32(sgn * step)
+            sc.update_field()
+            tape, l, _ = sc.adjoint_forward(w.sun, w.params, target, flux=False)
+            SolarScene.tape_free(tape)
+            vals.append(l)
+        out.append((vals[0] - vals[1]) / (2 * step))
+    sc.aim[:] = base_aim
+    sc.tilt[:] = base_tilt
+    sc.update_field()
+    return np.array(out)
 
 
 def test_gradients_match_central_differences_of_the_gpu_loss(case):
     w, sc, target = case
     loss, _, g = gpu_grad(sc, w, target)
-    rv = np.array([[-6.0, 144.0, 0.0], [-6.0, 156.0, 0.0], [6.0, 156.0, 0.0], [6.0, 144.0, 0.0]])
-    ew = np.array([-1.0, 0.0, 0.0])  # receiver width axis (v3 - v0) of the flat receiver facing -z
-    eh = np.array([0.0, 1.0, 0.0])   # receiver height axis (v1 - v0)
-    del rv
-    base_aim, base_tilt = sc.aim.copy(), sc.tilt.copy()
-    rel = []
-    for k in range(4):
-        hs = [int(i) for i in np.argsort(-np.abs(g[:, k]))[:3]]
-        for h in hs:
-            step = 1e-3 if k < 2 else 1e-5
-            vals = []
-            for sgn in (1.0, -1.0):
-                sc.aim[:] = base_aim
-                sc.tilt[:] = base_tilt
-                if k < 2:
-                    sc.aim[h] += (sgn * step * (ew if k == 0 else eh)).astype(np.float32)
-                else:
-                    sc.tilt[h, k - 2] += np.float32(sgn * step)
-                sc.update_field()
-                tape, l, _ = sc.adjoint_forward(w.sun, w.params, target, flux=False)
-                SolarScene.tape_free(tape)
-                vals.append(l)
-            fd = (vals[0] - vals[1]) / (2 * step)
-            rel.append(abs(fd - g[h, k]) / abs(g[h, k]))
-    sc.aim[:] = base_aim
-    sc.tilt[:] = base_tilt
-    sc.update_field()
+    pairs = [(int(h), k) for k in range(4) for h in np.argsort(-np.abs(g[:, k]))[:3]]
+    fd = central_differences(sc, w, target, pairs)
+    rel = [abs(f - g[h, k]) / abs(g[h, k]) for f, (h, k) in zip(fd, pairs)]
     # the loss differences also count rays whose visibility flips under the
     # step (a shadow or block edge crossing a sample), which the pathwise
     # gradient leaves out by design; each flip here is worth ~1e13
@@ -157,3 +171,48 @@ def test_reused_tape_gives_the_same_gradients(case):
         sc2.adjoint_forward(other.sun, other.params, t2, tape=tape)
     SolarScene.tape_free(tape)
     sc2.close()
+
+
+# ---------------------------------------- the differentiable configuration
+@pytest.fixture(scope="module")
+def full_case():
+    w = W.differentiable()  # 2000 heliostats, 128 x 128, 2^26 rays
+    sc = SolarScene(w.pos, w.size, w.receiver, w.grid, sigma=w.sigma, aim=w.aim.copy(), tilt=w.extra["tilt"].copy())
+    target = torch.as_tensor(w.extra["target"], device="cuda")
+    loss, flux, g = gpu_grad(sc, w, target)
+    yield w, sc, target, loss, flux, g
+    sc.close()
+
+
+def test_full_size_gradients_match_fp64_adjoint(full_case):
+    """All 8000 gradients, the loss and the flux map of the 2^26-ray
+    configuration against the FP64 adjoint of the same rays."""
+    w, sc, target, loss, flux, g = full_case
+    assert g.shape == (2000, 4) and w.params.rays == 1 << 26
+    oloss, oenergy, og = oracle_grad(sc, w)
+    err = compare_with_oracle(g, og, loss, oloss, flux, oenergy * scale_of(w))
+    print("config D against the FP64 adjoint:", err)
+    assert err["loss"] < 1e-4 and err["flux"] <= 1e-3, err
+    assert max(err["columns"]) <= 1e-2, err
+    assert err["all"] < 5e-3, err
+
+
+def test_full_size_gradients_match_central_differences(full_case):
+    """Central differences of the 2^26-ray loss on the 4 largest gradients of
+    each kind and on 4 heliostats drawn at random per kind.  Bars: the
+    largest gradients within 5 % (median) and 15 % (each); every pair within
+    2 % of its column's largest gradient, which bounds the error of the small
+    ones, where the visibility flips that the loss difference sees and the
+    pathwise gradient leaves out dominate."""
+    w, sc, target, loss, flux, g = full_case
+    rng = np.random.default_rng(5)
+    top = [(int(h), k) for k in range(4) for h in np.argsort(-np.abs(g[:, k]))[:4]]
+    rand = [(int(h), k) for k in range(4) for h in rng.choice(w.n, 4, replace=False)]
+    fd = central_differences(sc, w, target, top + rand)
+    colmax = np.abs(g).max(0)
+    rel_top = np.array([abs(f - g[h, k]) / abs(g[h, k]) for f, (h, k) in zip(fd[:16], top)])
+    abs_all = np.array([abs(f - g[h, k]) / colmax[k] for f, (h, k) in zip(fd, top + rand)])
+    print("config D central differences: top relative", np.round(rel_top, 4), "all / column max",
+          np.round(abs_all, 5))
+    assert np.median(rel_top) < 0.05 and rel_top.max() < 0.15, rel_top
+    assert abs_all.max() < 0.02, abs_all

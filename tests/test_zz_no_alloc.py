@@ -78,13 +78,20 @@ def test_limits_and_errors_are_reported():
                                        C.c_void_p(out.data_ptr()), C.c_void_p(h.data_ptr()), None)
     assert st == capi.ERR_INVALID_ARGUMENT
     # points that cannot fit report a sampling error and leave the entry point usable
+    bad_xz = torch.full((8000, 2), float("nan"), dtype=torch.float32, device="cuda")
+    bad_h = torch.full((8000,), -7, dtype=torch.int32, device="cuda")
     st = L.qmcrt_sample_points_noalloc(capi.as_fp(size), 4, 4 * 2000, C.c_float(0.3), 1,
-                                       C.c_void_p(torch.zeros((8000, 2), device="cuda").data_ptr()),
-                                       C.c_void_p(torch.zeros(8000, dtype=torch.int32, device="cuda").data_ptr()), None)
+                                       C.c_void_p(bad_xz.data_ptr()), C.c_void_p(bad_h.data_ptr()), None)
     assert st == capi.ERR_SAMPLING
     got_xz, got_h = noalloc_points(size, 8, 0.3, 5)
     ref_xz, ref_h = scene_points(size, 8, 0.3, 5)
     assert got_xz.tobytes() == ref_xz.tobytes() and np.array_equal(got_h, ref_h)
+    # a successful call into the same (partly written) outputs overwrites all of them
+    st = L.qmcrt_sample_points_noalloc(capi.as_fp(size), 4, 8, C.c_float(0.3), 5, C.c_void_p(bad_xz.data_ptr()),
+                                       C.c_void_p(bad_h.data_ptr()), None)
+    capi.check(st)
+    assert bad_xz[:8].cpu().numpy().tobytes() == ref_xz.tobytes()
+    assert np.array_equal(bad_h[:8].cpu().numpy(), ref_h)
     with pytest.raises(too_many):
         capi.check(L.qmcrt_sample_points_noalloc(None, 4, 8, C.c_float(0.3), 1, C.c_void_p(out.data_ptr()),
                                                  C.c_void_p(h.data_ptr()), None))
