@@ -3,6 +3,9 @@
 //
 // Each CTA stages its 32x8 output tile plus a halo of `radius` into shared
 // memory with coalesced loads, then each thread forms its clipped window.
+// Exact order statistics for radii 1-3 sort the window in registers with a
+// sorting network (smooth_sorted_kernel); larger radii insertion-sort into a
+// per-thread array.
 // Two definitions:
 //  - QMCRT_TRIM_SORTED: exact order statistics.  On integer counts the kept
 //    sum is an exact 64-bit integer and the mean is one IEEE division, so the
@@ -60,6 +63,96 @@ struct RefHeap {
     return s;
   }
 };
+
+// Exact order statistics for a small radius R, all in registers: the
+// (2R+1)^2 window values (positions outside the map hold the type's largest
+// value, so they sort after every real one) go through Batcher's odd-even
+// merge sort network, fully unrolled so every index is a compile-time
+// constant; the kept sum then runs over the sorted positions [k, cnt - k) in
+// ascending order, the order the general path's insertion sort gives.
+template <typename T>
+__device__ __forceinline__ void cmp_swap(T& a, T& b) {
+  const T lo = a < b ? a : b, hi = a < b ? b : a;
+  a = lo;
+  b = hi;
+}
+
+// The comparators of Batcher's odd-even merge sort for N keys, listed at
+// compile time.
+struct SortNet {
+  int n;
+  short a[640], b[640];
+};
+
+template <int N>
+constexpr SortNet batcher_net() {
+  SortNet net{};
+  int c = 0;
+  for (int p = 1; p < N; p <<= 1)
+    for (int k = p; k >= 1; k >>= 1)
+      for (int j = k % p; j + k < N; j += 2 * k)
+        for (int i = 0; i < k; ++i)
+          if (i + j + k < N && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
+            net.a[c] = (short)(i + j);
+            net.b[c] = (short)(i + j + k);
+            ++c;
+          }
+  net.n = c;
+  return net;
+}
+
+template <int N, typename T>
+__device__ __forceinline__ void batcher_sort(T (&v)[N]) {
+  constexpr SortNet net = batcher_net<N>();
+  static_assert(net.n <= 640, "sorting network larger than its table");
+#pragma unroll
+  for (int c = 0; c < net.n; ++c) cmp_swap(v[net.a[c]], v[net.b[c]]);
+}
+
+template <typename T>
+__device__ __forceinline__ T sort_pad() {
+  if constexpr (std::is_integral<T>::value) return (T)0xFFFFFFFFu;
+  else return __int_as_float(0x7f800000);  // +inf
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(kTileX* kTileY) smooth_sorted_kernel(const T* __restrict__ in,
+                                                                       float* __restrict__ out, int w, int h,
+                                                                       float ratio) {
+  constexpr int W = 2 * R + 1, N = W * W, TW = kTileX + 2 * R, TH = kTileY + 2 * R;
+  __shared__ T tile[TW * TH];
+  const int x0 = blockIdx.x * kTileX - R, y0 = blockIdx.y * kTileY - R;
+  const int tid = threadIdx.y * kTileX + threadIdx.x;
+  for (int i = tid; i < TW * TH; i += kTileX * kTileY) {
+    const int yy = y0 + i / TW, xx = x0 + i % TW;
+    tile[i] = (xx >= 0 && xx < w && yy >= 0 && yy < h) ? in[(int64_t)yy * w + xx] : sort_pad<T>();
+  }
+  __syncthreads();
+  const int x = blockIdx.x * kTileX + threadIdx.x, y = blockIdx.y * kTileY + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const int lx = max(x - R, 0), ly = max(y - R, 0), rx = min(x + R, w - 1), ry = min(y + R, h - 1);
+  const int cnt = (rx - lx + 1) * (ry - ly + 1);
+  const int k = (int)((float)cnt * ratio);  // image_smooth.cu:34
+  T v[N];
+#pragma unroll
+  for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+    for (int dx = 0; dx < W; ++dx) v[dy * W + dx] = tile[(threadIdx.y + dy) * TW + threadIdx.x + dx];
+  batcher_sort<N>(v);
+  const int lo = k, hi = cnt - k;
+  if constexpr (std::is_integral<T>::value) {  // integer counts: exact sum
+    unsigned long long s = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) s += (i >= lo && i < hi) ? (unsigned long long)v[i] : 0ull;
+    out[(int64_t)y * w + x] = __fdiv_rn(__ull2float_rn(s), (float)(cnt - 2 * k));
+  } else {
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      if (i >= lo && i < hi) s = __fadd_rn(s, as_float(v[i]));
+    out[(int64_t)y * w + x] = __fdiv_rn(s, (float)(cnt - 2 * k));
+  }
+}
 
 template <typename T, int METHOD>
 __global__ void __launch_bounds__(kTileX* kTileY) smooth_kernel(const T* __restrict__ in, float* __restrict__ out,
@@ -138,7 +231,10 @@ static qmcrt_status smooth(const T* d_in, float* d_out, int w, int h, int r, flo
   if (a0 < b1 && b0 < a1) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "input and output maps overlap");
   dim3 block(kTileX, kTileY), grid((w + kTileX - 1) / kTileX, (h + kTileY - 1) / kTileY);
   size_t smem = (size_t)(kTileX + 2 * r) * (kTileY + 2 * r) * sizeof(T);
-  if (method == QMCRT_TRIM_SORTED) smooth_kernel<T, QMCRT_TRIM_SORTED><<<grid, block, smem, st>>>(d_in, d_out, w, h, r, ratio);
+  if (method == QMCRT_TRIM_SORTED && r == 1) smooth_sorted_kernel<T, 1><<<grid, block, 0, st>>>(d_in, d_out, w, h, ratio);
+  else if (method == QMCRT_TRIM_SORTED && r == 2) smooth_sorted_kernel<T, 2><<<grid, block, 0, st>>>(d_in, d_out, w, h, ratio);
+  else if (method == QMCRT_TRIM_SORTED && r == 3) smooth_sorted_kernel<T, 3><<<grid, block, 0, st>>>(d_in, d_out, w, h, ratio);
+  else if (method == QMCRT_TRIM_SORTED) smooth_kernel<T, QMCRT_TRIM_SORTED><<<grid, block, smem, st>>>(d_in, d_out, w, h, r, ratio);
   else if (method == QMCRT_TRIM_HEAPS) smooth_kernel<T, QMCRT_TRIM_HEAPS><<<grid, block, smem, st>>>(d_in, d_out, w, h, r, ratio);
   else return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown trimmed-mean method");
   QM_CUDA(cudaGetLastError());

@@ -501,10 +501,16 @@ def test_grid_fine_div_must_be_a_power_of_two():
 
 def test_smoothing_u32_sorted_bit_exact():
     rng = np.random.default_rng(4)
+    # radii 1-3 take the register sorting network, the others the general path;
+    # maps narrower than the window, and counts up to the uint32 maximum (the
+    # network pads clipped windows with that value)
     for (h, w_), r, ratio in [((128, 128), 2, 0.2), ((67, 201), 3, 0.1), ((1, 1), 2, 0.2), ((5, 300), 7, 0.45),
-                              ((64, 64), 0, 0.2), ((40, 33), 2, 0.0)]:
+                              ((64, 64), 0, 0.2), ((40, 33), 2, 0.0), ((50, 77), 1, 0.3), ((3, 2), 3, 0.2),
+                              ((256, 256), 1, 0.0), ((9, 40), 2, 0.49), ((33, 31), 3, 0.45), ((20, 20), 4, 0.2)]:
         img = rng.integers(0, 5000, (h, w_)).astype(np.uint32)
         img[rng.random(img.shape) < 0.3] = 0
+        img[rng.random(img.shape) < 0.05] = 0xFFFFFFFF
+        img[rng.random(img.shape) < 0.05] = 0xFFFFFFF0
         d = torch.as_tensor(img.view(np.int32), device="cuda")
         out = image_smooth(d, r, ratio, capi.TRIM_SORTED).cpu().numpy()
         ref = O.smooth_u32(img, r, ratio, 0)
@@ -521,9 +527,11 @@ def test_smoothing_heaps_bit_exact_float_and_counts():
     imgu = rng.integers(0, 1000, (50, 70)).astype(np.uint32)
     out = image_smooth(torch.as_tensor(imgu.view(np.int32), device="cuda"), 2, 0.2, capi.TRIM_HEAPS).cpu().numpy()
     assert out.tobytes() == O.smooth_u32(imgu, 2, 0.2, 1).tobytes()
-    # float maps, sorted definition: FP32 sums against the FP64 oracle
-    out = image_smooth(torch.as_tensor(imgf, device="cuda"), 2, 0.2, capi.TRIM_SORTED).cpu().numpy()
-    assert np.allclose(out, O.smooth_f32(imgf, 2, 0.2, 0), rtol=1e-5, atol=1e-5)
+    # float maps, sorted definition: FP32 sums against the FP64 oracle (radii
+    # 1-3 on the register sorting network, 5 on the general path)
+    for r in (1, 2, 3, 5):
+        out = image_smooth(torch.as_tensor(imgf, device="cuda"), r, 0.2, capi.TRIM_SORTED).cpu().numpy()
+        assert np.allclose(out, O.smooth_f32(imgf, r, 0.2, 0), rtol=1e-5, atol=1e-5), r
 
 
 def test_smoothing_of_traced_counts_bit_exact(small):
