@@ -177,10 +177,15 @@ __device__ __forceinline__ Refl reflect_ray(const RaySetup& R) {
   return g;
 }
 
-// Visibility and hit geometry of one ray (shadow, reflection, block, receiver).
+// Visibility and hit geometry of one ray (reflection, shadow, block,
+// receiver).  The reflection comes first, as in the plain tracer, so the
+// mirror frame is dead before the walks; the ray's energy |s . n'| w (the
+// only use of the normal in the forward pass) is formed there too.
 template <bool CULL, bool LENGTHS = true>
 __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, float fy0, float fy1, Refl* g,
-                                         double* u, double* v, double* t) {
+                                         double* u, double* v, double* t, float* e = nullptr) {
+  *g = reflect_ray<LENGTHS>(R);
+  if (e) *e = (float)fabs(g->np.x * a.sdir[0] + g->np.y * a.sdir[1] + g->np.z * a.sdir[2]) * R.w;
   // with CULL (corrected mode) the heliostat's occluder candidates answer the
   // visibility questions (the grid walk where there are none)
   uint32_t nt = 0, nc = 0;
@@ -189,7 +194,6 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
   if (CULL ? list_blocked<false>(a, R.h, 0, of, sd, fy0, fy1, nt, nc, R.reach.x)
            : dda_blocked<false, false>(a, of, sd, R.h, fy0, fy1, nt, nc))
     return false;
-  *g = reflect_ray<LENGTHS>(R);
   if (CULL ? list_blocked<false>(a, R.h, 1, of, to_f(g->rd), fy0, fy1, nt, nc, R.reach.y)
            : dda_blocked<false, false>(a, of, to_f(g->rd), R.h, fy0, fy1, nt, nc))
     return false;
@@ -219,10 +223,10 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
     ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
     Refl g;
     double u, v, t;
-    const bool hit = ray_hits<CULL, false>(a, R, fy0, fy1, &g, &u, &v, &t);
+    float e;
+    const bool hit = ray_hits<CULL, false>(a, R, fy0, fy1, &g, &u, &v, &t, &e);
     if (r64 < A.saved) A.tape[r64] = hit ? 1 : 0;
     if (!hit) continue;
-    float e = (float)fabs(g.np.x * a.sdir[0] + g.np.y * a.sdir[1] + g.np.z * a.sdir[2]) * R.w;
     float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
     int i0 = (int)floorf(px), j0 = (int)floorf(py);
     float fx = px - (float)i0, fy = py - (float)j0;
@@ -236,6 +240,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
       atomicAdd(q + T + 1, e * wgt[3]);
       continue;
     }
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
       int ci = i0 + (k & 1), cj = j0 + (k >> 1);
       if (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) continue;

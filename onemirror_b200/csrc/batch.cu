@@ -206,8 +206,9 @@ struct qmcrt_batch {
     uint32_t* d_counts = nullptr;
     float* d_energy = nullptr;
     float* d_flux = nullptr;
-    uint2* d_mask = nullptr;  // per-point candidate masks for this item's sun
+    uint4* d_mask = nullptr;  // per-point candidate masks (and sigma, weight) for this item's sun
     double4* d_origin = nullptr;  // the points in world coordinates for this item's sun
+    const float* weight = nullptr;  // [n] mirror area per point of the item's scene
     const float2* pts = nullptr;
     const int32_t* pts_helio = nullptr;
     int64_t points = 0;
@@ -289,7 +290,7 @@ static qmcrt_status enqueue_pass(qmcrt_batch* b, cudaStream_t st) {
     auto& it = b->items[i];
     cudaStream_t s = b->side[i % K];
     if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, s))) return e;
-    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.points, it.d_mask, it.d_origin, s)))
+    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.weight, it.points, it.d_mask, it.d_origin, s)))
       return e;
     QM_CUDA(cudaMemsetAsync(it.d_counts, 0, it.res * sizeof(uint32_t), s));
     QM_CUDA(cudaMemsetAsync(it.d_energy, 0, it.res * sizeof(float), s));
@@ -405,10 +406,12 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     a.point_helio = b->pts_helio[items[i].scene];
     it.pts = a.point_xz;
     it.pts_helio = a.point_helio;
+    it.weight = b->weights[items[i].scene];
     it.points = scenes[items[i].scene]->points;
     if ((e = balloc(&it.d_mask, it.points)) || (e = balloc(&it.d_origin, it.points))) goto fail;
-    // every candidate until a pass builds the masks for the item's sun
-    if (cudaMemset(it.d_mask, 0xFF, it.points * sizeof(uint2)) != cudaSuccess) {
+    // all bits set until a pass builds the masks, sigmas and weights for the
+    // item's sun (every pass builds them before it traces)
+    if (cudaMemset(it.d_mask, 0xFF, it.points * sizeof(uint4)) != cudaSuccess) {
       e = set_error(QMCRT_ERR_CUDA, "batch mask initialisation");
       goto fail;
     }
@@ -491,7 +494,7 @@ qmcrt_status qmcrt_batch_autotune(qmcrt_batch* b, qmcrt_batch_tuning* chosen, vo
   for (int i = 0; i < n; ++i) {
     auto& it = b->items[i];
     if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, st))) return e;
-    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.points, it.d_mask, it.d_origin, st)))
+    if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.weight, it.points, it.d_mask, it.d_origin, st)))
       return e;
   }
   cudaEvent_t e0, e1;

@@ -123,11 +123,12 @@ __device__ __forceinline__ uint4 philox4x32_10_rk(uint4 c, const uint2* rk) {
 // Uniform in (0,1) from the top 24 bits: exact in float and double.
 QMCRT_HD float u24f(uint32_t w) { return ((float)(w >> 8) + 0.5f) * (1.0f / 16777216.0f); }
 
-// The ray sampler's uniform in (0,1): (k + 0.5) 2^-23 with k the top 23 bits
-// of w, built from the bits (1 + k 2^-23 as a float, minus 1, plus 2^-24; each
-// step exact) so that no integer-to-float conversion occupies the XU pipe.
+// The ray sampler's uniform in (0,1): (k + 0.5) 2^-23 with k the low 23 bits
+// of w, built from the bits: 1 + k 2^-23 as a float (one AND-OR of w), minus
+// (1 - 2^-24), a float whose difference with it is exactly (k + 0.5) 2^-23, so
+// one subtraction and no integer-to-float conversion on the XU pipe.
 __device__ __forceinline__ float u23f(uint32_t w) {
-  return (__uint_as_float(0x3F800000u | (w >> 9)) - 1.0f) + 5.9604645e-8f;
+  return __uint_as_float(0x3F800000u | (w & 0x7FFFFFu)) - 0x1.fffffep-1f;  // 1 - 2^-24
 }
 
 // Occluder candidates kept per heliostat and walk direction.

@@ -156,7 +156,7 @@ struct qmcrt_scene {
   uint64_t geom_version = 0, points_version = 0, mask_geom = ~0ull, mask_points = ~0ull;
   double sun_unit[3] = {0, 0, 0};   // the normalised sun direction of the current geometry
   int64_t mask_cap = 0;
-  uint2* d_point_mask = nullptr;     // [points] (shadow, block) candidate bits
+  uint4* d_point_mask = nullptr;     // [points] (shadow, block) candidate bits, slope sigma, area weight
   double4* d_point_origin = nullptr; // [points] the points in world coordinates for the current sun
   float2* d_point_xz = nullptr;
   int32_t* d_point_helio = nullptr;
@@ -194,7 +194,7 @@ qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStre
 // scene s and the (normalised) sun, into mask, and the points' world
 // coordinates (the rays' origins) into origin.
 qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
-                                const int32_t* helio, int64_t points, uint2* mask, double4* origin,
+                                const int32_t* helio, const float* weight, int64_t points, uint4* mask, double4* origin,
                                 cudaStream_t st);
 // The scene's masks for its current sun and points (rebuilt when stale).
 qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st);

@@ -507,9 +507,10 @@ struct MaskArgs {
   const float4* cand;
   const int* cand_n;
   const float* sigma;
+  const float* weight;  // [n] mirror area per point (NULL: 1)
   double sun[3];
   double shadow_tan, sun_alpha, zmax;
-  uint2* mask;      // [points] (shadow bits, block bits)
+  uint4* mask;      // [points] shadow bits, block bits, slope sigma and area weight of the point's heliostat
   double4* origin;  // [points] the point in world coordinates (the rays' origin); w: float x, y
 };
 
@@ -591,7 +592,8 @@ __global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
     for (int j = 0; j < m; ++j)
       if (point_reaches(p, L + 3 * j, d, e1, e2, ta)) bits[w] |= 1u << j;
   }
-  a.mask[g] = make_uint2(bits[0], bits[1]);
+  // the rays also take their heliostat's slope error and area weight from here
+  a.mask[g] = make_uint4(bits[0], bits[1], __float_as_uint(a.sigma[h]), __float_as_uint(a.weight ? a.weight[h] : 1.f));
 }
 
 // ------------------------------------------------------------ points
@@ -848,8 +850,8 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
 }
 
 qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
-                                const int32_t* helio, int64_t points, uint2* mask, double4* origin,
-                                cudaStream_t st) {
+                                const int32_t* helio, const float* weight, int64_t points, uint4* mask,
+                                double4* origin, cudaStream_t st) {
   if (points <= 0) return QMCRT_OK;
   MaskArgs m{};
   m.points = points;
@@ -859,6 +861,7 @@ qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const do
   m.cand = g.cand;
   m.cand_n = g.cand_n;
   m.sigma = s->d_sigma;
+  m.weight = weight;
   for (int i = 0; i < 3; ++i) m.sun[i] = sun[i];
   m.shadow_tan = std::tan(kSunAlphaMax + 1e-6);
   m.sun_alpha = kSunAlphaMax;
@@ -881,8 +884,8 @@ qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st) {
     if (e) return e;
     s->mask_cap = s->points;
   }
-  qmcrt_status e = launch_point_masks(s, scene_geom(s), s->sun_unit, s->d_point_xz, s->d_point_helio, s->points,
-                                      s->d_point_mask, s->d_point_origin, st);
+  qmcrt_status e = launch_point_masks(s, scene_geom(s), s->sun_unit, s->d_point_xz, s->d_point_helio,
+                                      s->d_helio_weight, s->points, s->d_point_mask, s->d_point_origin, st);
   if (e) return e;
   s->mask_geom = s->geom_version;
   s->mask_points = s->points_version;

@@ -33,7 +33,10 @@ struct TraceArgs {
   // (> kCandCap: the list overflowed); NULL: walk the grid
   const float4* cand;   // [n][2][kCandCap][3]
   const int* cand_n;    // [n][2]
-  const uint2* point_mask;  // [points] candidates reachable from each point (shadow, block bits); NULL: all
+  // [points] candidates reachable from each point (shadow, block bits), and
+  // the slope sigma and area weight of its heliostat (float bits); NULL: all
+  // candidates, sigma and weight read per heliostat
+  const uint4* point_mask;
   // [points] world coordinates of each point, w holding their float x and y
   // (Philox traces; table mode computes them)
   const double4* point_origin;
@@ -121,17 +124,19 @@ __device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float
   return __powf((uu - a.b_core) * a.b_B + a.b_C, a.b_inv);
 }
 
-// sin and cos of a small angle by their Taylor series (exact to float
-// rounding for |x| < 0.05: the first omitted terms are below 2e-11 relative);
-// sincosf otherwise.
+// sin and cos of a small angle by their Taylor series in Horner form,
+// x + x^3 (-1/6 + x^2/120) and 1 + x^2 (-1/2 + x^2/24): exact to float
+// rounding for |x| < 0.05 (the first omitted terms are below 2e-11 relative).
+// A Buie sample is at most 9.3 mrad (the aureole's end), so the sun sample
+// always takes this form; sincos_small falls back to sincosf above 0.05.
+__device__ __forceinline__ void sincos_taylor(float x, float* s, float* c) {
+  const float x2 = x * x;
+  *s = fmaf(x * x2, fmaf(x2, 1.f / 120.f, -1.f / 6.f), x);
+  *c = fmaf(x2, fmaf(x2, 1.f / 24.f, -0.5f), 1.f);
+}
 __device__ __forceinline__ void sincos_small(float x, float* s, float* c) {
-  if (fabsf(x) < 0.05f) {
-    float x2 = x * x;
-    *s = x * (1.f - x2 * (1.f / 6.f) * (1.f - x2 * (1.f / 20.f)));
-    *c = 1.f - x2 * 0.5f * (1.f - x2 * (1.f / 12.f));
-  } else {
-    sincosf(x, s, c);
-  }
+  if (fabsf(x) < 0.05f) sincos_taylor(x, s, c);
+  else sincosf(x, s, c);
 }
 
 // Does the ray o + t d hit the parallelogram A, E1, E2 at t > eps?  The test
@@ -297,13 +302,21 @@ __device__ bool dda_blocked(const TraceArgs& a, float3 o, float3 d, int own, flo
 // overflowed, or no lists (cand_n NULL), falls back to the grid walk.
 // reach: the candidates the ray's point can reach (bit j: list entry j), from
 // the per-point masks; every bit set when there are none.
+// A point mask is either all ones (no masks, a list that overflowed, or
+// every candidate reachable) or holds only bits below the list's count, as the
+// mask pass writes them; so a mask of 0 needs no list at all and only an
+// all-ones mask needs the list's count.
 template <bool STATS>
 __device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int which, float3 o, float3 d, float fy0,
                                              float fy1, uint32_t& ntest, uint32_t& ncell, uint32_t reach) {
-  const int m = a.cand_n ? __ldg(a.cand_n + 2 * h + which) : kCandCap + 1;  // no lists: walk
-  if (m > kCandCap) return dda_blocked<STATS, true>(a, o, d, h, fy0, fy1, ntest, ncell);
+  if (reach == 0u) return false;
+  uint32_t bits = reach;
+  if (reach == 0xffffffffu) {
+    const int m = a.cand_n ? __ldg(a.cand_n + 2 * h + which) : kCandCap + 1;  // no lists: walk
+    if (m > kCandCap) return dda_blocked<STATS, true>(a, o, d, h, fy0, fy1, ntest, ncell);
+    bits = m == 32 ? 0xffffffffu : (1u << m) - 1u;
+  }
   const float4* L = a.cand + (size_t)(2 * h + which) * (kCandCap * 3);
-  uint32_t bits = reach & (m == 32 ? 0xffffffffu : (1u << m) - 1u);
   while (bits) {  // the same bits on every lane of a warp (one point)
     const int i = __ffs(bits) - 1;
     bits &= bits - 1u;
@@ -443,12 +456,17 @@ __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4*
   // (__sincosf, __logf: absolute errors near 2^-21): they scale milliradian
   // polar angles, so a direction moves by ~1e-9 rad, far below FP32 rounding
   // of the geometry that follows.
-  sincos_small(th, &st, &ct);  // th <= 9.3 mrad
+  sincos_taylor(th, &st, &ct);  // th <= 9.3 mrad
   __sincosf(6.28318531f * u23f(r.y), &sp, &cp);
   *sl = f3(st * cp, ct, st * sp);  // angle2xyz (global_function.cuh:175-180)
-  float z = sqrtf(-2.f * __logf(u23f(r.z))) * __cosf(6.28318531f * u23f(r.w));
+  // the Box-Muller radius with the hardware square root (relative error
+  // ~2^-22, a slope angle moves by ~1e-9 rad)
+  float rad;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(rad) : "f"(-2.f * __logf(u23f(r.z))));
+  float z = rad * __cosf(6.28318531f * u23f(r.w));
   float ths = sigma * z;
-  uint32_t extra = (r.x & 0xFFu) | ((r.y & 0xFFu) << 8) | ((r.z & 0xFFu) << 16) | ((r.w & 0xFFu) << 24);
+  // the slope azimuth from the words' top bytes (the uniforms above use bits 0-22)
+  uint32_t extra = __byte_perm(__byte_perm(r.x, r.y, 0x0073u), __byte_perm(r.z, r.w, 0x0073u), 0x5410u);
   sincos_small(ths, &st, &ct);
   __sincosf(6.28318531f * u23f(extra), &sp, &cp);
   *tl = f3(st * cp, ct, st * sp);
@@ -464,7 +482,19 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
   if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
   R.h = h;
   R.xz = __ldg(a.point_xz + g);
-  R.reach = a.point_mask ? __ldg(a.point_mask + g) : make_uint2(0xffffffffu, 0xffffffffu);
+  float sigma_h = 0.f;
+  if (a.point_mask) {
+    const uint4 pm = __ldg(a.point_mask + g);
+    R.reach = make_uint2(pm.x, pm.y);
+    sigma_h = __uint_as_float(pm.z);
+    R.w = __uint_as_float(pm.w);
+  } else {
+    R.reach = make_uint2(0xffffffffu, 0xffffffffu);
+    if (!TABLES) {
+      sigma_h = __ldg(a.sigma + h);
+      R.w = a.weight ? __ldg(a.weight + h) : 1.f;
+    }
+  }
   // the frame axes (16-byte aligned record) as 16-byte loads
   const double2* F = reinterpret_cast<const double2*>(a.frame + kFrameStride * h);
   const double2 q0 = __ldg(F), q1 = __ldg(F + 1), q2 = __ldg(F + 2), q3 = __ldg(F + 3), q4 = __ldg(F + 4);
@@ -481,8 +511,8 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
     R.o = mk(oa.x, oa.y, ob.x);
     R.of = f3(__int_as_float(__double2loint(ob.y)), __int_as_float(__double2hiint(ob.y)), (float)ob.x);
   }
-  R.w = 1.f;
   if (TABLES) {
+    R.w = 1.f;
     // (start + j) mod T, kept in [0, T) for any caller-provided start
     int64_t ia = (((int64_t)__ldg(a.start + g) + j) % a.T + a.T) % a.T;
     // the reference's index restarts at each heliostat's launch
@@ -491,8 +521,7 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
     R.sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
     R.tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
   } else {
-    philox_samples(a, s_tab, s_guide, ray, __ldg(a.sigma + h), &R.sl, &R.tl, rk);
-    R.w = a.weight ? __ldg(a.weight + h) : 1.f;
+    philox_samples(a, s_tab, s_guide, ray, sigma_h, &R.sl, &R.tl, rk);
   }
   // world sample (local2world(sample, sun_dir)), incident direction
   const float3 sl = R.sl;
@@ -588,9 +617,10 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x,
                  nch = ((uint64_t)a.rays - a.ray0 + chunk - 1) / chunk;
   for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-    const uint64_t r0 = a.ray0 + ch * chunk, r1 = min(r0 + chunk, (uint64_t)a.rays);
-    for (uint64_t r64 = r0 + threadIdx.x; r64 < r1; r64 += blockDim.x)
-      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, (uint32_t)r64, fy0, fy1, c, dep, a.rk);
+    // 32-bit ray ids within a chunk (a trace holds fewer than 2^32 rays)
+    const uint32_t r0 = (uint32_t)(a.ray0 + ch * chunk), r1 = (uint32_t)min(a.ray0 + (ch + 1) * chunk, (uint64_t)a.rays);
+    for (uint32_t ray = r0 + threadIdx.x; ray < r1; ray += blockDim.x)
+      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, ray, fy0, fy1, c, dep, a.rk);
   }
   if (STATS) flush_counters(c, a.stats);
 }

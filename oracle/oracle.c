@@ -38,7 +38,8 @@ void orc_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint3
 }
 
 /* the tracer's uniform: (k + 0.5) 2^-23, k the top 23 bits of the Philox word */
-static inline double u23(uint32_t w) { return ((double)(w >> 9) + 0.5) * (1.0 / 8388608.0); }
+/* the ray sampler's uniform: (k + 0.5) 2^-23 with k the low 23 bits of w (u23f) */
+static inline double u23(uint32_t w) { return ((double)(w & 0x7FFFFFu) + 0.5) * (1.0 / 8388608.0); }
 
 /* ------------------------------------------------------------ Buie */
 static float buie_core(float theta) {
@@ -502,7 +503,8 @@ void orc_ray_samples(const orc_trace_cfg* c, double sigma, uint64_t ray, double 
   double th = orc_buie_sample(u23(w[0]), c->cdf_x, c->cdf_y, c->slope, c->bparams) / 1000.0;
   angle2xyz(th, 2.0 * M_PI * u23(w[1]), sun_local);
   double z = sqrt(-2.0 * log(u23(w[2]))) * cos(2.0 * M_PI * u23(w[3]));
-  uint32_t extra = (w[0] & 0xFFu) | ((w[1] & 0xFFu) << 8) | ((w[2] & 0xFFu) << 16) | ((w[3] & 0xFFu) << 24);
+  /* the slope azimuth from the words' top bytes (the other uniforms use bits 0-22) */
+  uint32_t extra = (w[0] >> 24) | ((w[1] >> 24) << 8) | ((w[2] >> 24) << 16) | (w[3] & 0xFF000000u);
   angle2xyz(sigma * z, 2.0 * M_PI * u23(extra), turb_local);
 }
 
