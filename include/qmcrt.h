@@ -155,7 +155,9 @@ typedef struct qmcrt_sun {
  * results_with_given_normal, Gtest.cu:10-63). */
 typedef struct qmcrt_trace_params {
   uint64_t seed;           /* Philox key; every ray is a function of (seed, ray id) */
-  uint64_t rays;           /* total rays; must be a multiple of rays_per_point (Poisson) */
+  uint64_t rays;           /* total rays; must be a multiple of rays_per_point (Poisson).  2^32 rays and more
+                              need a power-of-two rays_per_point (fewer than 2^31 points); the adjoint and
+                              batches take fewer than 2^32 */
   int32_t rays_per_point;  /* rays per micro-heliostat point (reference: 2048) */
   int32_t point_mode;      /* QMCRT_POINTS_* */
   float point_spacing;     /* Poisson: minimum spacing in m; GRID: pixel length in m */

@@ -1049,8 +1049,12 @@ qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStre
   } else {
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown point mode");
   }
-  if (total <= 0 || (uint64_t)total * (uint64_t)p->rays_per_point > 0xFFFFFFFFull)
-    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray count must be in [1, 2^32)");
+  // points are 32-bit ids; rays reach 2^32 and beyond only with a power-of-two
+  // count per point, which splits a ray id into its point with a shift
+  const bool pow2 = (p->rays_per_point & (p->rays_per_point - 1)) == 0;
+  if (total <= 0 || total > 0x7FFFFFFFll || (!pow2 && (uint64_t)total * (uint64_t)p->rays_per_point > 0xFFFFFFFFull))
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT,
+                     "points must be in [1, 2^31); rays below 2^32 unless rays_per_point is a power of two");
   if (total > s->points_cap) {
     dev_free(s->d_point_xz);
     dev_free(s->d_point_helio);

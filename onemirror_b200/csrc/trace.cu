@@ -252,14 +252,16 @@ static qmcrt_status check_params(const qmcrt_trace_params* p) {
   return QMCRT_OK;
 }
 
-// The range [ray_begin, ray_end) of a trace of `total` rays (all of them when ray_end is 0).
+// The range [ray_begin, ray_end) of a trace of `total` rays (all of them when
+// ray_end is 0), as 64-bit ray ids; run_and_finish splits it into launches
+// that each stay between two multiples of 2^32.
 static qmcrt_status apply_range(const qmcrt_trace_params* p, uint64_t total, TraceArgs* a) {
-  a->rays = (uint32_t)total;
+  a->rays = total;
   a->ray0 = 0;
   if (p->ray_end == 0) return QMCRT_OK;
   if (p->ray_end > total) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray_end is past the trace's last ray");
-  a->ray0 = (uint32_t)p->ray_begin;
-  a->rays = (uint32_t)p->ray_end;
+  a->ray0 = p->ray_begin;
+  a->rays = p->ray_end;
   return QMCRT_OK;
 }
 
@@ -301,7 +303,21 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
   if (cull && !tables && a.cand && s->buie.within_alpha && !(p->quirks & QMCRT_QUIRK_SELF_HIT) &&
       p->kernel_variant != 4 && p->kernel_variant != 5)
     cull = 3;
-  QM_CUDA(dispatch(a, tables, records, stats != nullptr, cull, p->kernel_variant, st));
+  // one launch per block of 2^32 ray ids: a launch's threads carry the low
+  // word of their ray id, the launch the high word (and the records pointers
+  // its offset)
+  for (uint64_t b = a.ray0; b < a.rays;) {
+    const uint64_t hi = b >> 32, end = std::min<uint64_t>(a.rays, (hi + 1) << 32);
+    TraceArgs sa = a;
+    sa.ray_hi = (uint32_t)hi;
+    sa.g_hi = a.rpp_shift >= 0 ? (uint32_t)((hi << 32) >> a.rpp_shift) : 0u;
+    sa.ray0 = b - (hi << 32);
+    sa.rays = end - (hi << 32);
+    if (sa.flags) sa.flags += hi << 32;
+    if (sa.pixel) sa.pixel += hi << 32;
+    QM_CUDA(dispatch(sa, tables, records, stats != nullptr, cull, p->kernel_variant, st));
+    b = end;
+  }
   QM_CUDA(cudaEventRecord(s->ev[3], st));
   const double scale = flux_scale(s, sun, p, weight_scale);
   FinalizeArgs f{};

@@ -58,8 +58,14 @@ struct TraceArgs {
   int res_x, res_y;
   // rays
   int n_helio;
-  uint32_t rays;  // one past the last ray traced
-  uint32_t ray0;  // the first ray traced (a range of the full set; 0 for whole traces)
+  // Rays of one launch: ids ray_hi * 2^32 + [ray0, rays).  A launch never
+  // crosses a multiple of 2^32, so a thread works with the low word of its
+  // ray id; the high word is word 1 of the Philox counter, and g_hi the
+  // point of ray ray_hi * 2^32 (power-of-two rays per point; 0 when ray_hi
+  // is 0).
+  uint64_t rays;
+  uint64_t ray0;
+  uint32_t ray_hi, g_hi;
   int rpp;
   int rpp_shift;  // log2(rpp) when rpp is a power of two, else -1
   uint2 rk[10];  // Philox round keys of the seed (philox_round_keys)
@@ -449,7 +455,7 @@ struct RaySetup {
 // faster memory).
 __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                                float sigma, float3* sl, float3* tl, const uint2* rk) {
-  uint4 r = philox4x32_10_rk(make_uint4(ray, 0u, a.item, kTagTrace), rk);
+  uint4 r = philox4x32_10_rk(make_uint4(ray, a.ray_hi, a.item, kTagTrace), rk);
   float th = buie_theta_mrad(a, s_tab, s_guide, u23f(r.x)) * 1e-3f;
   float st, ct, sp, cp;
   // The azimuths and the Box-Muller log use the hardware approximations
@@ -476,8 +482,8 @@ __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4*
 template <bool TABLES>
 __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
                                           RaySetup& R, const uint2* rk) {
-  const uint32_t g = a.rpp_shift >= 0 ? ray >> a.rpp_shift : ray / (uint32_t)a.rpp;
-  const uint32_t j = ray - g * (uint32_t)a.rpp;
+  const uint32_t g = a.rpp_shift >= 0 ? a.g_hi + (ray >> a.rpp_shift) : ray / (uint32_t)a.rpp;
+  const uint32_t j = ray - g * (uint32_t)a.rpp;  // table mode (ray_hi 0)
   const int h = __ldg(a.point_helio + g);
   if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
   R.h = h;
@@ -615,12 +621,13 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   // of a chunk, so its frame and candidates stay in L1, and the chunks are
   // small enough to keep the SMs evenly loaded
   const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x,
-                 nch = ((uint64_t)a.rays - a.ray0 + chunk - 1) / chunk;
+                 nch = (a.rays - a.ray0 + chunk - 1) / chunk;
   for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-    // 32-bit ray ids within a chunk (a trace holds fewer than 2^32 rays)
-    const uint32_t r0 = (uint32_t)(a.ray0 + ch * chunk), r1 = (uint32_t)min(a.ray0 + (ch + 1) * chunk, (uint64_t)a.rays);
-    for (uint32_t ray = r0 + threadIdx.x; ray < r1; ray += blockDim.x)
-      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, ray, fy0, fy1, c, dep, a.rk);
+    // the low words of the chunk's ray ids (the launch stays below 2^32)
+    const uint64_t b64 = a.ray0 + ch * chunk;
+    const uint32_t base = (uint32_t)b64, len = (uint32_t)(min(b64 + chunk, a.rays) - b64);
+    for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
+      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, base + j, fy0, fy1, c, dep, a.rk);
   }
   if (STATS) flush_counters(c, a.stats);
 }

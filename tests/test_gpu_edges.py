@@ -2,8 +2,10 @@
 test_gpu_parity): one heliostat, rays-per-point that is not a power of two,
 regular grid points through the full trace, given normals / tilts /
 per-heliostat slope errors, a sun below the horizon, zero DNI, accumulation,
-one scene across suns and point sets, the largest ray count, and the
+one scene across suns and point sets, traces past 2^32 rays, and the
 arguments that must be rejected."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -143,22 +145,53 @@ def test_one_scene_across_suns_and_point_sets_equals_fresh_scenes():
     sc.close()
 
 
-def test_largest_ray_count():
-    """2^32 - 4096 rays (ray ids fill 32 bits; 2^20 - 1 points x 4096): the
-    count map still sums to the hits; 2^32 rays are rejected before anything
-    is allocated or launched."""
+def test_traces_past_2_to_the_32_rays():
+    """2^32 + 2^24 rays (2^20 + 4096 points x 4096 on the mid field): ray ids
+    pass 32 bits, so the trace runs as two launches whose threads carry the
+    low word of their ray id and whose Philox counters carry the high word.
+    The count map sums to the hits; the records of a ray range straddling
+    2^32 equal the FP64 oracle's for the same 64-bit ray ids; the limits that
+    remain are refused before anything is allocated: 2^32 rays or more with a
+    rays-per-point that is not a power of two, and 2^31 points."""
+    from test_gpu_parity import AGREE, compare_records
     w = W.mid()
-    w.params = W.params((1 << 32) - 4096, 4096, 0.18)
+    total = (1 << 32) + (1 << 24)
+    w.params = W.params(total, 4096, 0.18)
     sc = SolarScene.from_workload(w)
     g = sc.trace(w.sun, w.params)
     st = g["stats"]
-    assert st.rays == (1 << 32) - 4096
+    assert st.rays == total
     assert g["counts"].sum().item() == st.hit - st.offmap
     assert 0.5 < st.hit / st.rays < 0.8
-    p = W.params(1 << 32, 4096, 0.18)
-    with pytest.raises(capi.QmcrtError) as e:
-        sc.trace(w.sun, p)
-    assert e.value.status == capi.ERR_INVALID_ARGUMENT
+    # a range across 2^32: records indexed by ray id, so the output pointers
+    # are given as if the buffers started at ray 0 (only [begin, end) is written)
+    begin, n = (1 << 32) - 8192, 16384
+    flags = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    pixel = torch.zeros(n, dtype=torch.int32, device="cuda")
+    o = capi.Outputs()
+    o.d_ray_flags = flags.data_ptr() - begin
+    o.d_ray_pixel = pixel.data_ptr() - 4 * begin
+    p = W.params(total, 4096, 0.18)
+    p.ray_begin, p.ray_end = begin, begin + n
+    capi.check(capi.lib().qmcrt_trace(sc.h, C.byref(w.sun), C.byref(p), C.byref(o), None,
+                                      C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    gi = sc.grid_info()
+    ref = O.Scene(w.pos, w.size, w.sigma, w.receiver, w.grid.cell[0], w.grid.margin, list(w.sun.dir), aim=w.aim,
+                  grid_csr=sc.read_grid(), grid_bounds=(list(gi.origin), list(gi.cell), list(gi.dims)))
+    sc.sample_points_count = total // 4096
+    xz, helio = sc.read_points()
+    weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
+    cfg = ref.cfg(w.sun.csr, p.seed, total, 4096, xz, helio, weight, ray_begin=begin, ray_end=begin + n)
+    orc = ref.trace_philox(cfg, maps=False)
+    frac, nbad = compare_records(flags.cpu().numpy(), pixel.cpu().numpy(), orc["flags"], orc["pixel"],
+                                 w.receiver.res_x)
+    assert frac >= AGREE, (frac, nbad)
+    assert (flags.cpu().numpy() & capi.RAY_HIT).any()
+    for bad in (W.params(3000 * 1431656, 3000, 0.18), W.params((1 << 31) * 256, 256, 0.18)):
+        with pytest.raises(capi.QmcrtError) as e:
+            sc.trace(w.sun, bad)
+        assert e.value.status == capi.ERR_INVALID_ARGUMENT
     sc.close()
 
 
