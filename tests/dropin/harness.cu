@@ -100,14 +100,27 @@ extern "C" {
 
 // The drop-in's traced results for a scene built from arrays: counts,
 // flux (W/m^2) and the smoothed map (radius, ratio, method, source as
-// qmcrt_smooth_params), and the resolution.  Returns the qmcrt status.
+// qmcrt_smooth_params), and the resolution.  normals_out [3n] and sun_out
+// [3] receive the heliostat normals and sun direction as the reference's
+// objects hold them (RectangleHelio::CRotate and the harness normalise in
+// float), which is what the drop-in passes on.  Returns the qmcrt status.
 int dropin_results(int n, const float* pos, const float* size, const float* normal, const float* gpos,
                    const float* gsize, const float* ginter, const float* rpos, const float* rsize, const float* rnorm,
                    int rface, int geometry_info, float helio_pixel, const float* sun_dir, float dni, float csr,
                    float sigma, int lights, unsigned long long seed, int radius, float ratio, int method, int source,
-                   uint32_t* h_counts, float* h_flux, float* h_smoothed, int* res_out, double* stats_out) {
+                   uint32_t* h_counts, float* h_flux, float* h_smoothed, int* res_out, double* stats_out,
+                   float* normals_out, float* sun_out) {
   ArrayScene* s = make_scene(n, pos, size, normal, gpos, gsize, ginter, rpos, rsize, rnorm, rface, geometry_info,
                              helio_pixel, sun_dir, dni, csr, sigma, lights);
+  for (int i = 0; i < n; ++i) {
+    const float3 q = s->heliostats[i]->normal_;
+    normals_out[3 * i] = q.x;
+    normals_out[3 * i + 1] = q.y;
+    normals_out[3 * i + 2] = q.z;
+  }
+  sun_out[0] = s->sunray_->sun_dir_.x;
+  sun_out[1] = s->sunray_->sun_dir_.y;
+  sun_out[2] = s->sunray_->sun_dir_.z;
   const qmcrt_smooth_params sm = {radius, ratio, method, source};
   std::vector<float> flux, smoothed;
   std::vector<uint32_t> counts;

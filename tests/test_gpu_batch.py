@@ -20,7 +20,7 @@ if not torch.cuda.is_available():
 
 from onemirror_b200.scene import Batch, SolarScene  # noqa: E402
 
-RAYS = 1 << 18
+RAYS = 1 << 20  # 4096 points per item: at least one per heliostat of the 4000-heliostat field
 
 
 # every third sun position of the day (the first and last, at 5 deg, spread

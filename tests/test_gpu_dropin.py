@@ -67,16 +67,22 @@ def dropin(L, s, radius, ratio, method, source):
     sm = np.zeros(res, np.float32)
     ro = np.zeros(2, np.int32)
     st = np.zeros(4, np.float64)
+    nrm = np.zeros_like(s["normal"])
+    sun = np.zeros(3, np.float32)
     rc = L.dropin_results(*args(s), C.c_ulonglong(SEED), radius, C.c_float(ratio), method, source,
                           counts.ctypes.data_as(C.POINTER(C.c_uint32)), flux.ctypes.data_as(fp), sm.ctypes.data_as(fp),
-                          ro.ctypes.data_as(C.POINTER(C.c_int)), st.ctypes.data_as(C.POINTER(C.c_double)))
+                          ro.ctypes.data_as(C.POINTER(C.c_int)), st.ctypes.data_as(C.POINTER(C.c_double)),
+                          nrm.ctypes.data_as(fp), sun.ctypes.data_as(fp))
     assert rc == 0
+    # the reference's objects hold the inputs re-normalised in float
+    assert np.allclose(nrm, s["normal"], atol=1e-6) and np.allclose(sun, s["sun"], atol=1e-6)
     shape = (int(ro[1]), int(ro[0]))
-    return counts.reshape(shape), flux.reshape(shape), sm.reshape(shape), st
+    return counts.reshape(shape), flux.reshape(shape), sm.reshape(shape), st, nrm, sun
 
 
-def python_side(s, radius, ratio, method, source):
-    """The same scene through the Python binding of the C-ABI."""
+def python_side(s, radius, ratio, method, source, normal=None, sun_dir=None):
+    """The same scene through the Python binding of the C-ABI (with the
+    normals and sun direction the drop-in passed on, when given)."""
     rec = capi.Receiver()
     rec.type = capi.RECEIVER_FLAT
     rec.pos[:], rec.size[:], rec.normal[:] = list(s["rpos"]), list(s["rsize"]), list(s["rnorm"])
@@ -85,9 +91,9 @@ def python_side(s, radius, ratio, method, source):
     gp = capi.GridParams()
     gp.cell[:], gp.origin[:], gp.extent[:] = list(s["inter"]), list(s["gpos"]), list(s["gsize"])
     gp.explicit_bounds, gp.fine_div = 1, 1
-    sc = SolarScene(s["pos"], s["size"], rec, gp, sigma=s["sigma"], normal=s["normal"])
+    sc = SolarScene(s["pos"], s["size"], rec, gp, sigma=s["sigma"], normal=s["normal"] if normal is None else normal)
     sun = capi.Sun()
-    sun.dir[:] = list(s["sun"])
+    sun.dir[:] = list(s["sun"] if sun_dir is None else sun_dir)
     sun.dni, sun.csr = s["dni"], s["csr"]
     p = W.params(0, LIGHTS, s["pixel"], seed=SEED, mode=capi.POINTS_GRID)
     out = sc.results_host(sun, p, radius, ratio, method, source, stats=True)
@@ -97,8 +103,8 @@ def python_side(s, radius, ratio, method, source):
 
 def test_dropin_equals_the_binding_on_counts_and_count_smoothing(scene):
     L, s = scene
-    counts, flux, sm, st = dropin(L, s, 2, 0.2, capi.TRIM_SORTED, capi.SMOOTH_COUNTS)
-    py = python_side(s, 2, 0.2, capi.TRIM_SORTED, capi.SMOOTH_COUNTS)
+    counts, flux, sm, st, nrm, sun = dropin(L, s, 2, 0.2, capi.TRIM_SORTED, capi.SMOOTH_COUNTS)
+    py = python_side(s, 2, 0.2, capi.TRIM_SORTED, capi.SMOOTH_COUNTS, nrm, sun)
     assert counts.sum() > 0 and np.array_equal(counts, py["counts"])
     assert sm.tobytes() == py["smoothed"].tobytes()
     assert np.allclose(flux, py["flux"], rtol=0, atol=1e-5 * flux.max())
@@ -108,8 +114,8 @@ def test_dropin_equals_the_binding_on_counts_and_count_smoothing(scene):
 
 def test_dropin_smooths_the_energy_image_as_the_reference_does(scene):
     L, s = scene
-    counts, flux, sm, _ = dropin(L, s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY)
-    py = python_side(s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY)
+    counts, flux, sm, _, nrm, sun = dropin(L, s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY)
+    py = python_side(s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY, nrm, sun)
     assert np.array_equal(counts, py["counts"])
     assert np.allclose(sm, py["smoothed"], rtol=0, atol=1e-5 * sm.max())
     # a smoothed flux map: same total scale as the flux, spread out
@@ -120,7 +126,8 @@ def test_results_with_given_normal_writes_the_reference_result_files(scene, tmp_
     L, s = scene
     ns, sm = tmp_path / "nonsmooth.txt", tmp_path / "smooth.txt"
     assert L.dropin_results_with_given_normal(*args(s), str(ns).encode(), str(sm).encode()) == 0
-    py = python_side(s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY)
+    _, _, _, _, nrm, sun_used = dropin(L, s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY)
+    py = python_side(s, 5, 0.02, capi.TRIM_HEAPS, capi.SMOOTH_ENERGY, nrm, sun_used)
     # total energy as Gtest.cu:29,39-44: sum |n . sun| DNI w h, times rho / S_rec
     sun = s["sun"] / np.linalg.norm(s["sun"])
     total = np.float32(0)
