@@ -168,9 +168,7 @@ typedef struct qmcrt_trace_params {
   int32_t kernel_variant;  /* 0 or 1: default (fastest: Philox rays test their heliostat's occluder
                               candidates); 2: grid walk without vertical culling (every cell on the path
                               tested); 3: the production kernel without its 4-CTA register cap;
-                              4: grid walk, a two-level grid on its fine level only; 5: grid walk;
-                              6: two rays per thread (Philox rays on occluder candidates, power-of-two
-                              rays_per_point, no records or statistics; otherwise the default) */
+                              4: grid walk, a two-level grid on its fine level only; 5: grid walk */
   uint32_t item;           /* Philox stream (counter word 2): distinct items give independent ray sets
                               (shards of one trace, items of a batch) */
   int32_t attenuation;     /* QMCRT_ATTEN_*: atmospheric transmittance of the mirror-to-receiver leg */

@@ -91,25 +91,8 @@ static cudaError_t dispatch2(const TraceArgs& a, bool stats, int cull, cudaStrea
   return cull ? launch_trace<TABLES, RECORDS, false, 1>(a, st) : launch_trace<TABLES, RECORDS, false, 0>(a, st);
 }
 
-template <int MINB>
-static cudaError_t launch_trace2(const TraceArgs& a, cudaStream_t st) {
-  auto k = trace2_kernel<MINB>;
-  int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTraceThreads, 0);
-  if (e != cudaSuccess) return e;
-  int64_t blocks = (int64_t)std::max(per_sm, 1) * sm_count();
-  int64_t need = ((int64_t)a.rays - a.ray0 + kTraceThreads - 1) / kTraceThreads;
-  blocks = std::max<int64_t>(1, std::min(blocks, need));
-  k<<<(unsigned)blocks, kTraceThreads, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
 static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool stats, int cull, int variant,
                             cudaStream_t st) {
-  // variant 6: two rays per thread (Philox rays on occluder candidates with
-  // point masks and a power-of-two count of rays per point)
-  if (variant == 6 && !tables && !records && !stats && cull == 3 && a.point_mask && a.rpp_shift >= 0)
-    return launch_trace2<3>(a, st);
   // the production path (no records, no statistics) is compiled for 4 resident
   // CTAs per SM (64 registers); variant 3 keeps the unconstrained build
   if (variant != 3 && !tables && !records && !stats && cull == 3) return launch_trace<false, false, false, 3, 4>(a, st);
@@ -261,7 +244,7 @@ static qmcrt_status check_params(const qmcrt_trace_params* p) {
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "reflectivity must be in [0,1]");
   if (p->quirks & ~QMCRT_QUIRKS_REFERENCE) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown quirk bits");
   if (p->deposit != QMCRT_DEPOSIT_NEAREST) return set_error(QMCRT_ERR_NOT_SUPPORTED, "bilinear deposition is only used by the adjoint");
-  if (p->kernel_variant < 0 || p->kernel_variant > 6) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "kernel_variant must be 0..6");
+  if (p->kernel_variant < 0 || p->kernel_variant > 5) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "kernel_variant must be 0..5");
   if (p->attenuation != QMCRT_ATTEN_NONE && p->attenuation != QMCRT_ATTEN_POLY_EXP)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
   if (p->ray_end != 0 && p->ray_begin >= p->ray_end)

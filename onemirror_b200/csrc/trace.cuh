@@ -646,95 +646,4 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
   if (STATS) flush_counters(c, a.stats);
 }
 
-// Two rays per thread, stage by stage (kernel_variant 6): the loads, Philox
-// blocks, sample directions, reflections and energies of both rays are
-// independent straight-line work the scheduler can interleave, which halves
-// the dependency stalls of those stages; the walks and the receiver run one
-// ray after the other.  The arithmetic of each ray is trace_ray's, so the
-// results are identical.  For Philox traces on occluder candidates with point
-// masks and a power-of-two count of rays per point (the production path).
-template <class Dep>
-__device__ __forceinline__ void trace_pair(const TraceArgs& a, const float4* s_tab, const int* s_guide,
-                                           const uint32_t (&ray)[2], float fy0, float fy1, RayCounters& c,
-                                           const Dep& deposit) {
-  int h[2];
-  uint32_t g[2];
-  uint2 reach[2];
-  float sig[2], w[2];
-  uint4 r[2];
-#pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    g[p] = a.g_hi + (ray[p] >> a.rpp_shift);
-    h[p] = __ldg(a.point_helio + g[p]);
-    const uint4 pm = __ldg(a.point_mask + g[p]);
-    reach[p] = make_uint2(pm.x, pm.y);
-    sig[p] = __uint_as_float(pm.z);
-    w[p] = __uint_as_float(pm.w);
-    r[p] = ray_block(a, ray[p], a.rk);
-  }
-  float th[2];
-#pragma unroll
-  for (int p = 0; p < 2; ++p) th[p] = buie_theta_mrad(a, s_tab, s_guide, u23f(r[p].x));
-  float3 tl[2];
-  d3 ws[2];
-#pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    float3 sl;
-    sample_dirs(r[p], th[p], sig[p], &sl, &tl[p]);
-    ws[p] = mk(sl.x * a.su[0] + sl.y * a.sn[0] + sl.z * a.sv[0], sl.x * a.su[1] + sl.y * a.sn[1] + sl.z * a.sv[1],
-               sl.x * a.su[2] + sl.y * a.sn[2] + sl.z * a.sv[2]);
-  }
-  d3 rd[2];
-  float e[2];
-#pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    const double2* F = reinterpret_cast<const double2*>(a.frame + kFrameStride * h[p]);
-    const double2 q0 = __ldg(F), q1 = __ldg(F + 1), q2 = __ldg(F + 2), q3 = __ldg(F + 3), q4 = __ldg(F + 4);
-    frame64 fr;
-    fr.u = mk(q0.x, q0.y, q1.x);
-    fr.n = mk(q1.y, q2.x, q2.y);
-    fr.v = mk(q3.x, q3.y, q4.x);
-    const d3 np = rnorm(apply(fr, (double)tl[p].x, (double)tl[p].y, (double)tl[p].z));
-    rd[p] = ws[p] - (2.0 * dot(ws[p], np)) * np;
-    e[p] = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * w[p];
-  }
-#pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    // the point's world coordinates, w holding their float x and y
-    const double2* O = reinterpret_cast<const double2*>(a.point_origin + g[p]);  // 32-byte records
-    const double2 oa = __ldg(O), ob = __ldg(O + 1);
-    const d3 o = mk(oa.x, oa.y, ob.x);
-    const float3 of = f3(__int_as_float(__double2loint(ob.y)), __int_as_float(__double2hiint(ob.y)), (float)ob.x);
-    const float3 sdir = f3((float)-ws[p].x, (float)-ws[p].y, (float)-ws[p].z);
-    if (list_blocked<false>(a, h[p], 0, of, sdir, fy0, fy1, c.test, c.cell, reach[p].x)) continue;
-    if (list_blocked<false>(a, h[p], 1, of, to_f(rd[p]), fy0, fy1, c.test, c.cell, reach[p].y)) continue;
-    int pix = -1;
-    double t = 0.0;
-    if (receiver_hit(a, o, rd[p], pix, &t) && pix >= 0)
-      deposit(pix, a.atten ? e[p] * atten_eta(a.atten, (float)t) : e[p]);
-  }
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(kTraceThreads, MINB) trace2_kernel(const TraceArgs a) {
-  __shared__ float4 s_tab[1024];
-  __shared__ int s_guide[kBuieBuckets];
-  const float fy0 = from_ordered(__ldg(a.field_yr)), fy1 = from_ordered(__ldg(a.field_yr + 1));
-  load_buie(a.buie, s_tab, s_guide);
-  __syncthreads();
-  RayCounters c;
-  const GlobalDeposit dep{a.counts, a.energy};
-  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = (a.rays - a.ray0 + chunk - 1) / chunk;
-  for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-    const uint64_t b64 = a.ray0 + ch * chunk;
-    const uint32_t base = (uint32_t)b64, len = (uint32_t)(min(b64 + chunk, a.rays) - b64);
-    uint32_t j = threadIdx.x;
-    for (; j + blockDim.x < len; j += 2 * blockDim.x) {
-      const uint32_t pr[2] = {base + j, base + j + blockDim.x};
-      trace_pair(a, s_tab, s_guide, pr, fy0, fy1, c, dep);
-    }
-    if (j < len) trace_ray<false, false, false, 3>(a, s_tab, s_guide, base + j, fy0, fy1, c, dep, a.rk);
-  }
-}
-
 }  // namespace qm

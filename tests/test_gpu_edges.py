@@ -298,23 +298,3 @@ def test_ray_range_traces_the_same_rays():
     p.ray_begin = p.ray_end = 0
     sc.close()
 
-
-@pytest.mark.parametrize("name", ["small", "mid", "large"])
-def test_two_rays_per_thread_equals_one(name):
-    """kernel_variant 6 traces two rays per thread, stage by stage, with each
-    ray's arithmetic unchanged: its integer count maps equal the default
-    kernel's exactly, its energy maps to float-atomic ordering; an odd tail
-    (rays not a multiple of 512 per chunk) takes the one-ray path."""
-    w = W.BUILDERS[name]() if name == "small" else W.BUILDERS[name](rays=(1 << 24) + 256 * 3)
-    sc = SolarScene.from_workload(w)
-    outs = []
-    for variant in (0, 6):
-        p = W.params(int(w.params.rays), 256, w.params.point_spacing, seed=31)
-        p.kernel_variant = variant
-        r = sc.trace(w.sun, p, stats=False)
-        torch.cuda.synchronize()
-        outs.append((r["counts"].cpu().numpy(), r["energy"].cpu().numpy()))
-    (c0, e0), (c6, e6) = outs
-    assert c0.sum() > 0 and np.array_equal(c0, c6)
-    assert np.allclose(e0, e6, rtol=1e-5, atol=1e-6 * e0.max())
-    sc.close()
