@@ -349,7 +349,7 @@ def batch_section(reps=3):
             "tuning": {"chunk_rays": tuning.chunk_rays, "ctas_per_sm": tuning.ctas_per_sm, "tile": tuning.tile}}
 
 
-def adjoint_section(reps=5):
+def adjoint_section(reps=5, check=True):
     """Adjoint cost on the differentiable field (2000 heliostats, 128x128,
     2^26 rays): plain trace, adjoint forward (bilinear deposit + tape + loss)
     and backward, CUDA events after warm-up."""
@@ -377,12 +377,36 @@ def adjoint_section(reps=5):
             tp.append(ev[0].elapsed_time(ev[1]))
             tf.append(ev[1].elapsed_time(ev[2]))
             tb.append(ev[2].elapsed_time(ev[3]))
+    # the gradients these timings produce, against the FP64 adjoint of the same rays
+    err = None
+    if check:
+        from oracle import oracle as O
+        _, loss, flux = sc.adjoint_forward(w.sun, w.params, target, tape=tape)
+        ga, gt = sc.adjoint_backward(tape)
+        g = np.concatenate([ga.cpu().numpy(), gt.cpu().numpy()], 1)
+        gi = sc.grid_info()
+        ref = O.Scene(w.pos, w.size, w.sigma, w.receiver, w.grid.cell[0], w.grid.margin, list(w.sun.dir), aim=sc.aim,
+                      tilt=sc.tilt, grid_csr=sc.read_grid(), grid_bounds=(list(gi.origin), list(gi.cell), list(gi.dims)))
+        sc.sample_points_count = int(w.params.rays) // w.params.rays_per_point
+        xz, helio = sc.read_points()
+        weight = np.asarray(w.size[:, 0] * w.size[:, 2], np.float64) / np.bincount(helio, minlength=w.n)
+        cfg = ref.cfg(w.sun.csr, w.params.seed, int(w.params.rays), w.params.rays_per_point, xz, helio, weight)
+        pix = (w.receiver.size[0] / w.receiver.res_x) * (w.receiver.size[1] / w.receiver.res_y)
+        scale = w.sun.dni * w.params.reflectivity / (w.params.rays_per_point * pix)
+        oloss, oenergy, og = ref.adjoint(cfg, w.extra["target"], scale)
+        flux = flux.cpu().numpy()
+        oflux = oenergy * scale
+        err = {"loss_rel": abs(loss - oloss) / oloss, "flux_rel_max": float(np.abs(flux - oflux).max() / oflux.max()),
+               "gradients_rel_norm": float(np.linalg.norm(g - og) / np.linalg.norm(og)),
+               "column_max_rel": [float(np.abs(g[:, k] - og[:, k]).max() / np.abs(og[:, k]).max()) for k in range(4)],
+               "method": "the timed field's loss, flux map and 8000 gradients against the FP64 CPU adjoint of the same "
+                         "2^26 rays (oracle/, per-ray central differences with visibility held)"}
     SolarScene.tape_free(tape)
     sc.close()
     f, b, p = statistics.median(tf), statistics.median(tb), statistics.median(tp)
     return {"heliostats": w.n, "rays": int(w.params.rays), "params": 4 * w.n, "plain_trace_ms": p,
             "adjoint_forward_ms": f, "adjoint_backward_ms": b, "backward_over_forward": b / f,
-            "adjoint_over_plain_forward": (f + b) / p}
+            "adjoint_over_plain_forward": (f + b) / p, "gradient_error_vs_fp64": err}
 
 
 def workload_name(w):

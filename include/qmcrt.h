@@ -525,6 +525,19 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* scene, const qmcrt_sun* sun, con
                                    const float* d_target, uint64_t state_bytes_max, float* d_flux, double* loss,
                                    qmcrt_tape** tape, void* stream);
 qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* tape, float* d_grad_aim, float* d_grad_tilt, void* stream);
+/* The forward pass again at the scene's current aim points and tilts (after
+ * qmcrt_scene_set_field), with every ray's visibility taken from `tape`
+ * instead of traced: a ray the tape marks as a hit deposits wherever its
+ * receiver-plane (u, v) falls now (corners off the map dropped), the others
+ * deposit nothing.  This is the estimator whose derivative the backward pass
+ * computes, so its central differences check the gradient without the jumps
+ * that visibility changes add to those of the full loss.  The tape must hold
+ * every ray (state_bytes_max 0) and is only read; like a forward pass, the
+ * call leaves its loss and adjoint map in the tape for a following backward
+ * pass.  Writes d_flux (may be NULL) and, if `loss` is not NULL,
+ * synchronises and returns L. */
+qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* tape, const float* d_target, float* d_flux, double* loss,
+                                  void* stream);
 qmcrt_status qmcrt_tape_loss(qmcrt_tape* tape, double* loss, void* stream);
 qmcrt_status qmcrt_tape_free(qmcrt_tape* tape);
 

@@ -167,6 +167,7 @@ PROTOTYPES = {
     "qmcrt_adjoint_forward": (C.c_int, [C.c_void_p, C.POINTER(Sun), C.POINTER(TraceParams), C.c_void_p, C.c_uint64,
                                         C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.c_void_p]),
     "qmcrt_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "qmcrt_adjoint_replay": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "qmcrt_tape_loss": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "qmcrt_tape_free": (C.c_int, [C.c_void_p]),
     "qmcrt_fp32_peak_probe": (C.c_int, [C.c_void_p, C.c_int32, dp, C.c_void_p]),

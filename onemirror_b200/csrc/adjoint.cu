@@ -147,6 +147,19 @@ __device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, doub
   return *t >= 1e-6;
 }
 
+// The receiver plane's (u, v) of the line o + t d, without the range tests:
+// the same arithmetic as receiver_uv.  The replayed forward pass deposits a
+// ray the tape marks as a hit wherever its (u, v) now falls.
+__device__ __forceinline__ void receiver_plane_uv(const TraceArgs& a, d3 o, d3 d, double* u, double* v) {
+  d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
+  d3 pv = cross(d, E2);
+  double inv = rcp_nr(dot(E1, pv));
+  d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
+  *u = dot(T, pv) * inv;
+  d3 qv = cross(T, E1);
+  *v = dot(d, qv) * inv;
+}
+
 // Reflection geometry of one ray: the perturbed unit normal and reflected
 // unit direction, and the lengths they had before normalising (for the
 // derivative of the normalisation in the backward pass).
@@ -200,7 +213,11 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
   return receiver_uv(a, R.o, g->rd, u, v, t);
 }
 
-template <bool CULL>
+// REPLAY: the visibility of every ray comes from the tape instead of the
+// walks (qmcrt_adjoint_replay), and a ray the tape marks as a hit deposits
+// wherever its (u, v) falls now, corners off the map dropped; the tape is
+// only read.
+template <bool CULL, bool REPLAY = false>
 __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
@@ -219,14 +236,21 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
   for (uint64_t r64 = ch * chunk + threadIdx.x, r1 = min((ch + 1) * chunk, (uint64_t)a.rays); r64 < r1;
        r64 += blockDim.x) {
     const uint32_t ray = (uint32_t)r64;
+    if (REPLAY && A.tape[r64] == 0) continue;
     RaySetup R;
     ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
     Refl g;
     double u, v, t;
     float e;
-    const bool hit = ray_hits<CULL, false>(a, R, fy0, fy1, &g, &u, &v, &t, &e);
-    if (r64 < A.saved) A.tape[r64] = hit ? 1 : 0;
-    if (!hit) continue;
+    if (REPLAY) {
+      g = reflect_ray<false>(R);
+      e = (float)fabs(g.np.x * a.sdir[0] + g.np.y * a.sdir[1] + g.np.z * a.sdir[2]) * R.w;
+      receiver_plane_uv(a, R.o, g.rd, &u, &v);
+    } else {
+      const bool hit = ray_hits<CULL, false>(a, R, fy0, fy1, &g, &u, &v, &t, &e);
+      if (r64 < A.saved) A.tape[r64] = hit ? 1 : 0;
+      if (!hit) continue;
+    }
     float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
     int i0 = (int)floorf(px), j0 = (int)floorf(py);
     float fx = px - (float)i0, fy = py - (float)j0;
@@ -358,6 +382,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         int i0 = (int)floorf(px), j0 = (int)floorf(py);
         float fx = px - (float)i0, fy = py - (float)j0;
         float Gc[4];
+#pragma unroll
         for (int k = 0; k < 4; ++k) {
           int ci = i0 + (k & 1), cj = j0 + (k >> 1);
           Gc[k] = (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) ? 0.f : __ldg(A.G + cj * a.res_x + ci);
@@ -383,23 +408,29 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
 #pragma unroll
         for (int r = 0; r < 9; ++r) Jr[r] = __ldg(J + r);
         const float x = R.xz.x, z = R.xz.y, hy = 0.5f * __ldg(a.size + 3 * h + 1);
+        // Reverse mode through the ray: the loss's sensitivity to the ray's
+        // frame components (c_u, c_n, c_v), then one product with the frame
+        // Jacobian per parameter.  The chain, forward: origin
+        // dO = x du + hy dn + z dv; normal dN = P_n(tl.x du + tl.y dn + tl.z dv) / |n'|;
+        // reflection dR = P_r(-2 ((dN.ws) n + (n.ws) dN)) / |r'| (P: the
+        // projections of the normalisations); hit b = dO + t dR, read along
+        // the plane as du = (b . (E2 x r)) / det and dv = (b . (r x E1)) / det;
+        // energy de = sgn(s.n) (s . dN) w; the loss term
+        // de gW + e (gWx res_x dv + gWy res_y du).  Each step below is the
+        // transpose of one of these.
+        const float3 beta = (e * gWy * (float)a.res_y * iden) * cr + (e * gWx * (float)a.res_x * iden) * cross(rdf, E1);
+        float3 rho = t * beta;                          // d/dR
+        rho = ilr * (rho - dot(rdf, rho) * rdf);        // through r's normalisation
+        float3 nu = -2.f * (dot(rho, npf) * wsf + nws * rho);  // d/dN from the reflection
+        nu = fma3(gW * sg * R.w, sd, nu);               // and from the energy
+        const float3 mu = ilnp * (nu - dot(npf, nu) * npf);  // through n's normalisation
+        const float3 cu = fma3(x, beta, R.tl.x * mu), cn = fma3(hy, beta, R.tl.y * mu),
+                     cv = fma3(z, beta, R.tl.z * mu);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const float3 du = f3(comp(Jr[0], k), comp(Jr[1], k), comp(Jr[2], k));
-          const float3 dn = f3(comp(Jr[3], k), comp(Jr[4], k), comp(Jr[5], k));
-          const float3 dv = f3(comp(Jr[6], k), comp(Jr[7], k), comp(Jr[8], k));
-          const float3 dO = fma3(x, du, fma3(hy, dn, z * dv));
-          float3 dN = fma3(R.tl.x, du, fma3(R.tl.y, dn, R.tl.z * dv));
-          dN = ilnp * (dN - dot(npf, dN) * npf);  // d(normalize)
-          float3 dR = -2.f * (dot(dN, wsf) * npf + nws * dN);
-          dR = ilr * (dR - dot(rdf, dR) * rdf);
-          const float3 b = dO + t * dR;  // d(hit point) = du E1 + dv E2 along the plane
-          const float duk = dot(b, cr) * iden;
-          const float dvk = dot(E1, cross(b, rdf)) * iden;
-          const float dpx = (float)a.res_x * dvk, dpy = (float)a.res_y * duk;
-          const float dek = sg * dot(sd, dN) * R.w;
-          gk[k] = dek * gW + e * (gWx * dpx + gWy * dpy);
-        }
+        for (int k = 0; k < 4; ++k)
+          gk[k] = cu.x * comp(Jr[0], k) + cu.y * comp(Jr[1], k) + cu.z * comp(Jr[2], k) + cn.x * comp(Jr[3], k) +
+                  cn.y * comp(Jr[4], k) + cn.z * comp(Jr[5], k) + cv.x * comp(Jr[6], k) + cv.y * comp(Jr[7], k) +
+                  cv.z * comp(Jr[8], k);
       }
     }
     // one atomic per warp and parameter when the warp's rays share a heliostat
@@ -459,6 +490,33 @@ struct qmcrt_tape {
 };
 
 namespace qm {
+// The tape's arguments against the scene's current geometry (after
+// tape_geometry): the pointers and per-sun values the kernels read.
+static AdjArgs tape_args(qmcrt_tape* t) {
+  qmcrt_scene* s = t->scene;
+  AdjArgs A = t->args;
+  fill_trace_args(s, scene_geom(s), &t->sun, t->params.quirks, &A.t);
+  A.t.buie = t->d_buie;
+  A.t.b_total = t->buie.params[3];
+  A.t.b_core = t->buie.params[2];
+  A.t.b_B = t->buie.params[4];
+  A.t.b_C = t->buie.params[5];
+  A.t.b_inv = 1 / (t->buie.params[1] + 1);
+  A.t.b_inv_bucket = t->buie.inv_bucket;
+  if (!t->buie.within_alpha) { A.t.cand = nullptr; A.t.cand_n = nullptr; }
+  A.t.rays = t->args.t.rays;
+  A.t.rpp = t->args.t.rpp;
+  A.t.rpp_shift = t->args.t.rpp_shift;
+  std::memcpy(A.t.rk, t->args.t.rk, sizeof(A.t.rk));
+  A.t.item = t->args.t.item;
+  A.t.point_xz = s->d_point_xz;
+  A.t.point_helio = s->d_point_helio;
+  A.t.point_mask = s->d_point_mask;
+  A.t.point_origin = s->d_point_origin;
+  A.t.energy = t->d_energy;
+  return A;
+}
+
 static qmcrt_status tape_geometry(qmcrt_tape* t, cudaStream_t st) {
   qmcrt_scene* s = t->scene;
   qmcrt_status e;
@@ -596,26 +654,7 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   qmcrt_scene* s = t->scene;
   qmcrt_status e;
   if ((e = tape_geometry(t, st))) return e;  // re-aims only if the scene moved on to another sun
-  AdjArgs A = t->args;
-  fill_trace_args(s, scene_geom(s), &t->sun, t->params.quirks, &A.t);
-  A.t.buie = t->d_buie;
-  A.t.b_total = t->buie.params[3];
-  A.t.b_core = t->buie.params[2];
-  A.t.b_B = t->buie.params[4];
-  A.t.b_C = t->buie.params[5];
-  A.t.b_inv = 1 / (t->buie.params[1] + 1);
-  A.t.b_inv_bucket = t->buie.inv_bucket;
-  if (!t->buie.within_alpha) { A.t.cand = nullptr; A.t.cand_n = nullptr; }
-  A.t.rays = t->args.t.rays;
-  A.t.rpp = t->args.t.rpp;
-  A.t.rpp_shift = t->args.t.rpp_shift;
-  std::memcpy(A.t.rk, t->args.t.rk, sizeof(A.t.rk));
-  A.t.item = t->args.t.item;
-  A.t.point_xz = s->d_point_xz;
-  A.t.point_helio = s->d_point_helio;
-  A.t.point_mask = s->d_point_mask;
-  A.t.point_origin = s->d_point_origin;
-  A.t.energy = t->d_energy;
+  AdjArgs A = tape_args(t);
   A.grad_aim = d_grad_aim;
   A.grad_tilt = d_grad_tilt;
   JacArgs j{};
@@ -639,6 +678,37 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   QM_CUDA(cudaGetLastError());
   adjoint_backward_kernel<true><<<adj_blocks(adjoint_backward_kernel<true>, A.t.rays), kAdjThreads, 0, st>>>(A);
   QM_CUDA(cudaGetLastError());
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* t, const float* d_target, float* d_flux, double* loss, void* stream) {
+  if (!t || !d_target) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (t->args.saved < t->params.rays)
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "replay needs a tape that holds every ray (state_bytes_max 0)");
+  cudaStream_t st = (cudaStream_t)stream;
+  qmcrt_scene* s = t->scene;
+  qmcrt_status e;
+  if ((e = tape_geometry(t, st))) return e;  // the scene's current aim points and tilts
+  AdjArgs A = tape_args(t);
+  const int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
+  const size_t tile_bytes = (size_t)A.tile * A.tile * sizeof(float);
+  QM_CUDA(cudaFuncSetAttribute(adjoint_forward_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)tile_bytes));
+  QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
+  QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
+  adjoint_forward_kernel<true, true>
+      <<<adj_blocks(adjoint_forward_kernel<true, true>, t->params.rays, tile_bytes), kAdjThreads, tile_bytes, st>>>(A);
+  QM_CUDA(cudaGetLastError());
+  const qmcrt_trace_params& p = t->params;
+  LossArgs la{t->d_energy, d_target, d_flux, t->d_G,
+              (float)((double)t->sun.dni * p.reflectivity / ((double)p.rays_per_point * s->rg.pixel_area)), res,
+              t->d_loss};
+  loss_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
+  QM_CUDA(cudaGetLastError());
+  if (loss) {
+    QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    QM_CUDA(cudaStreamSynchronize(st));
+  }
   return QMCRT_OK;
 }
 

@@ -194,6 +194,16 @@ class SolarScene:
         capi.check(capi.lib().qmcrt_adjoint_backward(tape, _ptr(ga), _ptr(gt), _stream()))
         return ga, gt
 
+    def adjoint_replay(self, tape, target, want_loss=True, flux=False):
+        """The forward pass at the current aim points and tilts with the
+        visibility recorded in `tape` (qmcrt_adjoint_replay).  Returns
+        (loss or None, flux map or None)."""
+        loss = C.c_double()
+        fl = torch.zeros(self.res, dtype=torch.float32, device="cuda") if flux else None
+        capi.check(capi.lib().qmcrt_adjoint_replay(tape, _ptr(target), _ptr(fl), C.byref(loss) if want_loss else None,
+                                                   _stream()))
+        return (loss.value if want_loss else None), fl
+
     @staticmethod
     def tape_free(tape):
         capi.lib().qmcrt_tape_free(tape)
