@@ -534,8 +534,9 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* tape, float* d_grad_aim, float* 
  * that visibility changes add to those of the full loss.  The tape must hold
  * every ray (state_bytes_max 0) and is only read; like a forward pass, the
  * call leaves its loss and adjoint map in the tape for a following backward
- * pass.  Writes d_flux (may be NULL) and, if `loss` is not NULL,
- * synchronises and returns L. */
+ * pass.  The replay deposits in 64-bit fixed point (2^-40) and forms the loss
+ * in double, so its loss is the same bit for bit from run to run.  Writes
+ * d_flux (may be NULL) and, if `loss` is not NULL, synchronises and returns L. */
 qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* tape, const float* d_target, float* d_flux, double* loss,
                                   void* stream);
 qmcrt_status qmcrt_tape_loss(qmcrt_tape* tape, double* loss, void* stream);

@@ -122,6 +122,7 @@ struct AdjArgs {
   int tile, tile_r0, tile_c0;  // forward: block-private tile of tile x tile pixels at (row r0, col c0); 0: none
   double ew[3], eh[3];  // receiver width / height unit axes (flat receivers)
   uint8_t* tape;        // one visibility byte per ray
+  unsigned long long* energy_fx;  // replay: the energy map in 2^-40 fixed point (exact sums in any order)
   uint64_t saved;       // rays with a byte in the tape
   const float* G;       // adjoint map (backward)
   const float* jac;     // frame Jacobians (backward)
@@ -216,7 +217,9 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
 // REPLAY: the visibility of every ray comes from the tape instead of the
 // walks (qmcrt_adjoint_replay), and a ray the tape marks as a hit deposits
 // wherever its (u, v) falls now, corners off the map dropped; the tape is
-// only read.
+// only read.  The deposits are 64-bit fixed point with 2^-40 resolution,
+// added with integer atomics: the sums are exact in any order, so the
+// replayed loss is the same bit for bit from run to run.
 template <bool CULL, bool REPLAY = false>
 __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[1024];
@@ -255,6 +258,15 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
     int i0 = (int)floorf(px), j0 = (int)floorf(py);
     float fx = px - (float)i0, fy = py - (float)j0;
     const float wgt[4] = {(1.f - fx) * (1.f - fy), fx * (1.f - fy), (1.f - fx) * fy, fx * fy};
+    if (REPLAY) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int ci = i0 + (k & 1), cj = j0 + (k >> 1);
+        if (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) continue;
+        atomicAdd(A.energy_fx + cj * a.res_x + ci, __double2ull_rn((double)(e * wgt[k]) * 0x1p40));
+      }
+      continue;
+    }
     if ((unsigned)(j0 - r0) < (unsigned)(T - 1) && (unsigned)(i0 - c0) < (unsigned)(T - 1)) {
       // all four corners in the tile (which lies inside the map): one check
       float* q = s_tile + (j0 - r0) * T + (i0 - c0);
@@ -299,6 +311,30 @@ __global__ void loss_kernel(LossArgs a) {
     float d = f - a.target[i];
     acc += (double)d * d;
     a.G[i] = 2.f * d * a.scale;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(a.loss, acc);
+}
+
+// The loss of a fixed-point energy map (the replay), in double throughout.
+struct LossFxArgs {
+  const unsigned long long* energy;
+  const float* target;
+  float* flux;  // may be NULL
+  float* G;
+  double scale;
+  int64_t res;
+  double* loss;
+};
+
+__global__ void loss_fx_kernel(LossFxArgs a) {
+  double acc = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.res; i += (int64_t)gridDim.x * blockDim.x) {
+    const double f = (double)a.energy[i] * 0x1p-40 * a.scale;
+    if (a.flux) a.flux[i] = (float)f;
+    const double d = f - (double)a.target[i];
+    acc += d * d;
+    a.G[i] = (float)(2.0 * d * a.scale);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(a.loss, acc);
@@ -482,6 +518,7 @@ struct qmcrt_tape {
   float* d_jac = nullptr;
   double* d_loss = nullptr;
   float* d_energy = nullptr;
+  unsigned long long* d_energy_fx = nullptr;  // replay: [res] fixed-point energy map
   bool cull = true;
   // capacities, so that a tape passed back to qmcrt_adjoint_forward reuses its buffers
   uint64_t cap_tape = 0;
@@ -691,19 +728,18 @@ qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* t, const float* d_target, float* d
   if ((e = tape_geometry(t, st))) return e;  // the scene's current aim points and tilts
   AdjArgs A = tape_args(t);
   const int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
-  const size_t tile_bytes = (size_t)A.tile * A.tile * sizeof(float);
-  QM_CUDA(cudaFuncSetAttribute(adjoint_forward_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)tile_bytes));
-  QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
+  if (!t->d_energy_fx) QM_CUDA(cudaMalloc(&t->d_energy_fx, t->cap_res * sizeof(unsigned long long)));
+  A.energy_fx = t->d_energy_fx;
+  A.tile = 0;  // every deposit a 64-bit integer atomic into the global map
+  QM_CUDA(cudaMemsetAsync(t->d_energy_fx, 0, res * sizeof(unsigned long long), st));
   QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
   adjoint_forward_kernel<true, true>
-      <<<adj_blocks(adjoint_forward_kernel<true, true>, t->params.rays, tile_bytes), kAdjThreads, tile_bytes, st>>>(A);
+      <<<adj_blocks(adjoint_forward_kernel<true, true>, t->params.rays), kAdjThreads, 0, st>>>(A);
   QM_CUDA(cudaGetLastError());
   const qmcrt_trace_params& p = t->params;
-  LossArgs la{t->d_energy, d_target, d_flux, t->d_G,
-              (float)((double)t->sun.dni * p.reflectivity / ((double)p.rays_per_point * s->rg.pixel_area)), res,
-              t->d_loss};
-  loss_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
+  LossFxArgs la{t->d_energy_fx, d_target, d_flux, t->d_G,
+                (double)t->sun.dni * p.reflectivity / ((double)p.rays_per_point * s->rg.pixel_area), res, t->d_loss};
+  loss_fx_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
   QM_CUDA(cudaGetLastError());
   if (loss) {
     QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -727,6 +763,7 @@ qmcrt_status qmcrt_tape_free(qmcrt_tape* t) {
   cudaFree(t->d_jac);
   cudaFree(t->d_loss);
   cudaFree(t->d_energy);
+  cudaFree(t->d_energy_fx);
   cudaFree(t->d_buie);
   delete t;
   return QMCRT_OK;
