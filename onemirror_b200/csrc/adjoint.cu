@@ -27,7 +27,7 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
 void buie_with_guide(float csr, BuieTable* t);
 
 constexpr int kAdjThreads = 256;
-constexpr int kAdjTileMax = 112;  // 50.2 KB of tile + 20 KB of Buie table: 3 CTAs per SM
+constexpr int kAdjTileMax = 112;  // 50.6 KB of tile (rows of 113) + 20 KB of Buie table: 3 CTAs per SM
 
 // ------------------------------------------------------------ dual numbers
 // value + derivatives with respect to the 4 parameters of one heliostat
@@ -227,9 +227,11 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
   // block-private tile of the energy map: many heliostats aim at the same
   // spot, so global atomics on it would queue at the hot pixels
   extern __shared__ float s_tile[];
-  const int T = A.tile, r0 = A.tile_r0, c0 = A.tile_c0;
+  // rows of the tile are T + 1 floats apart (an odd stride: hits in the same
+  // column a few rows apart fall in different shared-memory banks)
+  const int T = A.tile, TS = T + 1, r0 = A.tile_r0, c0 = A.tile_c0;
   const TraceArgs& a = A.t;
-  for (int i = threadIdx.x; i < T * T; i += blockDim.x) s_tile[i] = 0.f;
+  for (int i = threadIdx.x; i < T * TS; i += blockDim.x) s_tile[i] = 0.f;
   load_buie(a.buie, s_tab, s_guide);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
@@ -269,11 +271,11 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
     }
     if ((unsigned)(j0 - r0) < (unsigned)(T - 1) && (unsigned)(i0 - c0) < (unsigned)(T - 1)) {
       // all four corners in the tile (which lies inside the map): one check
-      float* q = s_tile + (j0 - r0) * T + (i0 - c0);
+      float* q = s_tile + (j0 - r0) * TS + (i0 - c0);
       atomicAdd(q, e * wgt[0]);
       atomicAdd(q + 1, e * wgt[1]);
-      atomicAdd(q + T, e * wgt[2]);
-      atomicAdd(q + T + 1, e * wgt[3]);
+      atomicAdd(q + TS, e * wgt[2]);
+      atomicAdd(q + TS + 1, e * wgt[3]);
       continue;
     }
 #pragma unroll
@@ -281,15 +283,16 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
       int ci = i0 + (k & 1), cj = j0 + (k >> 1);
       if (ci < 0 || cj < 0 || ci >= a.res_x || cj >= a.res_y) continue;
       if ((unsigned)(cj - r0) < (unsigned)T && (unsigned)(ci - c0) < (unsigned)T)
-        atomicAdd(s_tile + (cj - r0) * T + (ci - c0), e * wgt[k]);
+        atomicAdd(s_tile + (cj - r0) * TS + (ci - c0), e * wgt[k]);
       else
         atomicAdd(a.energy + cj * a.res_x + ci, e * wgt[k]);
     }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
-    const float v = s_tile[i];
-    if (v != 0.f) atomicAdd(a.energy + (r0 + i / T) * a.res_x + (c0 + i % T), v);
+    const int tr = i / T, tc = i - tr * T;
+    const float v = s_tile[tr * TS + tc];
+    if (v != 0.f) atomicAdd(a.energy + (r0 + tr) * a.res_x + (c0 + tc), v);
   }
 }
 
@@ -664,7 +667,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.tile = std::min({s->rg.res_x, s->rg.res_y, kAdjTileMax});
   A.tile_r0 = (s->rg.res_y - A.tile) / 2;
   A.tile_c0 = (s->rg.res_x - A.tile) / 2;
-  const size_t tile_bytes = (size_t)A.tile * A.tile * sizeof(float);
+  const size_t tile_bytes = (size_t)A.tile * (A.tile + 1) * sizeof(float);  // rows T + 1 floats apart
   QM_CUDA(cudaFuncSetAttribute(adjoint_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes));
   const int blocks = adj_blocks(adjoint_forward_kernel<true>, p->rays, tile_bytes);
   *tape = t;  // from here on the caller owns it, also when a launch below fails
