@@ -345,9 +345,6 @@ __global__ void loss_fx_kernel(LossFxArgs a) {
 
 __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(s * a.x + b.x, s * a.y + b.y, s * a.z + b.z); }
 
-// Component k (0..3, a compile-time constant after unrolling) of a float4.
-__device__ __forceinline__ float comp(float4 q, int k) { return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w; }
-
 template <bool CULL>
 __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[1024];
@@ -440,12 +437,6 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         const float3 cr = cross(E2, rdf);
         const float iden = __fdividef(1.f, dot(E1, cr));
         const float t = (float)tr;
-        // the frame Jacobian, row-major [9][4]: row r holds d(frame component r)
-        // for the 4 parameters, one float4 (144-byte records, 16-byte aligned)
-        const float4* J = reinterpret_cast<const float4*>(A.jac) + 9 * h;
-        float4 Jr[9];
-#pragma unroll
-        for (int r = 0; r < 9; ++r) Jr[r] = __ldg(J + r);
         const float x = R.xz.x, z = R.xz.y, hy = 0.5f * __ldg(a.size + 3 * h + 1);
         // Reverse mode through the ray: the loss's sensitivity to the ray's
         // frame components (c_u, c_n, c_v), then one product with the frame
@@ -465,11 +456,20 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
         const float3 mu = ilnp * (nu - dot(npf, nu) * npf);  // through n's normalisation
         const float3 cu = fma3(x, beta, R.tl.x * mu), cn = fma3(hy, beta, R.tl.y * mu),
                      cv = fma3(z, beta, R.tl.z * mu);
+        // the frame Jacobian, row-major [9][4]: row r holds d(frame component r)
+        // for the 4 parameters, one float4 (144-byte records, 16-byte aligned;
+        // the same heliostat for most of a warp: broadcast loads), read row by
+        // row into the 4 products
+        const float4* J = reinterpret_cast<const float4*>(A.jac) + 9 * h;
+        const float c9[9] = {cu.x, cu.y, cu.z, cn.x, cn.y, cn.z, cv.x, cv.y, cv.z};
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          gk[k] = cu.x * comp(Jr[0], k) + cu.y * comp(Jr[1], k) + cu.z * comp(Jr[2], k) + cn.x * comp(Jr[3], k) +
-                  cn.y * comp(Jr[4], k) + cn.z * comp(Jr[5], k) + cv.x * comp(Jr[6], k) + cv.y * comp(Jr[7], k) +
-                  cv.z * comp(Jr[8], k);
+        for (int r = 0; r < 9; ++r) {
+          const float4 jr = __ldg(J + r);
+          gk[0] = fmaf(c9[r], jr.x, gk[0]);
+          gk[1] = fmaf(c9[r], jr.y, gk[1]);
+          gk[2] = fmaf(c9[r], jr.z, gk[2]);
+          gk[3] = fmaf(c9[r], jr.w, gk[3]);
+        }
       }
     }
     // one atomic per warp and parameter when the warp's rays share a heliostat
