@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
   const float* loaded = nullptr;
   float fy0 = 0.f, fy1 = 0.f;
   RayCounters cnt;
-  if (T > 0)
+  if constexpr (T > 0)
     for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
       s_cnt[i] = 0;
       s_en[i] = 0.f;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
     }
     const unsigned long long r0 = (c - __ldg(chunk_begin + it)) * (unsigned long long)chunk_rays;
     const unsigned long long r1 = min(r0 + chunk_rays, (unsigned long long)s_a.rays);
-    if (T > 0) {
+    if constexpr (T > 0) {
       if (threadIdx.x == 0) {
         int ar = 0, ac = 0;
         s_anchor[2] = chunk_anchor(s_a, (uint32_t)r0, T, &ar, &ac) ? 1 : 0;
