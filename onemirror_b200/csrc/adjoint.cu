@@ -238,9 +238,9 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
   // chunks of consecutive rays taken grid-stride, as in the plain tracer
   const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = ((uint64_t)a.rays + chunk - 1) / chunk;
   for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x)
-  for (uint64_t r64 = ch * chunk + threadIdx.x, r1 = min((ch + 1) * chunk, (uint64_t)a.rays); r64 < r1;
-       r64 += blockDim.x) {
-    const uint32_t ray = (uint32_t)r64;
+  for (uint32_t ray = (uint32_t)(ch * chunk) + threadIdx.x, r1 = (uint32_t)min((ch + 1) * chunk, (uint64_t)a.rays);
+       ray < r1; ray += blockDim.x) {  // 32-bit ray ids: the adjoint takes fewer than 2^32 rays
+    const uint64_t r64 = ray;
     if (REPLAY && A.tape[r64] == 0) continue;
     RaySetup R;
     ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
@@ -257,8 +257,9 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
       if (!hit) continue;
     }
     float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
-    int i0 = (int)floorf(px), j0 = (int)floorf(py);
-    float fx = px - (float)i0, fy = py - (float)j0;
+    const float flx = floorf(px), fly = floorf(py);
+    const int i0 = (int)flx, j0 = (int)fly;
+    const float fx = px - flx, fy = py - fly;
     const float wgt[4] = {(1.f - fx) * (1.f - fy), fx * (1.f - fy), (1.f - fx) * fy, fx * fy};
     if (REPLAY) {
 #pragma unroll
@@ -330,9 +331,14 @@ struct LossFxArgs {
   double* loss;
 };
 
-__global__ void loss_fx_kernel(LossFxArgs a) {
+// One block of kLossThreads threads: every thread sums a fixed stride of the
+// pixels and the block reduces the partial sums in a fixed tree, so the
+// replayed loss is the same double from run to run.
+constexpr int kLossThreads = 1024;
+__global__ void __launch_bounds__(kLossThreads) loss_fx_kernel(LossFxArgs a) {
+  __shared__ double part[kLossThreads / 32];
   double acc = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.res; i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = threadIdx.x; i < a.res; i += kLossThreads) {
     const double f = (double)a.energy[i] * 0x1p-40 * a.scale;
     if (a.flux) a.flux[i] = (float)f;
     const double d = f - (double)a.target[i];
@@ -340,7 +346,13 @@ __global__ void loss_fx_kernel(LossFxArgs a) {
     a.G[i] = (float)(2.0 * d * a.scale);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(a.loss, acc);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = part[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) *a.loss = acc;
+  }
 }
 
 __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(s * a.x + b.x, s * a.y + b.y, s * a.z + b.z); }
@@ -415,8 +427,9 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
       if (hit) {
         // bilinear corners and the adjoint map there
         float px = (float)(v * a.res_x) - 0.5f, py = (float)(u * a.res_y) - 0.5f;
-        int i0 = (int)floorf(px), j0 = (int)floorf(py);
-        float fx = px - (float)i0, fy = py - (float)j0;
+        const float flx = floorf(px), fly = floorf(py);
+        const int i0 = (int)flx, j0 = (int)fly;
+        const float fx = px - flx, fy = py - fly;
         float Gc[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -742,7 +755,7 @@ qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* t, const float* d_target, float* d
   const qmcrt_trace_params& p = t->params;
   LossFxArgs la{t->d_energy_fx, d_target, d_flux, t->d_G,
                 (double)t->sun.dni * p.reflectivity / ((double)p.rays_per_point * s->rg.pixel_area), res, t->d_loss};
-  loss_fx_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
+  loss_fx_kernel<<<1, kLossThreads, 0, st>>>(la);
   QM_CUDA(cudaGetLastError());
   if (loss) {
     QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
