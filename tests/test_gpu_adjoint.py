@@ -92,19 +92,25 @@ def central_differences(sc, w, target, pairs, scale=1.0, replay=None):
     """Central differences of the GPU loss for (heliostat, parameter) pairs
     under common random numbers: h = 1e-3 m for aims, 1e-5 rad for tilts
     (times `scale`).  With `replay` (a tape holding every ray) the loss is
-    the replayed forward pass's, each ray's visibility held at the tape's."""
+    the replayed forward pass's, each ray's visibility held at the tape's.
+    The parameters are float32 (an aim point 150 m up has a 1.5e-5 m ulp),
+    so the quotient divides by the step the stored parameter actually took,
+    not the nominal 2 h."""
     base_aim, base_tilt = sc.aim.copy(), sc.tilt.copy()
     out = []
     for h, k in pairs:
         step = (1e-3 if k < 2 else 1e-5) * scale
-        vals = []
+        vals, taken = [], []
         for sgn in (1.0, -1.0):
             sc.aim[:] = base_aim
             sc.tilt[:] = base_tilt
             if k < 2:
-                sc.aim[h] += (sgn * step * (EW if k == 0 else EH)).astype(np.float32)
+                e = EW if k == 0 else EH
+                sc.aim[h] += (sgn * step * e).astype(np.float32)
+                taken.append(float(np.dot(sc.aim[h].astype(np.float64), e)))
             else:
                 sc.tilt[h, k - 2] += np.float32(sgn * step)
+                taken.append(float(sc.tilt[h, k - 2]))
             sc.update_field()
             if replay is not None:
                 l, _ = sc.adjoint_replay(replay, target)
@@ -112,7 +118,7 @@ def central_differences(sc, w, target, pairs, scale=1.0, replay=None):
                 tape, l, _ = sc.adjoint_forward(w.sun, w.params, target, flux=False)
                 SolarScene.tape_free(tape)
             vals.append(l)
-        out.append((vals[0] - vals[1]) / (2 * step))
+        out.append((vals[0] - vals[1]) / (taken[0] - taken[1]))
     sc.aim[:] = base_aim
     sc.tilt[:] = base_tilt
     sc.update_field()

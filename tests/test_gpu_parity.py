@@ -286,6 +286,34 @@ def test_big_fields_on_ray_ranges(name):
     sc.close()
 
 
+def test_cylinder_columns_agree_across_resolutions():
+    """The cylinder's column rule from 512 to 65 536 columns.  The column
+    edges of a map with 2r columns include every edge of the map with r
+    columns, bit for bit (the angles 2 pi k / r are formed as (2 pi k) / r,
+    and doubling k and r scales numerator and denominator by a power of two),
+    so each hit's column at r is its column at 2r halved.  512 and 32 768
+    columns take the polynomial column estimate, 65 536 the atan2f one; the
+    edge tests must settle both on the same column for every ray."""
+    cols, flags0 = {}, None
+    for res in (512, 1024, 32768, 65536):
+        w = W.large(rays=1 << 22)
+        w.receiver.res_x, w.receiver.res_y = res, 16
+        sc = SolarScene.from_workload(w)
+        g = sc.trace(w.sun, w.params, records=True)
+        f, p = g["flags"].cpu().numpy(), g["pixel"].cpu().numpy()
+        sc.close()
+        if flags0 is None:
+            flags0 = f
+        assert np.array_equal(f, flags0)
+        cols[res] = np.where(p >= 0, p % res, -1)
+    hit = cols[512] >= 0
+    assert hit.mean() > 0.5
+    for r in (512, 32768):
+        assert np.array_equal(cols[r][hit], cols[2 * r][hit] // 2), r
+    assert np.array_equal(cols[512][hit], cols[32768][hit] // 64)
+    assert np.all(cols[65536][~hit] == -1)
+
+
 def test_two_level_grid_equals_its_fine_level():
     """Large field on its 50 m / 12.5 m two-level grid: the coarse level only
     steps through coarse cells whose heights the ray cannot meet, so flags,
