@@ -509,13 +509,20 @@ qmcrt_status qmcrt_batch_read(qmcrt_batch* batch, int32_t item, uint32_t* h_coun
  * scene's current aim points and tilts.  Pathwise derivative under the same
  * random numbers; shadow/block/receiver visibility held constant.
  *
- * qmcrt_adjoint_forward traces params->rays rays (params->deposit must be
+ * qmcrt_adjoint_forward traces params->rays rays, or the range
+ * [ray_begin, ray_end) of them (params->deposit must be
  * QMCRT_DEPOSIT_BILINEAR, flat receiver, corrected mode), keeps one
- * visibility byte per ray for at most state_bytes_max rays (0 = all; rays past
- * the cap recompute their visibility in the backward pass), writes the flux
- * map to d_flux (may be NULL) and, if `loss` is not NULL, synchronises and
- * returns L.  qmcrt_adjoint_backward writes d_grad_aim [2n] and d_grad_tilt
- * [2n] (device).
+ * visibility byte per traced ray for at most state_bytes_max rays (0 = all;
+ * rays past the cap recompute their visibility in the backward pass), writes
+ * the flux map to d_flux (may be NULL) and, if `loss` is not NULL,
+ * synchronises and returns L.  qmcrt_adjoint_backward writes d_grad_aim [2n]
+ * and d_grad_tilt [2n] (device): the gradient of L through the rays the tape
+ * traced.
+ * Sharded over GPUs (one ray range per rank): each rank runs the forward on
+ * its range, the ranks sum their energy maps (qmcrt_tape_energy, then an
+ * all-reduce), each passes the sum to qmcrt_adjoint_loss, runs the backward,
+ * and the ranks sum their gradients.  The loss and the summed gradients are
+ * those of one GPU tracing every ray, to float rounding.
  * `tape` is in/out: *tape == NULL makes a new tape; a tape returned by an
  * earlier call on the same scene is reused, its device buffers kept where
  * they are large enough (an optimisation loop then allocates nothing after
@@ -539,6 +546,16 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* tape, float* d_grad_aim, float* 
  * d_flux (may be NULL) and, if `loss` is not NULL, synchronises and returns L. */
 qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* tape, const float* d_target, float* d_flux, double* loss,
                                   void* stream);
+/* Copy the tape's energy map (the forward's deposits before flux scaling,
+ * [res_y x res_x] floats) to d_energy (device). */
+qmcrt_status qmcrt_tape_energy(const qmcrt_tape* tape, float* d_energy, void* stream);
+/* Re-form the flux map, the loss and the adjoint map the backward pass reads
+ * from d_energy (an energy map of the tape's layout, e.g. the sum of the
+ * ranks' maps of one sharded trace; NULL: the tape's own), against d_target.
+ * Writes d_flux (may be NULL) and, if `loss` is not NULL, synchronises and
+ * returns L. */
+qmcrt_status qmcrt_adjoint_loss(qmcrt_tape* tape, const float* d_energy, const float* d_target, float* d_flux,
+                                double* loss, void* stream);
 qmcrt_status qmcrt_tape_loss(qmcrt_tape* tape, double* loss, void* stream);
 qmcrt_status qmcrt_tape_free(qmcrt_tape* tape);
 

@@ -169,6 +169,9 @@ PROTOTYPES = {
     "qmcrt_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "qmcrt_adjoint_replay": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "qmcrt_tape_loss": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+    "qmcrt_tape_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "qmcrt_adjoint_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                     C.c_void_p]),
     "qmcrt_tape_free": (C.c_int, [C.c_void_p]),
     "qmcrt_fp32_peak_probe": (C.c_int, [C.c_void_p, C.c_int32, dp, C.c_void_p]),
     "qmcrt_philox_blocks": (C.c_int, [u32p, u32p, C.c_int64, C.c_void_p, C.c_void_p]),

@@ -26,8 +26,12 @@ void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, u
 qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
 void buie_with_guide(float csr, BuieTable* t);
 
-constexpr int kAdjThreads = 256;
-constexpr int kAdjTileMax = 112;  // 50.6 KB of tile (rows of 113) + 20 KB of Buie table: 3 CTAs per SM
+// 2 CTAs of 512 threads per SM (32 warps) at <= 64 registers: against 3 CTAs
+// of 256 at 72 and 80 registers, the forward takes 12 % and the backward 4 %
+// less time (the backward spills a little at 64 registers and still gains)
+constexpr int kAdjThreads = 512;
+constexpr int kAdjCtasPerSm = 2;
+constexpr int kAdjTileMax = 112;  // 50.6 KB of tile (rows of 113) + 20 KB of Buie table
 
 // ------------------------------------------------------------ dual numbers
 // value + derivatives with respect to the 4 parameters of one heliostat
@@ -221,7 +225,7 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
 // added with integer atomics: the sums are exact in any order, so the
 // replayed loss is the same bit for bit from run to run.
 template <bool CULL, bool REPLAY = false>
-__global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_forward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
   // block-private tile of the energy map: many heliostats aim at the same
@@ -235,15 +239,18 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_forward_kernel(const A
   load_buie(a.buie, s_tab, s_guide);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
-  // chunks of consecutive rays taken grid-stride, as in the plain tracer
-  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = ((uint64_t)a.rays + chunk - 1) / chunk;
+  // chunks of consecutive rays taken grid-stride, as in the plain tracer;
+  // i counts the rays of the range [ray0, rays) (ray0 + i is the ray id and
+  // i its tape byte).  32-bit: the adjoint takes fewer than 2^32 rays.
+  const uint32_t n = (uint32_t)(a.rays - a.ray0), ray0 = (uint32_t)a.ray0;
+  const uint64_t chunk = (uint64_t)kChunkBlocks * blockDim.x, nch = ((uint64_t)n + chunk - 1) / chunk;
   for (uint64_t ch = blockIdx.x; ch < nch; ch += gridDim.x)
-  for (uint32_t ray = (uint32_t)(ch * chunk) + threadIdx.x, r1 = (uint32_t)min((ch + 1) * chunk, (uint64_t)a.rays);
-       ray < r1; ray += blockDim.x) {  // 32-bit ray ids: the adjoint takes fewer than 2^32 rays
-    const uint64_t r64 = ray;
+  for (uint32_t i = (uint32_t)(ch * chunk) + threadIdx.x, i1 = (uint32_t)min((ch + 1) * chunk, (uint64_t)n); i < i1;
+       i += blockDim.x) {
+    const uint64_t r64 = i;
     if (REPLAY && A.tape[r64] == 0) continue;
     RaySetup R;
-    ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
+    ray_setup<false>(a, s_tab, s_guide, ray0 + i, R, a.rk);
     Refl g;
     double u, v, t;
     float e;
@@ -358,7 +365,7 @@ __global__ void __launch_bounds__(kLossThreads) loss_fx_kernel(LossFxArgs a) {
 __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(s * a.x + b.x, s * a.y + b.y, s * a.z + b.z); }
 
 template <bool CULL>
-__global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_backward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[1024];
   __shared__ int s_guide[kBuieBuckets];
   const TraceArgs& a = A.t;
@@ -377,19 +384,20 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
   // that owns it).  Lost rays cost nothing, and a segment's rays mostly share
   // a heliostat, so the warp reduction below stays uniform.
   const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const uint64_t nseg = ((uint64_t)a.rays + 255) / 256;
+  // rays of the range [ray0, rays), counted from ray0 (the tape's indexing)
+  const uint64_t n = a.rays - a.ray0, nseg = (n + 255) / 256;
   for (uint64_t sg = (uint64_t)blockIdx.x * nwarps + (threadIdx.x >> 5); sg < nseg;
        sg += (uint64_t)gridDim.x * nwarps) {
     const uint64_t b0 = sg * 256 + 8 * lane;  // this lane's first ray (a multiple of 8)
     uint32_t m = 0;  // bit k: ray b0 + k is worked on
-    if (b0 + 8 <= A.saved && b0 + 8 <= a.rays) {
+    if (b0 + 8 <= A.saved && b0 + 8 <= n) {
       const uint2 t8 = *reinterpret_cast<const uint2*>(A.tape + b0);  // 8-byte aligned
 #pragma unroll
       for (int k = 0; k < 8; ++k) m |= (((k < 4 ? t8.x >> (8 * k) : t8.y >> (8 * (k - 4))) & 0xFFu) != 0u) << k;
     } else {
       for (int k = 0; k < 8; ++k) {
         const uint64_t r = b0 + k;
-        if (r < a.rays && (r >= A.saved || A.tape[r] != 0)) m |= 1u << k;
+        if (r < n && (r >= A.saved || A.tape[r] != 0)) m |= 1u << k;
       }
     }
     const int cnt = __popc(m);
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(kAdjThreads, 3) adjoint_backward_kernel(const 
     if (q < total) {
       for (int i = 0; i < skip; ++i) mo &= mo - 1u;  // drop the lower selected rays
       const uint64_t r64 = sg * 256 + 8 * own + (__ffs(mo) - 1);
-      const uint32_t ray = (uint32_t)r64;
+      const uint32_t ray = (uint32_t)(a.ray0 + r64);
       RaySetup R;
       ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
       h = R.h;
@@ -536,6 +544,8 @@ struct qmcrt_tape {
   float* d_energy = nullptr;
   unsigned long long* d_energy_fx = nullptr;  // replay: [res] fixed-point energy map
   bool cull = true;
+  // rays of the traced range [args.t.ray0, args.t.rays): one tape byte each
+  uint64_t count() const { return args.t.rays - args.t.ray0; }
   // capacities, so that a tape passed back to qmcrt_adjoint_forward reuses its buffers
   uint64_t cap_tape = 0;
   int64_t cap_res = 0;
@@ -558,6 +568,7 @@ static AdjArgs tape_args(qmcrt_tape* t) {
   A.t.b_inv_bucket = t->buie.inv_bucket;
   if (!t->buie.within_alpha) { A.t.cand = nullptr; A.t.cand_n = nullptr; }
   A.t.rays = t->args.t.rays;
+  A.t.ray0 = t->args.t.ray0;
   A.t.rpp = t->args.t.rpp;
   A.t.rpp_shift = t->args.t.rpp_shift;
   std::memcpy(A.t.rk, t->args.t.rk, sizeof(A.t.rk));
@@ -568,6 +579,26 @@ static AdjArgs tape_args(qmcrt_tape* t) {
   A.t.point_origin = s->d_point_origin;
   A.t.energy = t->d_energy;
   return A;
+}
+
+// Flux, loss and adjoint map from the tape's energy map: flux = energy x
+// DNI rho / (rays per point x pixel area) (Gtest.cu:40-46 with the map's
+// pixel area), L = sum (flux - target)^2 and G = dL/d(energy).
+static qmcrt_status tape_loss_pass(qmcrt_tape* t, const float* d_target, float* d_flux, double* loss, cudaStream_t st) {
+  qmcrt_scene* s = t->scene;
+  const int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
+  QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
+  LossArgs la{t->d_energy, d_target, d_flux, t->d_G,
+              (float)((double)t->sun.dni * t->params.reflectivity /
+                      ((double)t->params.rays_per_point * s->rg.pixel_area)),
+              res, t->d_loss};
+  loss_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
+  QM_CUDA(cudaGetLastError());
+  if (loss) {
+    QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    QM_CUDA(cudaStreamSynchronize(st));
+  }
+  return QMCRT_OK;
 }
 
 static qmcrt_status tape_geometry(qmcrt_tape* t, cudaStream_t st) {
@@ -595,7 +626,8 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint traces in corrected mode");
   if (p->attenuation != QMCRT_ATTEN_NONE)
     return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint has no attenuation term");
-  if (p->ray_end != 0) return set_error(QMCRT_ERR_NOT_SUPPORTED, "the adjoint traces every ray");
+  if (p->ray_end != 0 && (p->ray_begin >= p->ray_end || p->ray_end > p->rays))
+    return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray range must have ray_begin < ray_end <= rays");
   if (!(sun->csr > 0.f && sun->csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   cudaStream_t st = (cudaStream_t)stream;
   // a tape from an earlier call keeps its buffers where they are large enough
@@ -610,7 +642,9 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   t->params = *p;
   qmcrt_status e;
   int64_t res = (int64_t)s->rg.res_x * s->rg.res_y;
-  uint64_t saved = state_bytes_max == 0 ? p->rays : std::min<uint64_t>(p->rays, state_bytes_max);
+  // the rays [ray_begin, ray_end) of the trace (all of them when ray_end is 0)
+  const uint64_t r0 = p->ray_end ? p->ray_begin : 0, r1 = p->ray_end ? p->ray_end : p->rays, count = r1 - r0;
+  uint64_t saved = state_bytes_max == 0 ? count : std::min<uint64_t>(count, state_bytes_max);
   cudaError_t ce = cudaSuccess;
   if (saved > t->cap_tape) {
     cudaFree(t->d_tape);
@@ -650,7 +684,8 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.t.b_inv = 1 / (t->buie.params[1] + 1);
   A.t.b_inv_bucket = t->buie.inv_bucket;
   if (!t->buie.within_alpha) { A.t.cand = nullptr; A.t.cand_n = nullptr; }  // walk the grid
-  A.t.rays = (uint32_t)p->rays;
+  A.t.ray0 = r0;
+  A.t.rays = r1;
   A.t.rpp = p->rays_per_point;
   A.t.rpp_shift = (A.t.rpp & (A.t.rpp - 1)) ? -1 : __builtin_ctz((unsigned)A.t.rpp);
   philox_round_keys(make_uint2((uint32_t)p->seed, (uint32_t)(p->seed >> 32)), A.t.rk);
@@ -682,23 +717,13 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.tile_c0 = (s->rg.res_x - A.tile) / 2;
   const size_t tile_bytes = (size_t)A.tile * (A.tile + 1) * sizeof(float);  // rows T + 1 floats apart
   QM_CUDA(cudaFuncSetAttribute(adjoint_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes));
-  const int blocks = adj_blocks(adjoint_forward_kernel<true>, p->rays, tile_bytes);
+  const int blocks = adj_blocks(adjoint_forward_kernel<true>, count, tile_bytes);
   *tape = t;  // from here on the caller owns it, also when a launch below fails
   QM_CUDA(cudaMemcpyAsync(t->d_buie, t->buie.host.data(), t->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
-  QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
   adjoint_forward_kernel<true><<<blocks, kAdjThreads, tile_bytes, st>>>(A);
   QM_CUDA(cudaGetLastError());
-  LossArgs la{t->d_energy, d_target, d_flux, t->d_G,
-              (float)((double)sun->dni * p->reflectivity / ((double)p->rays_per_point * s->rg.pixel_area)), res,
-              t->d_loss};
-  loss_kernel<<<(unsigned)std::min<int64_t>((res + 255) / 256, 1024), 256, 0, st>>>(la);
-  QM_CUDA(cudaGetLastError());
-  if (loss) {
-    QM_CUDA(cudaMemcpyAsync(loss, t->d_loss, sizeof(double), cudaMemcpyDeviceToHost, st));
-    QM_CUDA(cudaStreamSynchronize(st));
-  }
-  return QMCRT_OK;
+  return qm::tape_loss_pass(t, d_target, d_flux, loss, st);
 }
 
 qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_grad_tilt, void* stream) {
@@ -729,14 +754,14 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   QM_CUDA(cudaMemsetAsync(d_grad_tilt, 0, 2 * (size_t)s->n * sizeof(float), st));
   frame_jacobian_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(j);
   QM_CUDA(cudaGetLastError());
-  adjoint_backward_kernel<true><<<adj_blocks(adjoint_backward_kernel<true>, A.t.rays), kAdjThreads, 0, st>>>(A);
+  adjoint_backward_kernel<true><<<adj_blocks(adjoint_backward_kernel<true>, t->count()), kAdjThreads, 0, st>>>(A);
   QM_CUDA(cudaGetLastError());
   return QMCRT_OK;
 }
 
 qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* t, const float* d_target, float* d_flux, double* loss, void* stream) {
   if (!t || !d_target) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (t->args.saved < t->params.rays)
+  if (t->args.saved < t->count())
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "replay needs a tape that holds every ray (state_bytes_max 0)");
   cudaStream_t st = (cudaStream_t)stream;
   qmcrt_scene* s = t->scene;
@@ -750,7 +775,7 @@ qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* t, const float* d_target, float* d
   QM_CUDA(cudaMemsetAsync(t->d_energy_fx, 0, res * sizeof(unsigned long long), st));
   QM_CUDA(cudaMemsetAsync(t->d_loss, 0, sizeof(double), st));
   adjoint_forward_kernel<true, true>
-      <<<adj_blocks(adjoint_forward_kernel<true, true>, t->params.rays), kAdjThreads, 0, st>>>(A);
+      <<<adj_blocks(adjoint_forward_kernel<true, true>, t->count()), kAdjThreads, 0, st>>>(A);
   QM_CUDA(cudaGetLastError());
   const qmcrt_trace_params& p = t->params;
   LossFxArgs la{t->d_energy_fx, d_target, d_flux, t->d_G,
@@ -762,6 +787,23 @@ qmcrt_status qmcrt_adjoint_replay(qmcrt_tape* t, const float* d_target, float* d
     QM_CUDA(cudaStreamSynchronize(st));
   }
   return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_tape_energy(const qmcrt_tape* t, float* d_energy, void* stream) {
+  if (!t || !d_energy) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  const int64_t res = (int64_t)t->scene->rg.res_x * t->scene->rg.res_y;
+  QM_CUDA(cudaMemcpyAsync(d_energy, t->d_energy, res * sizeof(float), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_adjoint_loss(qmcrt_tape* t, const float* d_energy, const float* d_target, float* d_flux,
+                                double* loss, void* stream) {
+  if (!t || !d_target) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t res = (int64_t)t->scene->rg.res_x * t->scene->rg.res_y;
+  if (d_energy && d_energy != t->d_energy)
+    QM_CUDA(cudaMemcpyAsync(t->d_energy, d_energy, res * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  return qm::tape_loss_pass(t, d_target, d_flux, loss, st);
 }
 
 qmcrt_status qmcrt_tape_loss(qmcrt_tape* t, double* loss, void* stream) {

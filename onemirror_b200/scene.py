@@ -204,6 +204,23 @@ class SolarScene:
                                                    _stream()))
         return (loss.value if want_loss else None), fl
 
+    def tape_energy(self, tape):
+        """The tape's energy map (device float32 [res], a copy):
+        qmcrt_tape_energy."""
+        e = torch.empty(self.res, dtype=torch.float32, device="cuda")
+        capi.check(capi.lib().qmcrt_tape_energy(tape, _ptr(e), _stream()))
+        return e
+
+    def adjoint_loss(self, tape, target, energy=None, want_loss=True, flux=False):
+        """Flux, loss and adjoint map re-formed from `energy` (e.g. the sum of
+        the ranks' energy maps; None: the tape's own): qmcrt_adjoint_loss.
+        Returns (loss or None, flux map or None)."""
+        loss = C.c_double()
+        fl = torch.zeros(self.res, dtype=torch.float32, device="cuda") if flux else None
+        capi.check(capi.lib().qmcrt_adjoint_loss(tape, _ptr(energy), _ptr(target), _ptr(fl),
+                                                 C.byref(loss) if want_loss else None, _stream()))
+        return (loss.value if want_loss else None), fl
+
     @staticmethod
     def tape_free(tape):
         capi.lib().qmcrt_tape_free(tape)

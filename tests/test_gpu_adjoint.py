@@ -139,6 +139,42 @@ def test_gradients_match_central_differences_of_the_gpu_loss(case):
     assert max(rel) < 0.25, rel
 
 
+def test_ray_ranges_compose_to_the_full_adjoint(case):
+    """The sharded adjoint on one GPU, the ranks run one after the other:
+    three ray ranges (cut as dist.shard_range cuts them, the last one with a
+    capped tape), their energy maps summed, each tape's loss and adjoint map
+    re-formed from the sum (qmcrt_adjoint_loss), and the three backward
+    passes summed.  Loss, flux and gradients equal one tape over every ray,
+    up to the order of the float atomics."""
+    from onemirror_b200 import dist as D
+    w, sc, target = case
+    loss, flux, g = gpu_grad(sc, w, target)
+    tapes, energy = [], None
+    for rank in range(3):
+        p = type(w.params).from_buffer_copy(w.params)
+        p.ray_begin, p.ray_end = D.shard_range(rank, 3, RAYS)
+        cap = (p.ray_end - p.ray_begin) // 3 if rank == 2 else 0
+        tape, _, _ = sc.adjoint_forward(w.sun, p, target, state_bytes_max=cap, want_loss=False, flux=False)
+        tapes.append(tape)
+        e = sc.tape_energy(tape)
+        energy = e if energy is None else energy + e
+    gs = 0
+    for tape in tapes:
+        l, fl = sc.adjoint_loss(tape, target, energy=energy, flux=True)
+        assert abs(l - loss) <= 1e-6 * loss, (l, loss)
+        assert np.allclose(fl.cpu().numpy(), flux, rtol=0, atol=1e-5 * flux.max())
+        ga, gt = sc.adjoint_backward(tape)
+        gs = gs + np.concatenate([ga.cpu().numpy(), gt.cpu().numpy()], 1)
+        SolarScene.tape_free(tape)
+    assert np.allclose(gs, g, rtol=1e-4, atol=1e-5 * np.abs(g).max())
+    # a range past the trace's last ray, or an empty one, is refused
+    for b, e in ((RAYS, RAYS + 1), (5, 5)):
+        p = type(w.params).from_buffer_copy(w.params)
+        p.ray_begin, p.ray_end = b, e
+        with pytest.raises(capi.QmcrtError):
+            sc.adjoint_forward(w.sun, p, target)
+
+
 def test_capped_tape_recomputes_visibility(case):
     w, sc, target = case
     _, _, g_full = gpu_grad(sc, w, target)
