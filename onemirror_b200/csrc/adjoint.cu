@@ -31,7 +31,9 @@ void buie_with_guide(float csr, BuieTable* t);
 // less time (the backward spills a little at 64 registers and still gains)
 constexpr int kAdjThreads = 512;
 constexpr int kAdjCtasPerSm = 2;
-constexpr int kAdjTileMax = 112;  // 50.6 KB of tile (rows of 113) + 20 KB of Buie table
+// up to 83.5 KB of tile (rows of 145) + 20 KB of Buie table: 2 CTAs per SM;
+// a 128 x 128 map fits whole (forward 1.18 -> 1.07 ms against a 112^2 tile)
+constexpr int kAdjTileMax = 144;
 
 // ------------------------------------------------------------ dual numbers
 // value + derivatives with respect to the 4 parameters of one heliostat
@@ -710,8 +712,8 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.saved = saved;
   A.G = t->d_G;
   A.jac = t->d_jac;
-  // the tile: the map's central T x T pixels, T as large as keeps 3 CTAs
-  // (with the 16 KB Buie table) on an SM
+  // the tile: the map's central T x T pixels, T as large as keeps 2 CTAs
+  // (with the 20 KB Buie table) on an SM
   A.tile = std::min({s->rg.res_x, s->rg.res_y, kAdjTileMax});
   A.tile_r0 = (s->rg.res_y - A.tile) / 2;
   A.tile_c0 = (s->rg.res_x - A.tile) / 2;
