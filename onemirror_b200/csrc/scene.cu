@@ -794,6 +794,11 @@ static qmcrt_status build_buckets(qmcrt_scene* s, const qmcrt_field* f, cudaStre
   return QMCRT_OK;
 }
 
+__global__ void fill_value_kernel(float* p, int n, float v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
 qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st) {
   size_t n = (size_t)f->n;
   QM_CUDA(cudaMemcpyAsync(s->d_pos, f->pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -803,10 +808,9 @@ qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st)
   if (f->tilt) QM_CUDA(cudaMemcpyAsync(s->d_tilt, f->tilt, 2 * n * sizeof(float), cudaMemcpyHostToDevice, st));
   if (f->slope_sigma) {
     QM_CUDA(cudaMemcpyAsync(s->d_sigma, f->slope_sigma, n * sizeof(float), cudaMemcpyHostToDevice, st));
-  } else {
-    std::vector<float> sg(n, f->sigma);
-    QM_CUDA(cudaMemcpyAsync(s->d_sigma, sg.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
-    QM_CUDA(cudaStreamSynchronize(st));  // sg is a temporary
+  } else {  // one sigma for the field: written on the device (no host staging, no wait)
+    fill_value_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s->d_sigma, (int)n, f->sigma);
+    QM_CUDA(cudaGetLastError());
   }
   // sample points depend only on the mirror sizes (and the trace parameters)
   bool sizes_changed = s->h_size.size() != 3 * n || std::memcmp(s->h_size.data(), f->size, 3 * n * sizeof(float)) != 0;
