@@ -24,7 +24,7 @@ using namespace qm;
 namespace qm {
 void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a);
 qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
-void buie_with_guide(float csr, BuieTable* t);
+bool buie_with_guide(float csr, BuieTable* t);
 
 // 2 CTAs of 512 threads per SM (32 warps) at <= 64 registers: against 3 CTAs
 // of 256 at 72 and 80 registers, the forward takes 12 % and the backward 4 %
@@ -228,8 +228,7 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
 // replayed loss is the same bit for bit from run to run.
 template <bool CULL, bool REPLAY = false>
 __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_forward_kernel(const AdjArgs A) {
-  __shared__ float4 s_tab[1024];
-  __shared__ int s_guide[kBuieBuckets];
+  __shared__ float4 s_tab[kBuieRecords];
   // block-private tile of the energy map: many heliostats aim at the same
   // spot, so global atomics on it would queue at the hot pixels
   extern __shared__ float s_tile[];
@@ -238,7 +237,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_forward_ke
   const int T = A.tile, TS = T + 1, r0 = A.tile_r0, c0 = A.tile_c0;
   const TraceArgs& a = A.t;
   for (int i = threadIdx.x; i < T * TS; i += blockDim.x) s_tile[i] = 0.f;
-  load_buie(a.buie, s_tab, s_guide);
+  load_buie(a.buie, s_tab);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   // chunks of consecutive rays taken grid-stride, as in the plain tracer;
@@ -252,7 +251,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_forward_ke
     const uint64_t r64 = i;
     if (REPLAY && A.tape[r64] == 0) continue;
     RaySetup R;
-    ray_setup<false>(a, s_tab, s_guide, ray0 + i, R, a.rk);
+    ray_setup<false>(a, s_tab, ray0 + i, R, a.rk);
     Refl g;
     double u, v, t;
     float e;
@@ -368,10 +367,9 @@ __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(
 
 template <bool CULL>
 __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_backward_kernel(const AdjArgs A) {
-  __shared__ float4 s_tab[1024];
-  __shared__ int s_guide[kBuieBuckets];
+  __shared__ float4 s_tab[kBuieRecords];
   const TraceArgs& a = A.t;
-  load_buie(a.buie, s_tab, s_guide);
+  load_buie(a.buie, s_tab);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   const float3 E1 = f3((float)a.rE1[0], (float)a.rE1[1], (float)a.rE1[2]);
@@ -423,7 +421,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_backward_k
       const uint64_t r64 = sg * 256 + 8 * own + (__ffs(mo) - 1);
       const uint32_t ray = (uint32_t)(a.ray0 + r64);
       RaySetup R;
-      ray_setup<false>(a, s_tab, s_guide, ray, R, a.rk);
+      ray_setup<false>(a, s_tab, ray, R, a.rk);
       h = R.h;
       bool hit;
       Refl g;
@@ -672,10 +670,11 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
     if (ce == cudaSuccess) t->cap_n = s->n;
   }
   if (ce == cudaSuccess && !t->d_loss) ce = cudaMalloc(&t->d_loss, sizeof(double));
-  if (ce == cudaSuccess && !t->d_buie) ce = cudaMalloc(&t->d_buie, (1025 + 1025 + 1024 + kBuieBuckets) * sizeof(float));
+  if (ce == cudaSuccess && !t->d_buie) ce = cudaMalloc(&t->d_buie, 4 * (size_t)kBuieRecords * sizeof(float));
   if (ce != cudaSuccess) return fail(cuda_error(ce, "adjoint tape allocation"));
   if ((e = tape_geometry(t, st))) return fail(e);
-  buie_with_guide(sun->csr, &t->buie);
+  if (!buie_with_guide(sun->csr, &t->buie))
+    return fail(set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries"));
   AdjArgs& A = t->args;
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &A.t);
   A.t.buie = t->d_buie;

@@ -22,7 +22,7 @@ using namespace qm;
 
 namespace qm {
 void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a);
-void buie_with_guide(float csr, BuieTable* t);
+bool buie_with_guide(float csr, BuieTable* t);
 
 constexpr int kBatchThreads = 256;
 
@@ -81,12 +81,12 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
                        int n_items, uint32_t chunk_rays, unsigned long long total_chunks,
                        unsigned long long* counter, const __grid_constant__ PhiloxKeys keys) {
   __shared__ TraceArgs s_a;
-  __shared__ float4 s_tab[1024];
-  __shared__ int s_guide[kBuieBuckets];
+  __shared__ float4 s_tab[kBuieRecords];
   __shared__ unsigned long long s_c;
   __shared__ int s_item, s_anchor[3];
-  __shared__ uint32_t s_cnt[T > 0 ? T * T : 1];
-  __shared__ float s_en[T > 0 ? T * T : 1];
+  // the flux tile (T > 0) in dynamic shared memory: T^2 counts, then T^2 energies
+  extern __shared__ uint32_t s_cnt[];
+  float* s_en = reinterpret_cast<float*>(s_cnt + T * T);
   int cur = -1;
   const float* loaded = nullptr;
   float fy0 = 0.f, fy1 = 0.f;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
       for (int i = threadIdx.x; i < (int)(sizeof(TraceArgs) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
       __syncthreads();
       if (s_a.buie != loaded) {
-        load_buie(s_a.buie, s_tab, s_guide);
+        load_buie(s_a.buie, s_tab);
         loaded = s_a.buie;
       }
       fy0 = from_ordered(__ldg(s_a.field_yr));
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
       const TileDeposit<T> dep{s_cnt, s_en, s_anchor[2] ? s_anchor[0] : -(1 << 30), s_anchor[1], s_a.res_x,
                                s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
+        trace_ray<false, false, false, 3>(s_a, s_tab, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
       __syncthreads();
       if (s_anchor[2]) {  // flush the tile's non-zero pixels, then clear it
         for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
     } else {
       const GlobalDeposit dep{s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, 3>(s_a, s_tab, s_guide, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
+        trace_ray<false, false, false, 3>(s_a, s_tab, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
     }
     __syncthreads();  // everyone is done with s_c / s_a / the tile before the next chunk
   }
@@ -255,6 +255,33 @@ static qmcrt_status upload_chunks(qmcrt_batch* b, cudaStream_t st) {
   return QMCRT_OK;
 }
 
+// Dynamic shared memory of the batched kernel's T x T tile: T^2 counts and
+// T^2 energies, beside the staged Buie table.
+template <int T>
+constexpr int batch_tile_bytes() {
+  return T * T * (int)(sizeof(uint32_t) + sizeof(float));
+}
+
+// Allow the tiles' dynamic shared memory (static + dynamic above 48 KB);
+// done once per batch, outside any graph capture.
+static cudaError_t batch_allow_tiles() {
+  cudaError_t ce = cudaFuncSetAttribute(batch_trace_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        batch_tile_bytes<32>());
+  if (ce == cudaSuccess)
+    ce = cudaFuncSetAttribute(batch_trace_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              batch_tile_bytes<48>());
+  return ce;
+}
+
+// One launch of the batched kernel with a T x T tile (T = 0: none).
+template <int T>
+static cudaError_t launch_batch(qmcrt_batch* b, int ctas, int items, unsigned long long total, cudaStream_t st) {
+  batch_trace_kernel<T><<<ctas, kBatchThreads, batch_tile_bytes<T>(), st>>>(b->d_args, b->d_chunk_begin, items,
+                                                                           b->tuning.chunk_rays, total, b->d_counter,
+                                                                           b->keys);
+  return cudaGetLastError();
+}
+
 // The trace pass alone over the first n items (all items when n < 0).
 static qmcrt_status enqueue_trace(qmcrt_batch* b, int n, cudaStream_t st) {
   int items = n < 0 ? (int)b->items.size() : std::min<int>(n, (int)b->items.size());
@@ -264,18 +291,14 @@ static qmcrt_status enqueue_trace(qmcrt_batch* b, int n, cudaStream_t st) {
   ctas = (int)std::min<unsigned long long>((unsigned long long)ctas, std::max<unsigned long long>(total, 1));
   switch (b->tuning.tile) {
     case 32:
-      batch_trace_kernel<32><<<ctas, kBatchThreads, 0, st>>>(b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays,
-                                                              total, b->d_counter, b->keys);
+      QM_CUDA(launch_batch<32>(b, ctas, items, total, st));
       break;
     case 48:
-      batch_trace_kernel<48><<<ctas, kBatchThreads, 0, st>>>(b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays,
-                                                              total, b->d_counter, b->keys);
+      QM_CUDA(launch_batch<48>(b, ctas, items, total, st));
       break;
     default:
-      batch_trace_kernel<0><<<ctas, kBatchThreads, 0, st>>>(b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays,
-                                                             total, b->d_counter, b->keys);
+      QM_CUDA(launch_batch<0>(b, ctas, items, total, st));
   }
-  QM_CUDA(cudaGetLastError());
   return QMCRT_OK;
 }
 
@@ -334,6 +357,10 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
   if (params->point_mode != QMCRT_POINTS_POISSON || params->rays_per_point <= 0 || params->rays == 0 ||
       params->rays > 0xFFFFFFFFull)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "batches need Poisson points and 0 < rays < 2^32");
+  {
+    const cudaError_t ce = batch_allow_tiles();
+    if (ce != cudaSuccess) return cuda_error(ce, "batch tile shared memory");
+  }
   qmcrt_batch* b = new qmcrt_batch();
   b->params = *params;
   qmcrt_status e = QMCRT_OK;
@@ -375,7 +402,10 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     if ((e = balloc(&it.d_counts, it.res)) || (e = balloc(&it.d_energy, it.res)) || (e = balloc(&it.d_flux, it.res))) goto fail;
     float csr = it.sun.csr;
     if (!b->tables.count(csr)) {
-      buie_with_guide(csr, &b->tables[csr]);
+      if (!buie_with_guide(csr, &b->tables[csr])) {
+        e = set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
+        goto fail;
+      }
       float* d = nullptr;
       if ((e = balloc(&d, b->tables[csr].host.size()))) goto fail;
       b->d_tables[csr] = d;

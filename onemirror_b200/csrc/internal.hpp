@@ -31,11 +31,17 @@ struct ReceiverGeom {
 };
 
 // Buie sunshape table (1025 + 1025 + 1024 floats) and its scalars.
+// Buie table staging: uniform buckets over the core CDF, each holding at
+// most one boundary of the table's 1024 intervals (checked when the table is
+// built), and one interval record per bucket plus one past the last.
+constexpr int kBuieBuckets = 2048;
+constexpr int kBuieRecords = kBuieBuckets + 1;
+
 struct BuieTable {
   float csr = -1.f;
-  std::vector<float> host;  // cdf_x | cdf_y | slope | guide (int bits)
+  std::vector<float> host;  // one {angle, cdf, slope, next cdf} record per bucket (kBuieRecords)
   float params[6];          // k, gamma, core, total, B, C
-  float inv_bucket = 0;     // guide buckets per unit of CDF
+  float inv_bucket = 0;     // buckets per unit of CDF
   bool within_alpha = false; // every sample lies within kSunAlphaMax of the sun axis
 };
 

@@ -1274,7 +1274,7 @@ qmcrt_status qmcrt_scene_create(const qmcrt_field* field, const qmcrt_receiver* 
   ALLOC(s->d_map_flux, res);
   ALLOC(s->d_map_smooth, res);
   ALLOC(s->d_stats, 16);
-  ALLOC(s->d_buie, 1025 + 1025 + 1024 + 1024);  // table + guide
+  ALLOC(s->d_buie, 4 * kBuieRecords);  // one record per bucket of the Buie table
 #undef ALLOC
   for (int i = 0; i < 5; ++i) {
     cudaError_t ce = cudaEventCreate(&s->ev[i]);

@@ -102,53 +102,75 @@ static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool 
   return records ? dispatch2<false, true>(a, stats, cull, st) : dispatch2<false, false>(a, stats, cull, st);
 }
 
-// Buie table plus its guide, in the layout the kernels stage into shared
-// memory: cdf_x | cdf_y | slope | guide (int bits).
-void buie_with_guide(float csr, BuieTable* t) {
-  t->host.resize(1025 + 1025 + 1024 + kBuieBuckets);
-  float* h = t->host.data();
-  buie_build(csr, h, h + 1025, h + 2050, t->params);
-  // guide table: for each uniform bucket of [0, core), the interval index of
-  // the smallest float the kernel maps to that bucket ((int)(uu * inv_bucket),
-  // one float multiply: the same rounding here), so a lower bound of the
-  // index of every value in the bucket, and the index itself unless an
-  // interval boundary falls inside the bucket (a warp then scans 1.2 steps on
-  // average at csr 0.1 instead of 2.2 with a bound one below)
-  const float* cy = h + 1025;
+// Buie table in the layout the kernels stage into shared memory: for each
+// uniform bucket of [0, core) (index (int)(uu * inv_bucket), one float
+// multiply: the same rounding here), the 16-byte record {angle, cdf, slope,
+// next interval's cdf} of the interval holding the bucket's smallest value,
+// plus one record past the last bucket.  The kernel takes record b, or
+// record b + 1 once uu reaches the record's next cdf; that is the interval
+// max_less_index finds as long as no bucket holds two interval boundaries,
+// which this checks (the core table does not depend on csr; its narrowest
+// interval, the last, is 0.88 buckets wide).  Returns false if a bucket
+// holds two.
+bool buie_with_guide(float csr, BuieTable* t) {
+  std::vector<float> raw(1025 + 1025 + 1024);
+  float* cx = raw.data();
+  float* cy = cx + 1025;
+  buie_build(csr, cx, cy, cy + 1025, t->params);
+  const float* sl = cy + 1025;
   const float inv_bucket = (float)kBuieBuckets / t->params[2];
   auto bucket_of = [inv_bucket](float x) {
     volatile float p = x * inv_bucket;  // rounded to float, as the kernel's FMUL
     return (int)p;
   };
+  std::vector<int> first(kBuieRecords);
   for (int b = 0; b < kBuieBuckets; ++b) {
-    float edge = 0.f;
+    float edge = 0.f;  // the smallest float the kernel maps to bucket b
     if (b > 0) {
       edge = (float)b / inv_bucket;
       while (bucket_of(edge) < b) edge = std::nextafter(edge, HUGE_VALF);
       while (bucket_of(std::nextafter(edge, 0.f)) >= b) edge = std::nextafter(edge, 0.f);
     }
-    int lo = 0, hi = 1024;
-    while (lo < hi) {  // largest i with cy[i] <= edge
+    int lo = 0, hi = 1023;
+    while (lo < hi) {  // largest i <= 1023 with cy[i] <= edge
       int mid = (lo + hi + 1) >> 1;
       if (cy[mid] <= edge) lo = mid;
       else hi = mid - 1;
     }
-    std::memcpy(h + 3074 + b, &lo, sizeof(int));
+    first[b] = lo;
+  }
+  first[kBuieBuckets] = std::min(first[kBuieBuckets - 1] + 1, 1023);
+  // the values of bucket b lie below bucket b + 1's smallest, so their
+  // intervals run from first[b] to first[b + 1]: at most one step apart; the
+  // last bucket's values lie below core, in intervals up to 1023
+  for (int b = 0; b + 1 < kBuieBuckets; ++b)
+    if (first[b + 1] - first[b] > 1) return false;
+  if (first[kBuieBuckets - 1] < 1022) return false;
+  t->host.resize(4 * (size_t)kBuieRecords);
+  for (int b = 0; b < kBuieRecords; ++b) {
+    const int i = first[b];
+    float* r = t->host.data() + 4 * b;
+    r[0] = cx[i];
+    r[1] = cy[i];
+    r[2] = sl[i];
+    r[3] = i < 1023 ? cy[i + 1] : HUGE_VALF;  // the last interval is never left
   }
   t->inv_bucket = inv_bucket;
   t->csr = csr;
   // the largest angle the sampler returns: the aureole's end (u -> 1) or the
   // core's last node, computed as the kernel computes it, plus rounding
-  const double core_max = h[1024];
+  const double core_max = cx[1024];
   const double aur_max = std::pow((double)(t->params[3] - t->params[2]) * t->params[4] + t->params[5],
                                   1.0 / ((double)t->params[1] + 1.0));
   t->within_alpha = std::max(core_max, aur_max) * 1e-3 * (1.0 + 1e-5) <= kSunAlphaMax;
+  return true;
 }
 
 static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
   if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   if (s->buie.csr == csr) return QMCRT_OK;
-  buie_with_guide(csr, &s->buie);
+  if (!buie_with_guide(csr, &s->buie))
+    return set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
   QM_CUDA(cudaMemcpyAsync(s->d_buie, s->buie.host.data(), s->buie.host.size() * sizeof(float),
                           cudaMemcpyHostToDevice, st));
   return QMCRT_OK;

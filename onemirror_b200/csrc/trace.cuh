@@ -6,11 +6,11 @@
 
 #include "../../include/qmcrt.h"
 #include "common.cuh"
+#include "internal.hpp"
 
 namespace qm {
 
 constexpr int kTraceThreads = 256;
-constexpr int kBuieBuckets = 1024;  // guide-table buckets over the core CDF
 constexpr int kChunkBlocks = 16;    // rays per CTA chunk = kChunkBlocks x blockDim
 constexpr int kPolyAtanCols = 32768;  // widest cylinder map the polynomial column estimate serves
 
@@ -112,17 +112,20 @@ __device__ __forceinline__ int max_less_index(const float* cdf_y, float value) {
 
 // Inverse CDF of the Buie sunshape (linear_interpolate, :115-137).  mrad.
 // The interval index equals max_less_index's (the largest i with
-// cdf_y[i] <= uu): a guide table over uniform buckets of [0, core) gives a
-// lower bound, then a short forward scan finishes.
-// The table is staged as one 16-byte record per interval, {angle, cdf,
-// slope, next interval's cdf}: each step of the scan is one shared load.
-__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float4* s_tab, const int* s_guide, float u) {
+// cdf_y[i] <= uu, at most 1023).  The table is staged per uniform bucket of
+// [0, core): record b is {angle, cdf, slope, next interval's cdf} of the
+// interval holding the bucket's smallest value.  A bucket holds at most one
+// interval boundary, and past it lies the interval of record b + 1, so one
+// compare picks between two records loaded together: no guide lookup, no
+// scan and no branch (68.8 G rays/s on the mid field with record b + 1
+// loaded only when needed, 69.2 G with both loaded; 67.6 G with the guide
+// table and scan this replaced).
+__device__ __forceinline__ float buie_theta_mrad(const TraceArgs& a, const float4* s_tab, float u) {
   float uu = u * a.b_total;
   if (uu < a.b_core) {
-    int b = min((int)(uu * a.b_inv_bucket), kBuieBuckets - 1);
-    int id = s_guide[b];
-    float4 q = s_tab[id];
-    while (id < 1023 && q.w <= uu) q = s_tab[++id];
+    const int b = min((int)(uu * a.b_inv_bucket), kBuieBuckets - 1);
+    const float4 q0 = s_tab[b], q1 = s_tab[b + 1];
+    const float4 q = uu >= q0.w ? q1 : q0;
     return (uu - q.y) * q.z + q.x;
   }
   // the aureole's analytic inverse (a few percent of the rays, but a warp
@@ -445,10 +448,9 @@ struct GlobalDeposit {
 // Load the Buie table and its guide into shared memory (all threads): the
 // table (angles [1025], cdf [1025], slopes [1024]) as one {angle, cdf, slope,
 // next cdf} record per interval.
-__device__ __forceinline__ void load_buie(const float* buie, float4* s_tab, int* s_guide) {
-  for (int i = threadIdx.x; i < 1024; i += blockDim.x)
-    s_tab[i] = make_float4(__ldg(buie + i), __ldg(buie + 1025 + i), __ldg(buie + 2050 + i), __ldg(buie + 1026 + i));
-  for (int i = threadIdx.x; i < kBuieBuckets; i += blockDim.x) s_guide[i] = __float_as_int(__ldg(buie + 3074 + i));
+__device__ __forceinline__ void load_buie(const float* buie, float4* s_tab) {
+  const float4* rec = reinterpret_cast<const float4*>(buie);  // kBuieRecords 16-byte records
+  for (int i = threadIdx.x; i < kBuieRecords; i += blockDim.x) s_tab[i] = __ldg(rec + i);
 }
 
 // Everything a ray needs before its traversals: heliostat, local point,
@@ -504,15 +506,15 @@ __device__ __forceinline__ void sample_dirs(uint4 r, float th_mrad, float sigma,
 // Gaussian (Box-Muller), phi uniform (set_samplelights, set_perturbation).
 // rk: the seed's Philox round keys (a.rk, or a copy the caller holds in
 // faster memory).
-__device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
+__device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4* s_tab, uint32_t ray,
                                                float sigma, float3* sl, float3* tl, const uint2* rk) {
   const uint4 r = ray_block(a, ray, rk);
-  sample_dirs(r, buie_theta_mrad(a, s_tab, s_guide, u23f(r.x)), sigma, sl, tl);
+  sample_dirs(r, buie_theta_mrad(a, s_tab, u23f(r.x)), sigma, sl, tl);
 }
 
 // Returns false for a ray to skip (table mode with an out-of-range heliostat id).
 template <bool TABLES>
-__device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
+__device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_tab, uint32_t ray,
                                           RaySetup& R, const uint2* rk) {
   const uint32_t g = a.rpp_shift >= 0 ? a.g_hi + (ray >> a.rpp_shift) : ray / (uint32_t)a.rpp;
   const uint32_t j = ray - g * (uint32_t)a.rpp;  // table mode (ray_hi 0)
@@ -559,7 +561,7 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
     R.sl = f3(__ldg(a.sun_local + 3 * ia), __ldg(a.sun_local + 3 * ia + 1), __ldg(a.sun_local + 3 * ia + 2));
     R.tl = f3(__ldg(a.turb_local + 3 * ib), __ldg(a.turb_local + 3 * ib + 1), __ldg(a.turb_local + 3 * ib + 2));
   } else {
-    philox_samples(a, s_tab, s_guide, ray, sigma_h, &R.sl, &R.tl, rk);
+    philox_samples(a, s_tab, ray, sigma_h, &R.sl, &R.tl, rk);
   }
   // world sample (local2world(sample, sun_dir)), incident direction
   const float3 sl = R.sl;
@@ -573,11 +575,11 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
 // of a two-level grid, 3 the per-heliostat occluder candidates (Philox
 // sampling only: their cones bound the sampler's directions).
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep>
-__device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_tab, const int* s_guide, uint32_t ray,
+__device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_tab, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit,
                                           const uint2* rk) {
   RaySetup R;
-  if (!ray_setup<TABLES>(a, s_tab, s_guide, ray, R, rk)) {
+  if (!ray_setup<TABLES>(a, s_tab, ray, R, rk)) {
     if (RECORDS) {
       if (a.flags) a.flags[ray] = 0;
       if (a.pixel) a.pixel[ray] = -1;
@@ -639,11 +641,10 @@ __device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned lo
 // The plain tracer: one grid-stride pass over the rays of one trace.
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
-  __shared__ float4 s_tab[1024];
-  __shared__ int s_guide[kBuieBuckets];
+  __shared__ float4 s_tab[kBuieRecords];
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   if (!TABLES) {
-    load_buie(a.buie, s_tab, s_guide);
+    load_buie(a.buie, s_tab);
     __syncthreads();
   }
   RayCounters c;
@@ -659,7 +660,7 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
     const uint64_t b64 = a.ray0 + ch * chunk;
     const uint32_t base = (uint32_t)b64, len = (uint32_t)(min(b64 + chunk, a.rays) - b64);
     for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
-      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, s_guide, base + j, fy0, fy1, c, dep, a.rk);
+      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, base + j, fy0, fy1, c, dep, a.rk);
   }
   if (STATS) flush_counters(c, a.stats);
 }

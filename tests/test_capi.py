@@ -75,6 +75,26 @@ def test_buie_table_is_the_oracles_bit_for_bit(csr):
     assert abs(x[-1] - 4.65) < 1e-4 and p[3] > p[2] > 0
 
 
+@pytest.mark.parametrize("csr", [0.01, 0.1, 0.5, 0.9])
+def test_buie_buckets_hold_one_interval_boundary_at_most(csr):
+    """The tracer looks the Buie inverse CDF up through 2048 uniform buckets
+    of [0, core): record b is the interval of the bucket's smallest value, and
+    record b + 1 the next one, which is right as long as no bucket holds two
+    interval boundaries.  A boundary y_k lies in bucket int(y_k * 2048 / core)
+    (the kernel's float multiply).  The library refuses to build a table that
+    breaks this; the core table does not depend on csr."""
+    x = np.zeros(1025, np.float32)
+    y = np.zeros(1025, np.float32)
+    s = np.zeros(1024, np.float32)
+    p = np.zeros(6, np.float32)
+    capi.check(capi.lib().qmcrt_buie_table(C.c_float(csr), capi.as_fp(x), capi.as_fp(y), capi.as_fp(s), capi.as_fp(p)))
+    inv = np.float32(2048) / p[2]
+    buckets = (y[1:1024] * inv).astype(np.float32).astype(np.int64)
+    assert len(np.unique(buckets)) == len(buckets)
+    # the narrowest interval is the last one, 0.88 buckets wide
+    assert np.diff(y.astype(np.float64)).min() * inv > 0.8
+
+
 def test_buie_rejects_bad_csr():
     a = np.zeros(1025, np.float32)
     b = np.zeros(1024, np.float32)
