@@ -600,6 +600,11 @@ qmcrt_status qmcrt_philox_blocks(const uint32_t ctr0[4], const uint32_t key[2], 
  * (test hook): d_rcp[i] = 1/x, d_rsqrt[i] = 1/sqrt(x); either may be NULL. */
 qmcrt_status qmcrt_fp64_recip_probe(const double* d_x, int64_t n, double* d_rcp, double* d_rsqrt, void* stream);
 
+/* The tracer's Buie inverse CDF (the sun sample's polar angle, mrad) on n
+ * device uniforms in [0, 1) (test hook): the table of `csr` staged and
+ * looked up as the trace kernels do.  Synchronises. */
+qmcrt_status qmcrt_buie_sample_probe(float csr, const float* d_u, int64_t n, float* d_theta_mrad, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

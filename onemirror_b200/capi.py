@@ -170,6 +170,7 @@ PROTOTYPES = {
     "qmcrt_adjoint_replay": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "qmcrt_tape_loss": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "qmcrt_tape_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "qmcrt_buie_sample_probe": (C.c_int, [C.c_float, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "qmcrt_adjoint_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                      C.c_void_p]),
     "qmcrt_tape_free": (C.c_int, [C.c_void_p]),

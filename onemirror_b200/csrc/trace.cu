@@ -166,6 +166,17 @@ bool buie_with_guide(float csr, BuieTable* t) {
   return true;
 }
 
+// The tracer's Buie inverse CDF on caller-provided uniforms (test hook,
+// qmcrt_buie_sample_probe): the shared-memory staging and lookup of the
+// trace kernels, reading only the sampler's scalars of `a`.
+__global__ void buie_probe_kernel(const TraceArgs a, const float* u, int64_t n, float* theta) {
+  __shared__ float4 s_tab[kBuieRecords];
+  load_buie(a.buie, s_tab);
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    theta[i] = buie_theta_mrad(a, s_tab, u[i]);
+}
+
 static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
   if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   if (s->buie.csr == csr) return QMCRT_OK;
@@ -460,6 +471,35 @@ qmcrt_status qmcrt_trace_host(qmcrt_scene* s, const qmcrt_field* field, const qm
   if (h_counts) QM_CUDA(cudaMemcpyAsync(h_counts, s->d_counts, res * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   if (h_flux) QM_CUDA(cudaMemcpyAsync(h_flux, s->d_energy, res * sizeof(float), cudaMemcpyDeviceToHost, st));
   QM_CUDA(cudaStreamSynchronize(st));
+  return QMCRT_OK;
+}
+
+qmcrt_status qmcrt_buie_sample_probe(float csr, const float* d_u, int64_t n, float* d_theta_mrad, void* stream) {
+  if (!d_u || !d_theta_mrad || n <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
+  BuieTable t;
+  if (!buie_with_guide(csr, &t)) return set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
+  cudaStream_t st = (cudaStream_t)stream;
+  TraceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.b_total = t.params[3];
+  a.b_core = t.params[2];
+  a.b_B = t.params[4];
+  a.b_C = t.params[5];
+  a.b_inv = 1 / (t.params[1] + 1);
+  a.b_inv_bucket = t.inv_bucket;
+  float* d_tab = nullptr;
+  QM_CUDA(cudaMalloc(&d_tab, t.host.size() * sizeof(float)));
+  a.buie = d_tab;
+  cudaError_t ce = cudaMemcpyAsync(d_tab, t.host.data(), t.host.size() * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess) {
+    buie_probe_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4 * sm_count()), 256, 0, st>>>(a, d_u, n,
+                                                                                                   d_theta_mrad);
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  cudaFree(d_tab);
+  if (ce != cudaSuccess) return cuda_error(ce, "Buie sample probe");
   return QMCRT_OK;
 }
 

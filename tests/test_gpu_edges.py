@@ -258,6 +258,51 @@ def test_fp64_reciprocals_within_bound():
     assert np.max(np.abs(q * np.sqrt(x[pos]) - 1.0)) < 3e-12
 
 
+@pytest.mark.parametrize("csr", [0.05, 0.2])
+def test_buie_bucket_lookup_equals_max_less_index(csr):
+    """The tracer's Buie inverse CDF (2048 uniform buckets, one interval
+    record each, the record of the next bucket past a boundary) against the
+    reference's search, max_less_index (scene_instance_process.cu:98-113),
+    and linear interpolation (:115-137) in float32: uniforms at random, at
+    every interval boundary and bucket edge (mapped back through the
+    kernel's float multiply) and their neighbours a few ulps away.  The
+    interval must be the reference's for every value of the core; the angle
+    is then the same float computation (one fused multiply-add), so equal to
+    the expected value within one ulp (a float64 stand-in for the fused
+    operation can round once more)."""
+    x = np.zeros(1025, np.float32)
+    y = np.zeros(1025, np.float32)
+    sl = np.zeros(1024, np.float32)
+    p = np.zeros(6, np.float32)
+    capi.check(capi.lib().qmcrt_buie_table(C.c_float(csr), capi.as_fp(x), capi.as_fp(y), capi.as_fp(sl), capi.as_fp(p)))
+    core, total = np.float32(p[2]), np.float32(p[3])
+    inv = np.float32(2048) / core
+    rng = np.random.default_rng(3)
+    marks = np.concatenate([y[1:1024], np.arange(1, 2048, dtype=np.float32) / inv]).astype(np.float32)
+    u0 = (marks / total).astype(np.float32)
+    up, down = [u0], [u0]
+    for _ in range(3):  # 1 to 3 ulps either side
+        up.append(np.nextafter(up[-1], np.float32(1)))
+        down.append(np.nextafter(down[-1], np.float32(0)))
+    u = np.concatenate([rng.random(1 << 20, dtype=np.float32)] + up + down[1:]).astype(np.float32)
+    u = u[(u >= 0) & (u < 1)]
+    du = torch.as_tensor(u, device="cuda")
+    th = torch.empty_like(du)
+    capi.check(capi.lib().qmcrt_buie_sample_probe(C.c_float(csr), C.c_void_p(du.data_ptr()), du.numel(),
+                                                  C.c_void_p(th.data_ptr()), None))
+    g = th.cpu().numpy()
+    uu = (u * total).astype(np.float32)
+    core_ = uu < core
+    uu, g = uu[core_], g[core_]
+    assert uu.size > (1 << 19)
+    idx = np.minimum(np.searchsorted(y, uu, side="right") - 1, 1023)  # largest i <= 1023 with y[i] <= uu
+    d = (uu - y[idx]).astype(np.float32)
+    want = (d.astype(np.float64) * sl[idx].astype(np.float64) + x[idx].astype(np.float64)).astype(np.float32)
+    ulp = np.spacing(np.abs(want))
+    assert np.all(np.abs(g - want) <= ulp), np.max(np.abs(g - want) / ulp)
+    assert np.mean(g == want) > 0.999
+
+
 def test_ray_range_traces_the_same_rays():
     """qmcrt_trace_params.ray_begin/ray_end: one heliostat's rays (one range,
     as the reference launches them) give the whole trace's flags and pixels
