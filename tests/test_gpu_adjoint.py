@@ -167,6 +167,12 @@ def test_ray_ranges_compose_to_the_full_adjoint(case):
         gs = gs + np.concatenate([ga.cpu().numpy(), gt.cpu().numpy()], 1)
         SolarScene.tape_free(tape)
     assert np.allclose(gs, g, rtol=1e-4, atol=1e-5 * np.abs(g).max())
+    # the same step through dist.adjoint_step in one process (no exchange)
+    tape, l1, f1, ga, gt = D.adjoint_step(sc, w.sun, w.params, target)
+    SolarScene.tape_free(tape)
+    assert abs(l1 - loss) <= 1e-6 * loss
+    g1 = np.concatenate([ga.cpu().numpy(), gt.cpu().numpy()], 1)
+    assert np.allclose(g1, g, rtol=1e-4, atol=1e-5 * np.abs(g).max())
     # a range past the trace's last ray, or an empty one, is refused
     for b, e in ((RAYS, RAYS + 1), (5, 5)):
         p = type(w.params).from_buffer_copy(w.params)
