@@ -43,6 +43,21 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(capi.PROTOTYPES)
 
 
+def test_argument_errors_need_no_gpu():
+    """Entry points refuse NULL and out-of-range arguments with a status and a
+    message before touching the device (these run on a machine without one)."""
+    L = capi.lib()
+    assert L.qmcrt_tape_energy(None, None, None) == capi.ERR_INVALID_ARGUMENT
+    assert L.qmcrt_adjoint_loss(None, None, None, None, None, None) == capi.ERR_INVALID_ARGUMENT
+    assert L.qmcrt_adjoint_replay(None, None, None, None, None) == capi.ERR_INVALID_ARGUMENT
+    assert L.qmcrt_adjoint_backward(None, None, None, None) == capi.ERR_INVALID_ARGUMENT
+    assert L.qmcrt_buie_sample_probe(C.c_float(0.1), None, 16, None, None) == capi.ERR_INVALID_ARGUMENT
+    dummy = C.c_void_p(16)  # never dereferenced: the csr check comes first
+    assert L.qmcrt_buie_sample_probe(C.c_float(1.5), dummy, 16, dummy, None) == capi.ERR_INVALID_ARGUMENT
+    assert b"csr" in L.qmcrt_last_error()
+    assert L.qmcrt_buie_sample_probe(C.c_float(0.1), dummy, 0, dummy, None) == capi.ERR_INVALID_ARGUMENT
+
+
 def test_version_and_status_strings():
     L = capi.lib()
     assert b"sm_100a" in L.qmcrt_version()
