@@ -127,6 +127,9 @@ struct AdjArgs {
   TraceArgs t;
   int tile, tile_r0, tile_c0;  // forward: block-private tile of tile x tile pixels at (row r0, col c0); 0: none
   double ew[3], eh[3];  // receiver width / height unit axes (flat receivers)
+  // backward: the receiver edges and the sun direction in float, read from
+  // the parameter space where they are used (no registers held across the ray loop)
+  float e1f[3], e2f[3], sdf[3];
   uint8_t* tape;        // one visibility byte per ray
   unsigned long long* energy_fx;  // replay: the energy map in 2^-40 fixed point (exact sums in any order)
   uint64_t saved;       // rays with a byte in the tape
@@ -367,8 +370,11 @@ __device__ __forceinline__ float3 fma3(float s, float3 a, float3 b) { return f3(
 
 // RECOMPUTE: the tape holds fewer rays than the trace (state_bytes_max), and
 // the rays past it walk again for their visibility; without it the walks
-// are compiled out (fewer live registers: 116 B of spills instead of 144 B,
-// backward 1.32 -> 1.27 ms on the differentiable field).
+// are compiled out.  Register pressure at the 64-register cap, measured on
+// the differentiable field: 144 B of spills and 1.32 ms with the walks
+// compiled in, 116 B and 1.27 ms without, 56 B and 1.21 ms once the
+// receiver edges and sun direction are read in float from the parameter
+// space instead of held in registers across the ray loop.
 template <bool CULL, bool RECOMPUTE>
 __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_backward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[kBuieRecords];
@@ -376,9 +382,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_backward_k
   load_buie(a.buie, s_tab);
   __syncthreads();
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
-  const float3 E1 = f3((float)a.rE1[0], (float)a.rE1[1], (float)a.rE1[2]);
-  const float3 E2 = f3((float)a.rE2[0], (float)a.rE2[1], (float)a.rE2[2]);
-  const float3 sd = f3((float)a.sdir[0], (float)a.sdir[1], (float)a.sdir[2]);
+
   // Each warp takes segments of 256 consecutive rays (grid-stride over all
   // warps) and works only on the rays that contribute: those the tape marks
   // as hits, and every ray past the saved part of the tape (their visibility
@@ -456,6 +460,8 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_backward_k
         // the tangents are FP32: reciprocals to ~1e-12 (and 2 ulp below) suffice
         const float ilnp = (float)rcp_nr(g.lnp), ilr = (float)rcp_nr(g.lr);
         const float nws = dot(npf, wsf);
+        const float3 sd = f3(A.sdf[0], A.sdf[1], A.sdf[2]);
+        const float3 E1 = f3(A.e1f[0], A.e1f[1], A.e1f[2]), E2 = f3(A.e2f[0], A.e2f[1], A.e2f[2]);
         const float sdn = dot(sd, npf);
         const float e = fabsf(sdn) * R.w, sg = sdn < 0.f ? -1.f : 1.f;
         // t along the reflected ray to the receiver plane (for d(hit) = do + t dr)
@@ -740,6 +746,11 @@ qmcrt_status qmcrt_adjoint_backward(qmcrt_tape* t, float* d_grad_aim, float* d_g
   AdjArgs A = tape_args(t);
   A.grad_aim = d_grad_aim;
   A.grad_tilt = d_grad_tilt;
+  for (int i = 0; i < 3; ++i) {
+    A.e1f[i] = (float)A.t.rE1[i];
+    A.e2f[i] = (float)A.t.rE2[i];
+    A.sdf[i] = (float)A.t.sdir[i];
+  }
   JacArgs j{};
   j.n = s->n;
   j.pos = s->d_pos;
