@@ -140,34 +140,32 @@ struct AdjArgs {
 };
 
 // Receiver hit with the continuous (u, v) (flat receivers): along E1 (rows)
-// and E2 (columns), each in [0, 1]; t along the ray.
+// and E2 (columns), each in [0, 1]; t along the ray.  The plane form of the
+// tracer's receiver_hit: t = ((A - o) . N) / (d . N) and the dual-edge
+// coordinates of the hit's offset from A.
 __device__ __forceinline__ bool receiver_uv(const TraceArgs& a, d3 o, d3 d, double* u, double* v, double* t) {
-  d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
-  d3 pv = cross(d, E2);
-  double det = dot(E1, pv);
-  if (fabs(det) < 1e-6) return false;
-  double inv = rcp_nr(det);
-  d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
-  *u = dot(T, pv) * inv;
+  const d3 N = mk(a.rN[0], a.rN[1], a.rN[2]);
+  const double dn = dot(d, N);
+  if (fabs(dn) < 1e-6) return false;
+  const d3 ao = mk(a.rA[0], a.rA[1], a.rA[2]) - o;
+  *t = dot(ao, N) * rcp_nr(dn);
+  if (*t < 1e-6) return false;
+  const d3 w = *t * d - ao;  // hit - A
+  *u = dot(w, mk(a.rD1[0], a.rD1[1], a.rD1[2]));
   if (*u < 0 || *u > 1) return false;
-  d3 qv = cross(T, E1);
-  *v = dot(d, qv) * inv;
-  if (*v < 0 || *v > 1) return false;
-  *t = dot(E2, qv) * inv;
-  return *t >= 1e-6;
+  *v = dot(w, mk(a.rD2[0], a.rD2[1], a.rD2[2]));
+  return *v >= 0 && *v <= 1;
 }
 
 // The receiver plane's (u, v) of the line o + t d, without the range tests:
 // the same arithmetic as receiver_uv.  The replayed forward pass deposits a
 // ray the tape marks as a hit wherever its (u, v) now falls.
 __device__ __forceinline__ void receiver_plane_uv(const TraceArgs& a, d3 o, d3 d, double* u, double* v) {
-  d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
-  d3 pv = cross(d, E2);
-  double inv = rcp_nr(dot(E1, pv));
-  d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
-  *u = dot(T, pv) * inv;
-  d3 qv = cross(T, E1);
-  *v = dot(d, qv) * inv;
+  const d3 N = mk(a.rN[0], a.rN[1], a.rN[2]);
+  const d3 ao = mk(a.rA[0], a.rA[1], a.rA[2]) - o;
+  const d3 w = (dot(ao, N) * rcp_nr(dot(d, N))) * d - ao;
+  *u = dot(w, mk(a.rD1[0], a.rD1[1], a.rD1[2]));
+  *v = dot(w, mk(a.rD2[0], a.rD2[1], a.rD2[2]));
 }
 
 // Reflection geometry of one ray: the perturbed unit normal and reflected

@@ -251,6 +251,22 @@ void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, u
     a->rE1[i] = s->rg.v1[i] - s->rg.v0[i];
     a->rE2[i] = s->rg.v3[i] - s->rg.v0[i];
   }
+  {
+    const double* E1 = a->rE1;
+    const double* E2 = a->rE2;
+    double* N = a->rN;
+    N[0] = E1[1] * E2[2] - E1[2] * E2[1];
+    N[1] = E1[2] * E2[0] - E1[0] * E2[2];
+    N[2] = E1[0] * E2[1] - E1[1] * E2[0];
+    const double nn = N[0] * N[0] + N[1] * N[1] + N[2] * N[2];
+    const double inn = nn > 0 ? 1.0 / nn : 0.0;
+    a->rD1[0] = (E2[1] * N[2] - E2[2] * N[1]) * inn;
+    a->rD1[1] = (E2[2] * N[0] - E2[0] * N[2]) * inn;
+    a->rD1[2] = (E2[0] * N[1] - E2[1] * N[0]) * inn;
+    a->rD2[0] = (N[1] * E1[2] - N[2] * E1[1]) * inn;
+    a->rD2[1] = (N[2] * E1[0] - N[0] * E1[2]) * inn;
+    a->rD2[2] = (N[0] * E1[1] - N[1] * E1[0]) * inn;
+  }
   for (int i = 0; i < 5; ++i) a->cyl[i] = s->rg.cyl[i];
   a->cyl[5] = s->rg.cyl[4] > 0 ? 1.0 / s->rg.cyl[4] : 0.0;
   a->cyl_edge = s->d_cyl_edge;

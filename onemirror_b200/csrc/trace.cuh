@@ -17,7 +17,7 @@ constexpr int kPolyAtanCols = 32768;  // widest cylinder map the polynomial colu
 struct TraceArgs {
   // sun: frame of local2world for the sun direction, and the direction
   double su[3], sn[3], sv[3], sdir[3];
-  // Buie table in global memory (cdf_x | cdf_y | slope | guide as int) and its scalars
+  // Buie table in global memory (kBuieRecords records, one per bucket) and its scalars
   const float* buie;
   float b_total, b_core, b_B, b_C, b_inv, b_inv_bucket;
   // field
@@ -54,6 +54,10 @@ struct TraceArgs {
   // receiver
   int rtype;
   double rA[3], rE1[3], rE2[3];
+  // flat receiver as a plane: N = E1 x E2, and the dual edges D1 = (E2 x N) / |N|^2,
+  // D2 = (N x E1) / |N|^2, so that w . D1 and w . D2 are the E1 and E2 coordinates
+  // of an in-plane offset w
+  double rN[3], rD1[3], rD2[3];
   double cyl[6];  // cylinder: bottom centre x, y, z, radius, height, 1 / height
   const double2* cyl_edge;  // cylinder: [res_x] (cos, sin) of each column's first edge, 2 pi k / res_x
   int res_x, res_y;
@@ -396,19 +400,20 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
     }
     col = c;
   } else {
-    d3 E1 = mk(a.rE1[0], a.rE1[1], a.rE1[2]), E2 = mk(a.rE2[0], a.rE2[1], a.rE2[2]);
-    d3 pv = cross(d, E2);
-    double det = dot(E1, pv);
-    if (fabs(det) < 1e-6) return false;
-    double inv = rcp_nr(det);
-    d3 T = o - mk(a.rA[0], a.rA[1], a.rA[2]);
-    u = dot(T, pv) * inv;
-    if (u < 0 || u > 1) return false;
-    d3 qv = cross(T, E1);
-    v = dot(d, qv) * inv;
-    if (v < 0 || v > 1) return false;
-    double t = dot(E2, qv) * inv;
+    // the parallelogram test of rayParallelogramIntersect (global_function.cuh:78-105)
+    // in plane form: its determinant E1 . (d x E2) is -d . N, t = ((A - o) . N) / (d . N),
+    // and (u, v) are the dual-edge coordinates of the hit's offset from A
+    const d3 N = mk(a.rN[0], a.rN[1], a.rN[2]);
+    const double dn = dot(d, N);
+    if (fabs(dn) < 1e-6) return false;
+    const d3 ao = mk(a.rA[0], a.rA[1], a.rA[2]) - o;
+    const double t = dot(ao, N) * rcp_nr(dn);
     if (t < 1e-6) return false;
+    const d3 w = t * d - ao;  // hit - A
+    u = dot(w, mk(a.rD1[0], a.rD1[1], a.rD1[2]));
+    if (u < 0 || u > 1) return false;
+    v = dot(w, mk(a.rD2[0], a.rD2[1], a.rD2[2]));
+    if (v < 0 || v > 1) return false;
     if (t_out) *t_out = t;
   }
   int row = (int)(u * a.res_y);  // rectgrid_raytracing.cu:144
