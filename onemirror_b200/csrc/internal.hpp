@@ -72,6 +72,11 @@ struct CandBuckets {
   double rmax;         // largest bounding radius (half-diagonal + 1 cm)
 };
 
+// The grid's cell-count scan: one CTA up to kScanOneCtaMax cells, above that
+// tiles of kScanTile cells, one CTA each.
+constexpr int64_t kScanOneCtaMax = 65536;
+constexpr int kScanTile = 4096;
+
 struct SunGeom {
   double* normal = nullptr;      // [3n]
   double* frame = nullptr;       // [kFrameStride n] u, n, v, mirror centre
@@ -83,6 +88,7 @@ struct SunGeom {
   float4* cell_rect = nullptr;   // [3*entry_cap]
   int4* cell_info = nullptr;     // [cells] first, end, ylo bits, yhi bits
   float2* coarse_yr = nullptr;   // [coarse_cells] two-level grid only
+  int64_t* scan_part = nullptr;  // [cells / kScanTile] tile totals of the multi-CTA scan (large grids only)
   float4* cand = nullptr;        // [n][2][kCandCap][3] rectangle records of each heliostat's shadow / block candidates
   int* cand_n = nullptr;         // [n][2] their counts (> kCandCap: too many, the rays walk the grid)
   int* field_yr = nullptr;       // [2]
@@ -149,6 +155,7 @@ struct qmcrt_scene {
   float4* d_cell_rect = nullptr;    // [3*entry_cap] cell-major rectangle records
   int4* d_cell_info = nullptr;      // [cells] run of each cell's rectangles and their height range
   float2* d_coarse_yr = nullptr;    // [coarse_cells] the same per coarse cell (two-level grid)
+  int64_t* d_scan_part = nullptr;   // [cells / kScanTile] tile totals of the multi-CTA scan (large grids only)
   double2* d_cyl_edge = nullptr;    // cylinder receivers: [res_x] direction of each column's first edge
   float4* d_cand = nullptr;         // [n][2][kCandCap][3] occluder candidates' rectangle records (shadow, block)
   int* d_cand_n = nullptr;          // [n][2]

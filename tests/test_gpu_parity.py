@@ -142,6 +142,26 @@ def test_geometry_and_grid_equal_oracle(small, quirks):
     assert np.array_equal(ent, ref.entries[: start[-1]])
 
 
+@pytest.mark.parametrize("name", ["mid", "large"])
+def test_big_field_grids_equal_oracle(name):
+    """The grid CSR of the mid field (one CTA scans its cell counts) and of
+    the large field's 12.5 m fine level (more than 65 536 cells: tiles of
+    4096 cells, one CTA each, then the tiles' offsets) against the oracle's
+    grid over the same bounds."""
+    w = W.BUILDERS[name](rays=1 << 20)
+    sc = SolarScene.from_workload(w)
+    sc.set_sun(w.sun, 0)
+    gi = sc.grid_info()
+    cells = int(np.prod(list(gi.dims)))
+    assert (cells > 65536) == (name == "large"), cells
+    ref = oracle_scene(w, sc, w.sun, 0, use_gpu_grid=False)
+    start, ent = sc.read_grid()
+    assert start.size == cells + 1
+    assert np.array_equal(start, ref.cell_start)
+    assert np.array_equal(ent, ref.entries[: start[-1]])
+    sc.close()
+
+
 def run_pair(w, sc, sun, params, quirks=0):
     params.quirks = quirks
     g = sc.trace(sun, params, records=True)
