@@ -76,6 +76,7 @@ struct CandBuckets {
 // tiles of kScanTile cells, one CTA each.
 constexpr int64_t kScanOneCtaMax = 65536;
 constexpr int kScanTile = 4096;
+constexpr int64_t kCellWarpMax = 16384;  // grids up to this many cells finish with a warp per cell
 
 struct SunGeom {
   double* normal = nullptr;      // [3n]

@@ -276,6 +276,40 @@ __device__ __forceinline__ int ordered(float f) {
 // record {first, end, ylo, yhi}: its run of rectangles and their height range
 // (for the traversal's vertical culling; one 16-byte load per DDA step), and
 // the height range of the whole field.
+// One thread per cell (large grids, most of whose cells are empty): the
+// cell's ids sorted in place by insertion, then as the warp-per-cell kernel
+// below.
+__global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t* entries,
+                                   const float4* rect, float4* cell_rect, int4* cell_info, int* field_yr) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  int b = start[c], e = start[c + 1];
+  for (int i = b + 1; i < e; ++i) {
+    int v = entries[i], j = i - 1;
+    while (j >= b && entries[j] > v) {
+      entries[j + 1] = entries[j];
+      --j;
+    }
+    entries[j + 1] = v;
+  }
+  float ylo = 3.0e38f, yhi = -3.0e38f;
+  for (int i = b; i < e; ++i) {
+    int h = entries[i];
+    float4 r0 = rect[3 * h], r1 = rect[3 * h + 1], r2 = rect[3 * h + 2];
+    cell_rect[3 * (int64_t)i] = r0;
+    cell_rect[3 * (int64_t)i + 1] = r1;
+    cell_rect[3 * (int64_t)i + 2] = r2;
+    float y0 = r0.y, y1 = r0.y + r1.y, y2 = r0.y + r2.y, y3 = r0.y + r1.y + r2.y;
+    ylo = fminf(ylo, fminf(fminf(y0, y1), fminf(y2, y3)));
+    yhi = fmaxf(yhi, fmaxf(fmaxf(y0, y1), fmaxf(y2, y3)));
+  }
+  cell_info[c] = make_int4(b, e, __float_as_int(ylo), __float_as_int(yhi));
+  if (e > b) {
+    atomicMin(field_yr, ordered(ylo));
+    atomicMax(field_yr + 1, ordered(yhi));
+  }
+}
+
 // One warp per cell: the cell's heliostat ids in ascending order (the
 // reference's push_back order, grid.cpp:53-83), its cell-major rectangle
 // records, its 16-byte cell record {first, end, ylo, yhi} and the field's
@@ -284,7 +318,7 @@ __device__ __forceinline__ int ordered(float f) {
 // ids against all of the cell's ids (cached loads), the warp writes them in
 // order.  Larger cells (none in the bench's fields) sort on one lane.
 constexpr int kCellRankMax = 128;
-__global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t* entries,
+__global__ void cell_finish_warp_kernel(int64_t cells, const int32_t* start, int32_t* entries,
                                    const float4* rect, float4* cell_rect, int4* cell_info, int* field_yr) {
   const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -1143,8 +1177,15 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, g.cellbox, g.cell_start, g.cell_count, g.entries,
                                                   s->gdims[1], s->gdims[2], s->entry_cap);
   QM_CUDA(cudaGetLastError());
-  cell_finish_kernel<<<(unsigned)((s->cells + 7) / 8), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
-                                                                    g.cell_rect, g.cell_info, g.field_yr);  // a warp per cell
+  // a warp per cell on small grids (few cells, many ids each), a thread per
+  // cell on large ones (mostly empty cells): 13.2 -> 4.4 us on the small
+  // field, and 6.8 us instead of 77 us on the large field's 176 000 cells
+  if (s->cells <= kCellWarpMax)
+    cell_finish_warp_kernel<<<(unsigned)((s->cells + 7) / 8), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
+                                                                         g.cell_rect, g.cell_info, g.field_yr);
+  else
+    cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
+                                                                          g.cell_rect, g.cell_info, g.field_yr);
   QM_CUDA(cudaGetLastError());
   if (s->coarse_cells) {
     int3 cd = make_int3(s->gdims[0] / s->fine_div, s->gdims[1] / s->fine_div, s->gdims[2] / s->fine_div);
