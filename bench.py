@@ -464,12 +464,13 @@ class FieldRun:
         from onemirror_b200.scene import image_smooth
         return image_smooth(counts, self.w.smooth_radius, self.w.smooth_ratio, capi.TRIM_SORTED)
 
-    def step(self, k, item, want_stats=False):
+    def step(self, k, item, want_stats=False, sun=None):
         """Trace with a sun moved by 0.01 deg per step, exchange the maps
-        (N > 1), smooth the summed count map."""
+        (N > 1), smooth the summed count map.  `sun`: the step's sun, when
+        the caller has formed it already."""
         from onemirror_b200 import dist as D
         self.p.item = item
-        r = self.sc.trace(self.sun(k), self.p, stats=want_stats, outputs=self.outs)
+        r = self.sc.trace(sun if sun is not None else self.sun(k), self.p, stats=want_stats, outputs=self.outs)
         _, _, sm = D.step_maps(r["counts"], r["energy"], self.smooth)
         return r, sm
 
@@ -480,10 +481,15 @@ class FieldRun:
         from onemirror_b200 import dist as D
         step_ms, kern_ms, setup_ms = [], [], []
         for k in range(steps):
-            self.flush.zero_()
+            # the step's sun and events are formed before the flush, so that the
+            # host enqueues the step while the flush runs and the events time the
+            # step's device work, not the host's preparation of it (as when
+            # steps follow each other without a flush)
+            sun, item = self.sun(k0 + k), D.shard_item(self.rank, k)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            self.flush.zero_()
             e0.record()
-            self.step(k0 + k, D.shard_item(self.rank, k))
+            self.step(k0 + k, item, sun=sun)
             e1.record()
             t = self.sc.timing()
             kern_ms.append(t.trace_kernel_ms)
