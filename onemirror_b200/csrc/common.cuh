@@ -131,6 +131,24 @@ __device__ __forceinline__ float u23f(uint32_t w) {
   return __uint_as_float(0x3F800000u | (w & 0x7FFFFFu)) - 0x1.fffffep-1f;  // 1 - 2^-24
 }
 
+// Programmatic dependent launch (sm_90 and later): a kernel launched with
+// programmatic stream serialization may start while the kernel before it in
+// the stream finishes; pdl_wait() returns once that kernel has completed and
+// its writes are visible, so it comes before any memory access.  A kernel
+// launched without the attribute returns from it at once.  pdl_trigger()
+// lets the next kernel start launching once every block of this one has
+// passed it (it is implicit at a block's exit).
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void pdl_trigger() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
 // Occluder candidates kept per heliostat and walk direction.
 constexpr int kCandCap = 32;
 

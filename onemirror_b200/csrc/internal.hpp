@@ -31,6 +31,25 @@ struct ReceiverGeom {
 };
 
 // Buie sunshape table (1025 + 1025 + 1024 floats) and its scalars.
+// Launch `kernel` on `st`, with programmatic stream serialization when `pdl`
+// (the kernel then starts while its predecessor in the stream finishes, and
+// waits for it in pdl_wait()).
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? at : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Buie table staging: uniform buckets over the core CDF, each holding at
 // most one boundary of the table's 1024 intervals (checked when the table is
 // built), and one interval record per bucket plus one past the last.
@@ -200,16 +219,18 @@ SunGeom scene_geom(qmcrt_scene* s);
 // Allocate / free a SunGeom sized for scene s.
 qmcrt_status alloc_sun_geom(const qmcrt_scene* s, SunGeom* g);
 void free_sun_geom(SunGeom* g);
-// Enqueue aiming + grid build of scene s for the (normalised) sun direction into g.
+// Enqueue aiming + grid build of scene s for the (normalised) sun direction
+// into g.  pdl: launch the kernels with programmatic stream serialization
+// (each starts while the one before it finishes; not inside graph captures).
 qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
-                             cudaStream_t st);
+                             cudaStream_t st, bool pdl = false);
 qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
 // Per-point candidate masks of `points` points (xz, helio) for geometry g of
 // scene s and the (normalised) sun, into mask, and the points' world
 // coordinates (the rays' origins) into origin.
 qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
                                 const int32_t* helio, const float* weight, int64_t points, uint4* mask, double4* origin,
-                                cudaStream_t st);
+                                cudaStream_t st, bool pdl = false);
 // The scene's masks for its current sun and points (rebuilt when stale).
 qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st);
 }  // namespace qm

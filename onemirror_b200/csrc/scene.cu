@@ -56,6 +56,8 @@ __device__ __forceinline__ frame64 frame_of(d3 n, uint32_t quirks) {
 }
 
 __global__ void aim_kernel(AimArgs a) {
+  pdl_wait();
+  pdl_trigger();
   int h = blockIdx.x * blockDim.x + threadIdx.x;
   double pw = 0;
   if (h < a.n) {
@@ -136,6 +138,8 @@ __global__ void aim_kernel(AimArgs a) {
 // each scanning a contiguous run), then zero cell_count for the fill cursor.
 __global__ void __launch_bounds__(1024) scan_kernel(int32_t* count, int32_t* start, int64_t cells,
                                                     int64_t cap, int32_t* flag, int* field_yr) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ int64_t part[1024];
   const int t = threadIdx.x;
   if (t == 0) {  // empty height range for cell_finish_kernel's atomicMin/Max
@@ -173,6 +177,8 @@ __global__ void __launch_bounds__(1024) scan_kernel(int32_t* count, int32_t* sta
 // prefix into start and its total into part.
 __global__ void __launch_bounds__(1024) scan_tiles_kernel(const int32_t* count, int32_t* start, int64_t cells,
                                                           int64_t* part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ int64_t warp_sum[32];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int64_t b = (int64_t)blockIdx.x * kScanTile + 4 * t;
@@ -212,6 +218,8 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(const int32_t* count, 
 // the empty height range for cell_finish_kernel.
 __global__ void __launch_bounds__(1024) scan_parts_kernel(int64_t* part, int64_t tiles, int32_t* start,
                                                           int64_t cells, int64_t cap, int32_t* flag, int* field_yr) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ int64_t acc[1024];
   const int t = threadIdx.x;
   if (t == 0) {
@@ -244,6 +252,8 @@ __global__ void __launch_bounds__(1024) scan_parts_kernel(int64_t* part, int64_t
 // Pass 3: each cell's start = its tile's offset + its tile-local prefix
 // (clamped to the capacity); the count is zeroed for the fill cursor.
 __global__ void scan_add_kernel(int32_t* count, int32_t* start, int64_t cells, const int64_t* part, int64_t cap) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= cells) return;
   start[i] = (int32_t)min(part[i / kScanTile] + start[i], cap);
@@ -252,6 +262,8 @@ __global__ void scan_add_kernel(int32_t* count, int32_t* start, int64_t cells, c
 
 __global__ void fill_kernel(int n, const int4* cellbox, const int32_t* start, int32_t* cursor,
                             int32_t* entries, int gy, int gz, int64_t cap) {
+  pdl_wait();
+  pdl_trigger();
   int h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= n) return;
   int4 lo = cellbox[2 * h], hi = cellbox[2 * h + 1];
@@ -281,6 +293,8 @@ __device__ __forceinline__ int ordered(float f) {
 // below.
 __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t* entries,
                                    const float4* rect, float4* cell_rect, int4* cell_info, int* field_yr) {
+  pdl_wait();
+  pdl_trigger();
   int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= cells) return;
   int b = start[c], e = start[c + 1];
@@ -320,6 +334,8 @@ __global__ void cell_finish_kernel(int64_t cells, const int32_t* start, int32_t*
 constexpr int kCellRankMax = 128;
 __global__ void cell_finish_warp_kernel(int64_t cells, const int32_t* start, int32_t* entries,
                                    const float4* rect, float4* cell_rect, int4* cell_info, int* field_yr) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (c >= cells) return;  // whole warps leave together
@@ -380,6 +396,8 @@ __global__ void cell_finish_warp_kernel(int64_t cells, const int32_t* start, int
 // ranges of its div^3 fine cells (empty cells contribute nothing).
 __global__ void coarse_finish_kernel(int64_t coarse_cells, int div, int3 cdims, int gy, int gz, const int4* cell_info,
                                      float2* coarse_yr) {
+  pdl_wait();
+  pdl_trigger();
   int64_t cc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (cc >= coarse_cells) return;
   int cz = (int)(cc % cdims.z), cy = (int)((cc / cdims.z) % cdims.y), cx = (int)(cc / ((int64_t)cdims.z * cdims.y));
@@ -627,6 +645,8 @@ __device__ int cand_search(const CandArgs& a, const CandBuckets& B, int h, d3 ch
 // search, which finds the same set.
 template <bool EXHAUSTIVE>
 __global__ void __launch_bounds__(128) cand_kernel(CandArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (w >= 2 * a.n) return;  // w is uniform across the warp
   const int h = w >> 1, walk = w & 1;
@@ -703,6 +723,8 @@ __device__ bool point_reaches(d3 p, const float4* r, float3 d, float3 e1, float3
 }
 
 __global__ void __launch_bounds__(256) point_mask_kernel(MaskArgs a) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= a.points) return;
   const int h = a.point_helio[g];
@@ -996,7 +1018,7 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
   if (!(l > 0) || !std::isfinite(l)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "sun direction is zero or not finite");
   for (int i = 0; i < 3; ++i) sd[i] /= l;
   QM_CUDA(cudaEventRecord(s->ev[0], st));
-  qmcrt_status e = launch_sun_geom(s, scene_geom(s), sd, k.quirks, st);
+  qmcrt_status e = launch_sun_geom(s, scene_geom(s), sd, k.quirks, st, true);
   if (e) return e;
   QM_CUDA(cudaEventRecord(s->ev[1], st));
   s->setup_timed = true;
@@ -1008,7 +1030,7 @@ qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, c
 
 qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const double sun[3], const float2* xz,
                                 const int32_t* helio, const float* weight, int64_t points, uint4* mask,
-                                double4* origin, cudaStream_t st) {
+                                double4* origin, cudaStream_t st, bool pdl) {
   if (points <= 0) return QMCRT_OK;
   MaskArgs m{};
   m.points = points;
@@ -1025,8 +1047,7 @@ qmcrt_status launch_point_masks(const qmcrt_scene* s, const SunGeom& g, const do
   m.zmax = kSlopeZMax;
   m.mask = mask;
   m.origin = origin;
-  point_mask_kernel<<<(unsigned)((points + 255) / 256), 256, 0, st>>>(m);
-  QM_CUDA(cudaGetLastError());
+  QM_CUDA(launch_pdl(pdl, point_mask_kernel, dim3((unsigned)((points + 255) / 256)), dim3(256), 0, st, m));
   return QMCRT_OK;
 }
 
@@ -1042,7 +1063,7 @@ qmcrt_status ensure_masks(qmcrt_scene* s, cudaStream_t st) {
     s->mask_cap = s->points;
   }
   qmcrt_status e = launch_point_masks(s, scene_geom(s), s->sun_unit, s->d_point_xz, s->d_point_helio,
-                                      s->d_helio_weight, s->points, s->d_point_mask, s->d_point_origin, st);
+                                      s->d_helio_weight, s->points, s->d_point_mask, s->d_point_origin, st, true);
   if (e) return e;
   s->mask_geom = s->geom_version;
   s->mask_points = s->points_version;
@@ -1105,7 +1126,7 @@ void free_sun_geom(SunGeom* g) {
 // Occluder candidates of every heliostat of scene s for the (normalised) sun,
 // from the aimed frames and rectangle records, into cand / cand_n.
 static qmcrt_status launch_cand(const qmcrt_scene* s, const double* frame, const float4* rect, const double sun[3],
-                                bool exhaustive, float4* cand, int* cand_n, cudaStream_t st) {
+                                bool exhaustive, float4* cand, int* cand_n, cudaStream_t st, bool pdl = false) {
   CandArgs ca{};
   ca.n = s->n;
   ca.pos = s->d_pos;
@@ -1127,17 +1148,16 @@ static qmcrt_status launch_cand(const qmcrt_scene* s, const double* frame, const
   ca.bucket_start = s->d_bucket_start;
   ca.bucket_ids = s->d_bucket_ids;
   if (exhaustive)
-    cand_kernel<true><<<(2 * s->n + 3) / 4, 128, 0, st>>>(ca);
+    QM_CUDA(launch_pdl(pdl, cand_kernel<true>, dim3((2 * s->n + 3) / 4), dim3(128), 0, st, ca));
   else
-    cand_kernel<false><<<(2 * s->n + 3) / 4, 128, 0, st>>>(ca);
-  QM_CUDA(cudaGetLastError());
+    QM_CUDA(launch_pdl(pdl, cand_kernel<false>, dim3((2 * s->n + 3) / 4), dim3(128), 0, st, ca));
   return QMCRT_OK;
 }
 
 // Aim every heliostat for the sun (normalised) and rebuild the grid into g:
 // stream-ordered kernels only, so the sequence can be captured in a graph.
 qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool pdl) {
   AimArgs a{};
   a.n = s->n;
   a.pos = s->d_pos;
@@ -1159,39 +1179,38 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   a.power = g.power;
   QM_CUDA(cudaMemsetAsync(g.cell_count, 0, s->cells * sizeof(int32_t), st));
   QM_CUDA(cudaMemsetAsync(g.power, 0, sizeof(double), st));
-  aim_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(a);
-  QM_CUDA(cudaGetLastError());
-  qmcrt_status e = launch_cand(s, g.frame, g.rect, sun, false, g.cand, g.cand_n, st);
+  QM_CUDA(launch_pdl(pdl, aim_kernel, dim3((s->n + 127) / 128), dim3(128), 0, st, a));
+  qmcrt_status e = launch_cand(s, g.frame, g.rect, sun, false, g.cand, g.cand_n, st, pdl);
   if (e) return e;
   if (s->cells <= kScanOneCtaMax) {
-    scan_kernel<<<1, 1024, 0, st>>>(g.cell_count, g.cell_start, s->cells, s->entry_cap, s->d_flag, g.field_yr);
+    QM_CUDA(launch_pdl(pdl, scan_kernel, dim3(1), dim3(1024), 0, st, g.cell_count, g.cell_start, s->cells,
+                       s->entry_cap, s->d_flag, g.field_yr));
   } else {
     const int64_t tiles = (s->cells + kScanTile - 1) / kScanTile;
-    scan_tiles_kernel<<<(unsigned)tiles, 1024, 0, st>>>(g.cell_count, g.cell_start, s->cells, g.scan_part);
-    scan_parts_kernel<<<1, 1024, 0, st>>>(g.scan_part, tiles, g.cell_start, s->cells, s->entry_cap, s->d_flag,
-                                          g.field_yr);
-    scan_add_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(g.cell_count, g.cell_start, s->cells,
-                                                                        g.scan_part, s->entry_cap);
+    QM_CUDA(launch_pdl(pdl, scan_tiles_kernel, dim3((unsigned)tiles), dim3(1024), 0, st, g.cell_count, g.cell_start,
+                       s->cells, g.scan_part));
+    QM_CUDA(launch_pdl(pdl, scan_parts_kernel, dim3(1), dim3(1024), 0, st, g.scan_part, tiles, g.cell_start,
+                       s->cells, s->entry_cap, s->d_flag, g.field_yr));
+    QM_CUDA(launch_pdl(pdl, scan_add_kernel, dim3((unsigned)((s->cells + 255) / 256)), dim3(256), 0, st,
+                       g.cell_count, g.cell_start, s->cells, g.scan_part, s->entry_cap));
   }
-  QM_CUDA(cudaGetLastError());
-  fill_kernel<<<(s->n + 127) / 128, 128, 0, st>>>(s->n, g.cellbox, g.cell_start, g.cell_count, g.entries,
-                                                  s->gdims[1], s->gdims[2], s->entry_cap);
-  QM_CUDA(cudaGetLastError());
+  QM_CUDA(launch_pdl(pdl, fill_kernel, dim3((s->n + 127) / 128), dim3(128), 0, st, s->n, g.cellbox, g.cell_start,
+                     g.cell_count, g.entries, s->gdims[1], s->gdims[2], s->entry_cap));
   // a warp per cell on small grids (few cells, many ids each), a thread per
   // cell on large ones (mostly empty cells): 13.2 -> 4.4 us on the small
   // field, and 6.8 us instead of 77 us on the large field's 176 000 cells
   if (s->cells <= kCellWarpMax)
-    cell_finish_warp_kernel<<<(unsigned)((s->cells + 7) / 8), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
-                                                                         g.cell_rect, g.cell_info, g.field_yr);
+    QM_CUDA(launch_pdl(pdl, cell_finish_warp_kernel, dim3((unsigned)((s->cells + 7) / 8)), dim3(256), 0, st,
+                       s->cells, g.cell_start, g.entries, g.rect, g.cell_rect, g.cell_info, g.field_yr));
   else
-    cell_finish_kernel<<<(unsigned)((s->cells + 255) / 256), 256, 0, st>>>(s->cells, g.cell_start, g.entries, g.rect,
-                                                                          g.cell_rect, g.cell_info, g.field_yr);
+    QM_CUDA(launch_pdl(pdl, cell_finish_kernel, dim3((unsigned)((s->cells + 255) / 256)), dim3(256), 0, st,
+                       s->cells, g.cell_start, g.entries, g.rect, g.cell_rect, g.cell_info, g.field_yr));
   QM_CUDA(cudaGetLastError());
   if (s->coarse_cells) {
     int3 cd = make_int3(s->gdims[0] / s->fine_div, s->gdims[1] / s->fine_div, s->gdims[2] / s->fine_div);
-    coarse_finish_kernel<<<(unsigned)((s->coarse_cells + 127) / 128), 128, 0, st>>>(
-        s->coarse_cells, s->fine_div, cd, s->gdims[1], s->gdims[2], g.cell_info, g.coarse_yr);
-    QM_CUDA(cudaGetLastError());
+    QM_CUDA(launch_pdl(pdl, coarse_finish_kernel, dim3((unsigned)((s->coarse_cells + 127) / 128)), dim3(128), 0, st,
+                       s->coarse_cells, s->fine_div, cd, s->gdims[1], s->gdims[2], (const int4*)g.cell_info,
+                       g.coarse_yr));
   }
   return QMCRT_OK;
 }

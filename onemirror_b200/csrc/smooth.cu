@@ -119,6 +119,8 @@ template <typename T, int R>
 __global__ void __launch_bounds__(kTileX* kTileY) smooth_sorted_kernel(const T* __restrict__ in,
                                                                        float* __restrict__ out, int w, int h,
                                                                        float ratio) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int W = 2 * R + 1, N = W * W, TW = kTileX + 2 * R, TH = kTileY + 2 * R;
   __shared__ T tile[TW * TH];
   const int x0 = blockIdx.x * kTileX - R, y0 = blockIdx.y * kTileY - R;
@@ -157,6 +159,8 @@ __global__ void __launch_bounds__(kTileX* kTileY) smooth_sorted_kernel(const T* 
 template <typename T, int METHOD>
 __global__ void __launch_bounds__(kTileX* kTileY) smooth_kernel(const T* __restrict__ in, float* __restrict__ out,
                                                                 int w, int h, int r, float ratio) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);
   const int tw = kTileX + 2 * r, th = kTileY + 2 * r;
@@ -231,13 +235,16 @@ static qmcrt_status smooth(const T* d_in, float* d_out, int w, int h, int r, flo
   if (a0 < b1 && b0 < a1) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "input and output maps overlap");
   dim3 block(kTileX, kTileY), grid((w + kTileX - 1) / kTileX, (h + kTileY - 1) / kTileY);
   size_t smem = (size_t)(kTileX + 2 * r) * (kTileY + 2 * r) * sizeof(T);
-  if (method == QMCRT_TRIM_SORTED && r == 1) smooth_sorted_kernel<T, 1><<<grid, block, 0, st>>>(d_in, d_out, w, h, ratio);
-  else if (method == QMCRT_TRIM_SORTED && r == 2) smooth_sorted_kernel<T, 2><<<grid, block, 0, st>>>(d_in, d_out, w, h, ratio);
-  else if (method == QMCRT_TRIM_SORTED && r == 3) smooth_sorted_kernel<T, 3><<<grid, block, 0, st>>>(d_in, d_out, w, h, ratio);
-  else if (method == QMCRT_TRIM_SORTED) smooth_kernel<T, QMCRT_TRIM_SORTED><<<grid, block, smem, st>>>(d_in, d_out, w, h, r, ratio);
-  else if (method == QMCRT_TRIM_HEAPS) smooth_kernel<T, QMCRT_TRIM_HEAPS><<<grid, block, smem, st>>>(d_in, d_out, w, h, r, ratio);
+  // launched with programmatic stream serialization: each kernel waits for
+  // the stream's previous kernel in pdl_wait() before touching memory
+  cudaError_t ce;
+  if (method == QMCRT_TRIM_SORTED && r == 1) ce = launch_pdl(true, smooth_sorted_kernel<T, 1>, grid, block, 0, st, d_in, d_out, w, h, ratio);
+  else if (method == QMCRT_TRIM_SORTED && r == 2) ce = launch_pdl(true, smooth_sorted_kernel<T, 2>, grid, block, 0, st, d_in, d_out, w, h, ratio);
+  else if (method == QMCRT_TRIM_SORTED && r == 3) ce = launch_pdl(true, smooth_sorted_kernel<T, 3>, grid, block, 0, st, d_in, d_out, w, h, ratio);
+  else if (method == QMCRT_TRIM_SORTED) ce = launch_pdl(true, smooth_kernel<T, QMCRT_TRIM_SORTED>, grid, block, smem, st, d_in, d_out, w, h, r, ratio);
+  else if (method == QMCRT_TRIM_HEAPS) ce = launch_pdl(true, smooth_kernel<T, QMCRT_TRIM_HEAPS>, grid, block, smem, st, d_in, d_out, w, h, r, ratio);
   else return set_error(QMCRT_ERR_INVALID_ARGUMENT, "unknown trimmed-mean method");
-  QM_CUDA(cudaGetLastError());
+  QM_CUDA(ce);
   return QMCRT_OK;
 }
 

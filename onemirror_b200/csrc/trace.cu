@@ -42,6 +42,8 @@ struct FinalizeArgs {
 };
 
 __global__ void finalize_kernel(FinalizeArgs a) {
+  pdl_wait();
+  pdl_trigger();
   double acc = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.res; i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t c = a.counts[i];
@@ -75,8 +77,7 @@ static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
   int64_t blocks = (int64_t)std::max(per_sm, 1) * sm_count();
   int64_t need = ((int64_t)a.rays - a.ray0 + kTraceThreads - 1) / kTraceThreads;
   blocks = std::max<int64_t>(1, std::min(blocks, need));
-  k<<<(unsigned)blocks, kTraceThreads, 0, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(true, k, dim3((unsigned)blocks), dim3(kTraceThreads), 0, st, a);
 }
 
 template <bool TABLES, bool RECORDS>
@@ -380,8 +381,7 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
   f.accumulate = p->accumulate;
   f.stats = s->d_stats;
   int fb = (int)std::min<int64_t>((res + 255) / 256, 4 * sm_count());
-  finalize_kernel<<<fb, 256, 0, st>>>(f);
-  QM_CUDA(cudaGetLastError());
+  QM_CUDA(launch_pdl(true, finalize_kernel, dim3(fb), dim3(256), 0, st, f));
   QM_CUDA(cudaEventRecord(s->ev[4], st));
   s->traced = true;
   if (stats) {

@@ -646,6 +646,7 @@ __device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned lo
 // The plain tracer: one grid-stride pass over the rays of one trace.
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
+  pdl_wait();
   __shared__ float4 s_tab[kBuieRecords];
   const float fy0 = CULL ? from_ordered(__ldg(a.field_yr)) : 0.f, fy1 = CULL ? from_ordered(__ldg(a.field_yr + 1)) : 0.f;
   if (!TABLES) {
