@@ -24,7 +24,6 @@ using namespace qm;
 namespace qm {
 void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a);
 qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
-bool buie_with_guide(float csr, BuieTable* t);
 
 // 2 CTAs of 512 threads per SM (32 warps) at <= 64 registers: against 3 CTAs
 // of 256 at 72 and 80 registers, the forward takes 12 % and the backward 4 %
@@ -681,7 +680,7 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   if (ce == cudaSuccess && !t->d_buie) ce = cudaMalloc(&t->d_buie, 4 * (size_t)kBuieRecords * sizeof(float));
   if (ce != cudaSuccess) return fail(cuda_error(ce, "adjoint tape allocation"));
   if ((e = tape_geometry(t, st))) return fail(e);
-  if (!buie_with_guide(sun->csr, &t->buie))
+  if (!buie_bucket_table(sun->csr, &t->buie))
     return fail(set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries"));
   AdjArgs& A = t->args;
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &A.t);

@@ -22,7 +22,6 @@ using namespace qm;
 
 namespace qm {
 void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a);
-bool buie_with_guide(float csr, BuieTable* t);
 
 constexpr int kBatchThreads = 256;
 
@@ -402,7 +401,7 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     if ((e = balloc(&it.d_counts, it.res)) || (e = balloc(&it.d_energy, it.res)) || (e = balloc(&it.d_flux, it.res))) goto fail;
     float csr = it.sun.csr;
     if (!b->tables.count(csr)) {
-      if (!buie_with_guide(csr, &b->tables[csr])) {
+      if (!buie_bucket_table(csr, &b->tables[csr])) {
         e = set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
         goto fail;
       }

@@ -64,6 +64,11 @@ struct BuieTable {
   bool within_alpha = false; // every sample lies within kSunAlphaMax of the sun axis
 };
 
+// The Buie table of `csr` in the kernels' staging layout (one interval
+// record per uniform bucket of the core CDF) and its scalars; false if a
+// bucket would hold two interval boundaries.
+bool buie_bucket_table(float csr, BuieTable* t);
+
 // Build the table exactly as set_samplelights does (float arithmetic).
 void buie_build(float csr, float* cdf_x, float* cdf_y, float* slope, float params[6]);
 

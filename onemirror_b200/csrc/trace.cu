@@ -113,7 +113,7 @@ static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool 
 // which this checks (the core table does not depend on csr; its narrowest
 // interval, the last, is 0.88 buckets wide).  Returns false if a bucket
 // holds two.
-bool buie_with_guide(float csr, BuieTable* t) {
+bool buie_bucket_table(float csr, BuieTable* t) {
   std::vector<float> raw(1025 + 1025 + 1024);
   float* cx = raw.data();
   float* cy = cx + 1025;
@@ -181,7 +181,7 @@ __global__ void buie_probe_kernel(const TraceArgs a, const float* u, int64_t n, 
 static qmcrt_status ensure_buie(qmcrt_scene* s, float csr, cudaStream_t st) {
   if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   if (s->buie.csr == csr) return QMCRT_OK;
-  if (!buie_with_guide(csr, &s->buie))
+  if (!buie_bucket_table(csr, &s->buie))
     return set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
   QM_CUDA(cudaMemcpyAsync(s->d_buie, s->buie.host.data(), s->buie.host.size() * sizeof(float),
                           cudaMemcpyHostToDevice, st));
@@ -494,7 +494,7 @@ qmcrt_status qmcrt_buie_sample_probe(float csr, const float* d_u, int64_t n, flo
   if (!d_u || !d_theta_mrad || n <= 0) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "bad probe arguments");
   if (!(csr > 0.f && csr < 1.f)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "csr must be in (0,1)");
   BuieTable t;
-  if (!buie_with_guide(csr, &t)) return set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
+  if (!buie_bucket_table(csr, &t)) return set_error(QMCRT_ERR_INTERNAL, "Buie table: a bucket holds two interval boundaries");
   cudaStream_t st = (cudaStream_t)stream;
   TraceArgs a;
   std::memset(&a, 0, sizeof(a));

@@ -450,9 +450,9 @@ struct GlobalDeposit {
   }
 };
 
-// Load the Buie table and its guide into shared memory (all threads): the
-// table (angles [1025], cdf [1025], slopes [1024]) as one {angle, cdf, slope,
-// next cdf} record per interval.
+// Load the Buie table's bucket records into shared memory (all threads): one
+// {angle, cdf, slope, next cdf} record per uniform bucket of the core CDF,
+// of the interval holding the bucket's smallest value (kBuieRecords of them).
 __device__ __forceinline__ void load_buie(const float* buie, float4* s_tab) {
   const float4* rec = reinterpret_cast<const float4*>(buie);  // kBuieRecords 16-byte records
   for (int i = threadIdx.x; i < kBuieRecords; i += blockDim.x) s_tab[i] = __ldg(rec + i);
