@@ -593,26 +593,51 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_ta
   }
   const int h = R.h;
   const d3 o = R.o, ws = R.ws;
-  const float3 of = R.of;
   // perturbed normal, reflected direction (i - 2 n (n.i)) and energy first,
   // so that the mirror frame is dead before the walks.  The reflection keeps
   // the length of ws (1 to float rounding of the sample), and nothing that
   // uses rd depends on its length beyond that: the receiver's (u, v), the
   // rectangle tests and the walk's cell order are scale-free, the slant range
   // for attenuation moves by ~1e-7 relative; so rd is not renormalised.
-  const d3 np = rnorm(apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z));
-  const d3 rd = ws - (2.0 * dot(ws, np)) * np;
-  // calEnergy (rectgrid_raytracing.cu:129-133)
-  const float e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * R.w;
+  const d3 npu = apply(R.fr, (double)R.tl.x, (double)R.tl.y, (double)R.tl.z);
+  const double nn = dot(npu, npu);
+  d3 rd;
+  float e;  // calEnergy (rectgrid_raytracing.cu:129-133)
+  if (TABLES) {  // caller tables may hold vectors of any length
+    const d3 np = rsqrt_nr(nn) * npu;
+    rd = ws - (2.0 * dot(ws, np)) * np;
+    e = (float)fabs(np.x * a.sdir[0] + np.y * a.sdir[1] + np.z * a.sdir[2]) * R.w;
+  } else {
+    // A Philox perturbation is a unit vector to float rounding and the frame
+    // is orthonormal in FP64, so nn = 1 + t with |t| < 2e-6.  Then
+    // 1 / nn = 1 - t + t^2 to within t^3 (below 1e-17), and 1 / sqrt(nn) =
+    // 1.5 - nn / 2 to within 3 t^2 / 8 (below 2e-12, for the float energy):
+    // no square root or reciprocal, and the normal is never scaled.
+    const double t = nn - 1.0;
+    const double k = -2.0 * dot(ws, npu) * fma(t, t - 1.0, 1.0);
+    rd = mk(fma(k, npu.x, ws.x), fma(k, npu.y, ws.y), fma(k, npu.z, ws.z));
+    e = (float)(fabs(npu.x * a.sdir[0] + npu.y * a.sdir[1] + npu.z * a.sdir[2]) * fma(-0.5, nn, 1.5)) * R.w;
+  }
   uint8_t flag = 0;
   int pix = -1;
   double th = 0.0;
-  const float3 sdir = f3((float)-ws.x, (float)-ws.y, (float)-ws.z);
-  if (CULL == 3 ? list_blocked<STATS>(a, h, 0, of, sdir, fy0, fy1, c.test, c.cell, R.reach.x)
-                : dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, sdir, h, fy0, fy1, c.test, c.cell)) {
+  // The walks' FP32 origin and directions are formed only for a walk that
+  // runs: a point mask of 0 (most points) skips its walk, and with it five to
+  // seven FP64-to-FP32 conversions on the XU pipe.
+  auto of = [&]() { return TABLES ? R.of : f3(R.of.x, R.of.y, (float)o.z); };
+  auto sdir = [&]() { return f3((float)-ws.x, (float)-ws.y, (float)-ws.z); };
+  bool shadowed, blocked = false;
+  if (CULL == 3) {
+    shadowed = R.reach.x != 0u && list_blocked<STATS>(a, h, 0, of(), sdir(), fy0, fy1, c.test, c.cell, R.reach.x);
+    if (!shadowed)
+      blocked = R.reach.y != 0u && list_blocked<STATS>(a, h, 1, of(), to_f(rd), fy0, fy1, c.test, c.cell, R.reach.y);
+  } else {
+    shadowed = dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of(), sdir(), h, fy0, fy1, c.test, c.cell);
+    if (!shadowed) blocked = dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of(), to_f(rd), h, fy0, fy1, c.test, c.cell);
+  }
+  if (shadowed) {
     flag = QMCRT_RAY_SHADOWED;
-  } else if (CULL == 3 ? list_blocked<STATS>(a, h, 1, of, to_f(rd), fy0, fy1, c.test, c.cell, R.reach.y)
-                       : dda_blocked<STATS, (CULL > 0), (CULL == 2)>(a, of, to_f(rd), h, fy0, fy1, c.test, c.cell)) {
+  } else if (blocked) {
     flag = QMCRT_RAY_BLOCKED;
   } else if (receiver_hit(a, o, rd, pix, &th)) {
     flag = QMCRT_RAY_HIT;
