@@ -55,6 +55,18 @@ __device__ __forceinline__ frame64 frame_of(d3 n, uint32_t quirks) {
   return f;
 }
 
+// Clears the per-sun registration counts of the grid cells and the field's
+// total power before aim_kernel adds to them: one launch in place of two
+// memsets, so that it joins the chain of kernels launched with programmatic
+// dependent launch.
+__global__ void zero_geom_kernel(int32_t* cell_count, int64_t cells, double* power) {
+  pdl_wait();
+  pdl_trigger();
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t i = i0; i < cells; i += (int64_t)gridDim.x * blockDim.x) cell_count[i] = 0;
+  if (i0 == 0) *power = 0.0;
+}
+
 __global__ void aim_kernel(AimArgs a) {
   pdl_wait();
   pdl_trigger();
@@ -1177,8 +1189,8 @@ qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const doubl
   std::memcpy(a.gcell, s->gcell, sizeof(a.gcell));
   std::memcpy(a.gdims, s->gdims, sizeof(a.gdims));
   a.power = g.power;
-  QM_CUDA(cudaMemsetAsync(g.cell_count, 0, s->cells * sizeof(int32_t), st));
-  QM_CUDA(cudaMemsetAsync(g.power, 0, sizeof(double), st));
+  QM_CUDA(launch_pdl(pdl, zero_geom_kernel, dim3((unsigned)std::min<int64_t>((s->cells + 255) / 256, 592)), dim3(256), 0,
+                     st, g.cell_count, s->cells, g.power));
   QM_CUDA(launch_pdl(pdl, aim_kernel, dim3((s->n + 127) / 128), dim3(128), 0, st, a));
   qmcrt_status e = launch_cand(s, g.frame, g.rect, sun, false, g.cand, g.cand_n, st, pdl);
   if (e) return e;
