@@ -474,11 +474,15 @@ class FieldRun:
         _, _, sm = D.step_maps(r["counts"], r["energy"], self.smooth)
         return r, sm
 
-    def timed(self, steps, k0):
+    def timed(self, steps, k0, stages=0):
         """`steps` device-timed steps, L2 flushed before each (outside the
-        events); returns per-step ms, trace-kernel ms and setup ms."""
+        events); returns per-step ms, and the trace-kernel and setup ms of the
+        stages the library timed (`stages`: capi.TIMING_* bits; a timed stage
+        adds CUDA events to the step)."""
         import torch
+        from onemirror_b200 import capi
         from onemirror_b200 import dist as D
+        self.sc.set_timing(stages)
         step_ms, kern_ms, setup_ms = [], [], []
         for k in range(steps):
             # the step's sun and events are formed before the flush, so that the
@@ -491,11 +495,15 @@ class FieldRun:
             e0.record()
             self.step(k0 + k, item, sun=sun)
             e1.record()
-            t = self.sc.timing()
-            kern_ms.append(t.trace_kernel_ms)
-            setup_ms.append(t.setup_ms)
+            if stages & (capi.TIMING_TRACE | capi.TIMING_FINALIZE):
+                t = self.sc.timing()
+                if t.trace_kernel_ms >= 0:
+                    kern_ms.append(t.trace_kernel_ms)
+                if t.setup_ms >= 0:
+                    setup_ms.append(t.setup_ms)
             e1.synchronize()
             step_ms.append(e0.elapsed_time(e1))
+        self.sc.set_timing(0)
         return step_ms, kern_ms, setup_ms
 
     def e2e(self, steps):
@@ -564,12 +572,16 @@ def field_block(name, rank, world, dev, flush, steps, e2e_steps, warmup=3):
     """Throughput of another field at its own configuration (a sub-block of
     the default line): device-timed steps and the end-to-end call."""
     import statistics as S
+    from onemirror_b200 import capi
     from onemirror_b200 import workloads as W
     w = W.BUILDERS[name]()
     run = FieldRun(w, rank, world, dev, flush)
     for k in range(warmup):
         run.step(k, 60000 + k)
-    step_ms, kern_ms, _ = run.timed(steps, warmup)
+    step_ms, _, _ = run.timed(steps, warmup)
+    # the trace kernel's time from further steps that time it (the events
+    # would lengthen the small field's step)
+    _, kern_ms, _ = run.timed(10, warmup + steps, capi.TIMING_TRACE)
     e2e = run.e2e(e2e_steps)
     run.close()
     total = sum(step_ms)
@@ -756,11 +768,14 @@ def b200_arm(a, rank, world, local):
     clk.start()
     time.sleep(0.3)  # nvidia-smi's first samples; the summary keeps only the timed region's
     t_begin = time.time()
-    step_ms, kern_ms, setup_ms = run.timed(a.steps, a.warmup + 1)
+    # the trace kernel's own events stay in the timed steps (its time is the
+    # roofline's denominator); the setup is timed on a few steps after them
+    step_ms, kern_ms, _ = run.timed(a.steps, a.warmup + 1, capi.TIMING_TRACE)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clocks = clk.stop((t_begin, time.time()))
+    _, _, setup_ms = run.timed(5, a.warmup + 1 + a.steps, capi.TIMING_SETUP | capi.TIMING_TRACE)
     total_ms = float(sum(step_ms))
     if world > 1:
         total_ms = D.max_over_ranks(total_ms, dev)
@@ -823,8 +838,10 @@ def b200_arm(a, rank, world, local):
     if traffic is not None:
         roof["hbm_achieved_gbs"] = traffic / kern_s / 1e9
         roof["hbm_frac"] = roof["hbm_achieved_gbs"] / roof["hbm_peak_gbs"]
-    per_step = {"aim": 1, "candidates": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1, "point_masks": 1,
-                "trace": 1, "finalize": 1, "smooth": 1}
+    per_step = {"zero_geometry": 1, "aim": 1, "candidates": 1, "grid_scan": 1, "grid_fill": 1, "grid_cells": 1,
+                "point_masks": 1, "zero_maps": 1, "trace": 1, "finalize": 1, "smooth": 1}
+    if sc.grid_info().cells > 65536:  # the cell-count scan over tiles: three launches
+        per_step["grid_scan"] = 3
     if w.grid.fine_div > 1:
         per_step["grid_coarse"] = 1
     launches = sum(per_step.values())
@@ -835,7 +852,8 @@ def b200_arm(a, rank, world, local):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "flux_rmse": accuracy,
             "gpu_launches": launches * a.steps,
             "launches_per_step": per_step,
-            "setup_ms": statistics.mean([s for s in setup_ms if s >= 0]) if any(s >= 0 for s in setup_ms) else None,
+            "setup_ms": statistics.mean(setup_ms) if setup_ms else None,
+            "setup_ms_note": "aim, candidates and grid build, timed on 5 steps after the timed region",
             "clocks": clocks,
             "fields": fields or None,
             "reference_cuda": refcuda,

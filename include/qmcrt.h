@@ -350,7 +350,10 @@ qmcrt_status qmcrt_scene_set_sun(qmcrt_scene* scene, const qmcrt_sun* sun, uint3
 
 qmcrt_status qmcrt_scene_grid_info(qmcrt_scene* scene, qmcrt_grid_info* info);
 
-/* Copy the grid CSR to host (cells+1 offsets, entries heliostat ids).  Syncs. */
+/* Copy the grid CSR to host (cells+1 offsets, entries heliostat ids).  The
+ * geometry of a trace that tests occluder candidates builds its grid only if a
+ * candidate list overflows; this call (and qmcrt_scene_grid_info) builds it
+ * first when it was left unbuilt.  Syncs. */
 qmcrt_status qmcrt_scene_read_grid(qmcrt_scene* scene, int32_t* h_cell_start, int32_t* h_entries,
                                    void* stream);
 
@@ -572,10 +575,25 @@ qmcrt_status qmcrt_smooth_trimmed_f32(const float* d_in, float* d_out, int32_t w
                                       int32_t height, int32_t radius, float ratio, int32_t method,
                                       void* stream);
 
+/* Stage timing (no counterpart in the reference).  Off by default: a timed
+ * stage records a CUDA event on the call's stream before and after it, and an
+ * event between two kernels keeps the second from starting while the first
+ * finishes (the kernels of a trace use programmatic dependent launch), which
+ * cost about a tenth of the small field's step with every stage timed. */
+enum {
+  QMCRT_TIMING_TRACE = 1,    /* the trace kernel launches */
+  QMCRT_TIMING_SETUP = 2,    /* aiming, occluder candidates and grid build, when the sun changed */
+  QMCRT_TIMING_FINALIZE = 4, /* flux scaling and the copy to the outputs */
+  QMCRT_TIMING_ALL = 7
+};
+/* Which stages the scene's later traces time (QMCRT_TIMING_* bits; 0: none). */
+qmcrt_status qmcrt_scene_set_timing(qmcrt_scene* scene, uint32_t stages);
+
 /* Device time of the stages of the last qmcrt_trace / qmcrt_trace_tables on
- * this scene, from CUDA events recorded on the call's stream.  setup_ms is
- * the aiming + grid build (negative when that trace reused the cached
- * geometry).  Waits for the last trace to finish. */
+ * this scene, from the CUDA events it recorded on the call's stream; -1 for a
+ * stage it did not time (setup_ms also when that trace reused the cached
+ * geometry).  QMCRT_ERR_INVALID_ARGUMENT if it timed neither the trace kernel
+ * nor the finalize stage.  Waits for the last trace to finish. */
 typedef struct qmcrt_timing {
   float setup_ms;
   float trace_kernel_ms;

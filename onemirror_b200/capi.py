@@ -28,6 +28,7 @@ ATTEN_NONE, ATTEN_POLY_EXP = 0, 1
 CAND_CAP = 32  # QMCRT_CAND_CAP: occluder candidates kept per heliostat and walk
 TRIM_SORTED, TRIM_HEAPS = 0, 1
 SMOOTH_COUNTS, SMOOTH_ENERGY = 0, 1
+TIMING_TRACE, TIMING_SETUP, TIMING_FINALIZE, TIMING_ALL = 1, 2, 4, 7
 RAY_SHADOWED, RAY_BLOCKED, RAY_HIT, RAY_OFFMAP = 1, 2, 4, 8
 
 fp = C.POINTER(C.c_float)
@@ -164,6 +165,7 @@ PROTOTYPES = {
     "qmcrt_smooth_trimmed_f32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                            C.c_int32, C.c_void_p]),
     "qmcrt_scene_timing": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qmcrt_scene_set_timing": (C.c_int, [C.c_void_p, C.c_uint32]),
     "qmcrt_adjoint_forward": (C.c_int, [C.c_void_p, C.POINTER(Sun), C.POINTER(TraceParams), C.c_void_p, C.c_uint64,
                                         C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.c_void_p]),
     "qmcrt_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -23,7 +23,6 @@ using namespace qm;
 
 namespace qm {
 void fill_trace_args(qmcrt_scene* s, const SunGeom& geo, const qmcrt_sun* sun, uint32_t quirks, TraceArgs* a);
-qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
 
 // 2 CTAs of 512 threads per SM (32 warps) at <= 64 registers: against 3 CTAs
 // of 256 at 72 and 80 registers, the forward takes 12 % and the backward 4 %

@@ -118,6 +118,7 @@ struct SunGeom {
   int* cand_n = nullptr;         // [n][2] their counts (> kCandCap: too many, the rays walk the grid)
   int* field_yr = nullptr;       // [2]
   double* power = nullptr;       // [1] sum |n . sun| * A
+  int* grid_ctl = nullptr;       // [4] the grid's build control words (zero_geom_kernel, scene.cu)
 };
 
 struct PointsKey {
@@ -185,6 +186,8 @@ struct qmcrt_scene {
   float4* d_cand = nullptr;         // [n][2][kCandCap][3] occluder candidates' rectangle records (shadow, block)
   int* d_cand_n = nullptr;          // [n][2]
   int* d_field_yr = nullptr;        // [2] height range of the field (order-preserving ints)
+  int* d_grid_ctl = nullptr;        // [4] grid build control words of the current geometry
+  bool grid_forced = false;         // the current geometry's grid is built (or being built) in the stream
   qm::SunKey sun_key;
 
   // points
@@ -212,9 +215,12 @@ struct qmcrt_scene {
   qm::BuieTable buie;
   float* d_buie = nullptr;
 
-  // stage timing of the last trace: [0,1] setup, [2,3] trace kernel, [4] finalize end
+  // stage timing of the last trace: [0,1] setup, [2,3] trace kernel, [3,4]
+  // finalize; timing_stages (QMCRT_TIMING_*) says which stages record their
+  // events, timed those the last trace recorded
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  bool setup_timed = false;
+  uint32_t timing_stages = 0;
+  uint32_t timed = 0;
   bool traced = false;
 };
 
@@ -227,8 +233,17 @@ void free_sun_geom(SunGeom* g);
 // Enqueue aiming + grid build of scene s for the (normalised) sun direction
 // into g.  pdl: launch the kernels with programmatic stream serialization
 // (each starts while the one before it finishes; not inside graph captures).
+// force_grid false: the grid is built only if a candidate list overflows (the
+// traces that test candidates walk the grid only there).
 qmcrt_status launch_sun_geom(const qmcrt_scene* s, const SunGeom& g, const double sun[3], uint32_t quirks,
-                             cudaStream_t st, bool pdl = false);
+                             cudaStream_t st, bool pdl = false, bool force_grid = true);
+// The scene's sun geometry for `sun`, rebuilt when the sun, the quirks that
+// shape it or the field changed; need_grid: the caller walks the grid (table
+// traces, quirk modes, grid-walk variants), so it is built whatever the
+// candidate lists hold.
+qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st, bool need_grid = true);
+// Build the current geometry's grid if it was left unbuilt.
+qmcrt_status ensure_grid(qmcrt_scene* s, cudaStream_t st);
 qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
 // Per-point candidate masks of `points` points (xz, helio) for geometry g of
 // scene s and the (normalised) sun, into mask, and the points' world

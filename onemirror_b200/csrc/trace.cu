@@ -24,7 +24,6 @@ using namespace qm;
 
 namespace qm {
 
-qmcrt_status ensure_sun(qmcrt_scene* s, const qmcrt_sun* sun, uint32_t quirks, cudaStream_t st);
 qmcrt_status ensure_points(qmcrt_scene* s, const qmcrt_trace_params* p, cudaStream_t st);
 qmcrt_status upload_field(qmcrt_scene* s, const qmcrt_field* f, cudaStream_t st);
 
@@ -343,6 +342,17 @@ __global__ void scale_kernel(float* m, int64_t n, float k) {
     m[i] *= k;
 }
 
+// Philox rays of the corrected method test their heliostat's occluder
+// candidates instead of walking the grid (variants 4 and 5 walk the grid; the
+// lists leave out the ray's own heliostat, so not under QMCRT_QUIRK_SELF_HIT;
+// vertical culling needs every rectangle registered in every cell it touches
+// and the origin cell tested, so not under the two grid quirks or variant 2).
+static bool uses_candidates(const qmcrt_scene* s, const qmcrt_trace_params* p, bool tables) {
+  const bool cull = p->kernel_variant != 2 && !(p->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS));
+  return cull && !tables && s->buie.within_alpha && !(p->quirks & QMCRT_QUIRK_SELF_HIT) && p->kernel_variant != 4 &&
+         p->kernel_variant != 5;
+}
+
 static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace_params* p, TraceArgs& a,
                                    bool tables, double weight_scale, const qmcrt_outputs* out,
                                    qmcrt_trace_stats* stats, cudaStream_t st) {
@@ -354,18 +364,17 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
     a.flags = out->d_ray_flags;
     a.pixel = out->d_ray_pixel;
   }
-  QM_CUDA(cudaEventRecord(s->ev[2], st));
+  // timing events on request only: an event between two kernels keeps the
+  // second from starting while the first finishes (programmatic dependent
+  // launch), about 10 % of the small field's step with every stage timed
+  const bool t_trace = s->timing_stages & QMCRT_TIMING_TRACE, t_fin = s->timing_stages & QMCRT_TIMING_FINALIZE;
+  if (t_trace) QM_CUDA(cudaEventRecord(s->ev[2], st));
   // vertical culling needs every rectangle registered in every cell it
   // touches and the origin cell tested: off under the two grid quirks
   // (level 2 adds the coarse level of a two-level grid)
   int cull = p->kernel_variant != 2 && !(p->quirks & (QMCRT_QUIRK_SKIP_ORIGIN_CELL | QMCRT_QUIRK_AABB_RADIUS));
   if (cull && a.coarse_yr && p->kernel_variant != 4) cull = 2;
-  // Philox rays of the corrected method test their heliostat's occluder
-  // candidates instead of walking the grid (variants 4 and 5 walk the grid)
-  // (the lists leave out the ray's own heliostat: not under QMCRT_QUIRK_SELF_HIT)
-  if (cull && !tables && a.cand && s->buie.within_alpha && !(p->quirks & QMCRT_QUIRK_SELF_HIT) &&
-      p->kernel_variant != 4 && p->kernel_variant != 5)
-    cull = 3;
+  if (a.cand && uses_candidates(s, p, tables)) cull = 3;
   // one launch per block of 2^32 ray ids: a launch's threads carry the low
   // word of their ray id, the launch the high word (and the records pointers
   // its offset)
@@ -381,7 +390,7 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
     QM_CUDA(dispatch(sa, tables, records, stats != nullptr, cull, p->kernel_variant, st));
     b = end;
   }
-  QM_CUDA(cudaEventRecord(s->ev[3], st));
+  if (t_trace || t_fin) QM_CUDA(cudaEventRecord(s->ev[3], st));
   const double scale = flux_scale(s, sun, p, weight_scale);
   FinalizeArgs f{};
   f.res = res;
@@ -395,7 +404,8 @@ static qmcrt_status run_and_finish(qmcrt_scene* s, const qmcrt_sun* sun, const q
   f.stats = s->d_stats;
   int fb = (int)std::min<int64_t>((res + 255) / 256, 4 * sm_count());
   QM_CUDA(launch_pdl(true, finalize_kernel, dim3(fb), dim3(256), 0, st, f));
-  QM_CUDA(cudaEventRecord(s->ev[4], st));
+  if (t_fin) QM_CUDA(cudaEventRecord(s->ev[4], st));
+  s->timed |= (t_trace ? QMCRT_TIMING_TRACE : 0u) | (t_fin ? QMCRT_TIMING_FINALIZE : 0u);
   s->traced = true;
   if (stats) {
     unsigned long long h[16];
@@ -433,8 +443,9 @@ qmcrt_status qmcrt_trace(qmcrt_scene* s, const qmcrt_sun* sun, const qmcrt_trace
   cudaStream_t st = (cudaStream_t)stream;
   if (!(sun->dni >= 0)) return set_error(QMCRT_ERR_INVALID_ARGUMENT, "dni must be non-negative");
   if ((e = ensure_buie(s, sun->csr, st))) return e;
-  s->setup_timed = false;
-  if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
+  s->timed = 0;
+  // a trace that tests candidates needs the grid only where a list overflows
+  if ((e = ensure_sun(s, sun, p->quirks, st, !uses_candidates(s, p, false)))) return e;
   if ((e = ensure_points(s, p, st))) return e;
   TraceArgs a{};
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);
@@ -464,7 +475,7 @@ qmcrt_status qmcrt_trace_tables(qmcrt_scene* s, const qmcrt_sun* sun, const qmcr
   if ((uint64_t)t->points * (uint64_t)t->rays_per_point > 0xFFFFFFFFull)
     return set_error(QMCRT_ERR_INVALID_ARGUMENT, "ray count must be below 2^32");
   cudaStream_t st = (cudaStream_t)stream;
-  s->setup_timed = false;
+  s->timed = 0;
   if ((e = ensure_sun(s, sun, p->quirks, st))) return e;
   TraceArgs a{};
   fill_trace_args(s, scene_geom(s), sun, p->quirks, &a);

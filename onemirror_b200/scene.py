@@ -225,6 +225,10 @@ class SolarScene:
     def tape_free(tape):
         capi.lib().qmcrt_tape_free(tape)
 
+    def set_timing(self, stages):
+        """Which stages later traces time (capi.TIMING_* bits; 0: none, the default)."""
+        capi.check(capi.lib().qmcrt_scene_set_timing(self.h, stages))
+
     def timing(self):
         t = capi.Timing()
         capi.check(capi.lib().qmcrt_scene_timing(self.h, C.byref(t)))

@@ -56,6 +56,8 @@ def test_argument_errors_need_no_gpu():
     assert L.qmcrt_buie_sample_probe(C.c_float(1.5), dummy, 16, dummy, None) == capi.ERR_INVALID_ARGUMENT
     assert b"csr" in L.qmcrt_last_error()
     assert L.qmcrt_buie_sample_probe(C.c_float(0.1), dummy, 0, dummy, None) == capi.ERR_INVALID_ARGUMENT
+    assert L.qmcrt_scene_set_timing(None, capi.TIMING_TRACE) == capi.ERR_INVALID_ARGUMENT
+    assert L.qmcrt_scene_timing(None, None) == capi.ERR_INVALID_ARGUMENT
 
 
 def test_version_and_status_strings():

@@ -343,3 +343,34 @@ def test_ray_range_traces_the_same_rays():
     p.ray_begin = p.ray_end = 0
     sc.close()
 
+
+
+def test_stage_timing_is_opt_in_and_leaves_the_maps_unchanged():
+    """qmcrt_scene_set_timing: no stage is timed by default (qmcrt_scene_timing
+    refuses), each enabled stage reports a duration and the others -1, and
+    the timing events change none of the trace's results."""
+    w = W.small()
+    sc = SolarScene.from_workload(w)
+    plain = sc.trace(w.sun, w.params)["counts"].cpu().numpy()
+    with pytest.raises(capi.QmcrtError):
+        sc.timing()
+    sc.set_timing(capi.TIMING_TRACE)
+    g = sc.trace(W.make_sun(44.0, 180.0), w.params)  # a new sun: the setup runs, untimed
+    t = sc.timing()
+    assert t.trace_kernel_ms > 0 and t.setup_ms == -1.0 and t.finalize_ms == -1.0
+    sc.set_timing(capi.TIMING_ALL)
+    g = sc.trace(w.sun, w.params)
+    t = sc.timing()
+    assert t.setup_ms > 0 and t.trace_kernel_ms > 0 and t.finalize_ms > 0
+    assert np.array_equal(g["counts"].cpu().numpy(), plain)
+    sc.set_timing(capi.TIMING_FINALIZE)
+    sc.trace(w.sun, w.params)  # cached geometry: no setup
+    t = sc.timing()
+    assert t.finalize_ms > 0 and t.trace_kernel_ms == -1.0 and t.setup_ms == -1.0
+    with pytest.raises(capi.QmcrtError):
+        sc.set_timing(8)
+    sc.set_timing(0)
+    sc.trace(w.sun, w.params)
+    with pytest.raises(capi.QmcrtError):
+        sc.timing()
+    sc.close()

@@ -162,6 +162,29 @@ def test_big_field_grids_equal_oracle(name):
     sc.close()
 
 
+@pytest.mark.parametrize("name", ["small", "mid", "large"])
+def test_grid_built_on_demand_after_a_candidate_trace(name):
+    """A Philox trace that tests occluder candidates leaves its geometry's
+    grid unbuilt unless a list overflows; reading the grid afterwards (and a
+    grid-walk trace of the same sun) builds it then, through the single-CTA
+    scan (small, mid) or the tiled scan (large), equal to the oracle's CSR,
+    and a second demand does not build it twice."""
+    w = W.small() if name == "small" else W.BUILDERS[name](rays=1 << 22)
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    cnt = sc.trace(w.sun, p, stats=True)["counts"].clone()
+    ref = oracle_scene(w, sc, w.sun, 0, use_gpu_grid=False)
+    for _ in range(2):
+        start, ent = sc.read_grid()
+        assert np.array_equal(start, ref.cell_start)
+        assert np.array_equal(ent, ref.entries[: start[-1]])
+    p.kernel_variant = 5  # the grid walk, same sun: the cached geometry and its grid
+    g5 = sc.trace(w.sun, p, stats=True)
+    assert torch.equal(g5["counts"], cnt) and g5["stats"].dda_cells > 0
+    p.kernel_variant = 0
+    sc.close()
+
+
 def run_pair(w, sc, sun, params, quirks=0):
     params.quirks = quirks
     g = sc.trace(sun, params, records=True)
