@@ -348,6 +348,9 @@ qmcrt_status qmcrt_scene_set_field(qmcrt_scene* scene, const qmcrt_field* field,
 qmcrt_status qmcrt_scene_set_sun(qmcrt_scene* scene, const qmcrt_sun* sun, uint32_t quirks,
                                  void* stream);
 
+/* The grid's bounds and its CSR entry count.  When the last trace left its
+ * geometry's grid unbuilt (see qmcrt_scene_read_grid), this waits for the
+ * device to be idle and builds it on the default stream.  Syncs. */
 qmcrt_status qmcrt_scene_grid_info(qmcrt_scene* scene, qmcrt_grid_info* info);
 
 /* Copy the grid CSR to host (cells+1 offsets, entries heliostat ids).  The

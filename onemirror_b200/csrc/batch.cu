@@ -311,7 +311,10 @@ static qmcrt_status enqueue_pass(qmcrt_batch* b, cudaStream_t st) {
   for (size_t i = 0; i < b->items.size(); ++i) {
     auto& it = b->items[i];
     cudaStream_t s = b->side[i % K];
-    if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, s))) return e;
+    // the items' rays test occluder candidates: their grids are built only
+    // where a list overflows, or for every ray when the sunshape is too wide
+    // for the candidate cones
+    if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, s, false, !b->tables.at(it.sun.csr).within_alpha))) return e;
     if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.weight, it.points, it.d_mask, it.d_origin, s)))
       return e;
     QM_CUDA(cudaMemsetAsync(it.d_counts, 0, it.res * sizeof(uint32_t), s));
@@ -522,7 +525,7 @@ qmcrt_status qmcrt_batch_autotune(qmcrt_batch* b, qmcrt_batch_tuning* chosen, vo
   int n = std::min<int>((int)b->items.size(), 12);
   for (int i = 0; i < n; ++i) {
     auto& it = b->items[i];
-    if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, st))) return e;
+    if ((e = launch_sun_geom(it.scene, it.geo, it.sdir, 0, st, false, !b->tables.at(it.sun.csr).within_alpha))) return e;
     if ((e = launch_point_masks(it.scene, it.geo, it.sdir, it.pts, it.pts_helio, it.weight, it.points, it.d_mask, it.d_origin, st)))
       return e;
   }

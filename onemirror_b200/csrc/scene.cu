@@ -1651,8 +1651,13 @@ qmcrt_status qmcrt_scene_grid_info(qmcrt_scene* s, qmcrt_grid_info* info) {
   std::memcpy(info->dims, s->gdims, sizeof(info->dims));
   info->cells = s->cells;
   int32_t tot = 0;
-  qmcrt_status e = ensure_grid(s, 0);  // the grid of a candidate trace's geometry may be unbuilt
-  if (e) return e;
+  if (!s->grid_forced && s->geom_version) {
+    // the grid of a candidate trace's geometry may be unbuilt: build it on the
+    // default stream once the device is idle (the trace's stream is not known)
+    QM_CUDA(cudaDeviceSynchronize());
+    qmcrt_status e = ensure_grid(s, 0);
+    if (e) return e;
+  }
   if (s->d_cell_start) QM_CUDA(cudaMemcpy(&tot, s->d_cell_start + s->cells, sizeof(int32_t), cudaMemcpyDeviceToHost));
   info->entries = tot;
   info->fine_div = s->fine_div;
