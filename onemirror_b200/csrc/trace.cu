@@ -14,6 +14,7 @@
 // so pixel indices agree with the FP64 oracle except where a hit lies within
 // ~1e-6 m of a pixel edge.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -71,15 +72,21 @@ __global__ void zero_maps_kernel(uint32_t* counts, float* energy, int64_t res, u
   if (i0 < 10 && i0 != 8) stats[i0] = 0ull;
 }
 
-static int g_sm_count = 0;
+// SM count of the current device, cached per device (the process may drive
+// several GPUs; the attribute query is cheap but not free per launch).
+static std::atomic<int> g_sm_count[64];
 static int sm_count() {
-  if (g_sm_count == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sm_count <= 0) g_sm_count = 148;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  int v = g_sm_count[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    int q = 0;
+    if (cudaDeviceGetAttribute(&q, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || q <= 0) q = 148;
+    g_sm_count[dev].store(q, std::memory_order_relaxed);
+    v = q;
   }
-  return g_sm_count;
+  return v;
 }
 
 template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
