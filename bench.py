@@ -3,8 +3,9 @@
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload mid|small|large] [--impl b200|reference]
 
 One step = one pass of the hot path over one batch: aim the field for the
-step's sun position, rebuild the grid, the per-heliostat occluder
-candidates and the per-point candidate masks on the GPU, trace 2^28 rays (Buie sampling, shadow and block tests,
+step's sun position, rebuild the per-heliostat occluder candidates (and the
+grid, where a candidate list overflows) and the per-point candidate masks on
+the GPU, trace 2^28 rays (Buie sampling, shadow and block tests,
 receiver deposition), scale the flux map and smooth the count map (trimmed
 mean).  Every step uses a fresh Philox stream
 and a slightly moved sun, so no output or geometry is reused.  Under torchrun
@@ -223,7 +224,8 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ arms
-STEP = ("aim + occluder candidates + grid build + point masks + trace + flux scaling + all-reduce of the maps "
+STEP = ("aim + occluder candidates + grid build (its passes build only when a candidate list overflows) + point "
+        "masks + trace + flux scaling + all-reduce of the maps "
         "(N > 1) + trimmed-mean smoothing of the summed count map; the Poisson sample points depend only on the "
         "mirror sizes and are sampled once per scene, before the timed steps")
 SUN_ELEV = {"small": 45.0, "mid": 30.0, "large": 20.0}
