@@ -342,10 +342,13 @@ __device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int whic
 
 // Receiver intersection in FP64; returns true on a hit and the pixel index
 // (-1 when the hit falls outside the map, QMCRT_QUIRK_PIXEL_EDGE only).
+// RT: the receiver type when known at compile time (QMCRT_RECEIVER_*), -1
+// to read it from the arguments.
+template <int RT = -1>
 __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int& pix, double* t_out = nullptr) {
   double u, v = 0.0;
   int col = -1;  // set directly by the cylinder
-  if (a.rtype == QMCRT_RECEIVER_CYLINDER) {
+  if (RT < 0 ? a.rtype == QMCRT_RECEIVER_CYLINDER : RT == QMCRT_RECEIVER_CYLINDER) {
     double ox = o.x - a.cyl[0], oz = o.z - a.cyl[2], R = a.cyl[3], H = a.cyl[4];
     double qa = d.x * d.x + d.z * d.z;
     if (qa < 1e-18) return false;
@@ -579,7 +582,7 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
 // CULL: 0 no culling, 1 vertical culling, 2 vertical culling on both levels
 // of a two-level grid, 3 the per-heliostat occluder candidates (Philox
 // sampling only: their cones bound the sampler's directions).
-template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep>
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep, int RT = -1>
 __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_tab, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit,
                                           const uint2* rk) {
@@ -639,7 +642,7 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_ta
     flag = QMCRT_RAY_SHADOWED;
   } else if (blocked) {
     flag = QMCRT_RAY_BLOCKED;
-  } else if (receiver_hit(a, o, rd, pix, &th)) {
+  } else if (receiver_hit<RT>(a, o, rd, pix, &th)) {
     flag = QMCRT_RAY_HIT;
     if (pix < 0) flag |= QMCRT_RAY_OFFMAP;
     else deposit(pix, a.atten ? e * atten_eta(a.atten, (float)th) : e);  // times eta(t) (:147)
@@ -668,8 +671,9 @@ __device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned lo
   }
 }
 
-// The plain tracer: one grid-stride pass over the rays of one trace.
-template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1>
+// The plain tracer: one grid-stride pass over the rays of one trace.  RT:
+// the receiver type, or -1 to read it from the arguments.
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1, int RT = -1>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
   pdl_wait();
   __shared__ float4 s_tab[kBuieRecords];
@@ -691,7 +695,7 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
     const uint64_t b64 = a.ray0 + ch * chunk;
     const uint32_t base = (uint32_t)b64, len = (uint32_t)(min(b64 + chunk, a.rays) - b64);
     for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
-      trace_ray<TABLES, RECORDS, STATS, CULL>(a, s_tab, base + j, fy0, fy1, c, dep, a.rk);
+      trace_ray<TABLES, RECORDS, STATS, CULL, GlobalDeposit, RT>(a, s_tab, base + j, fy0, fy1, c, dep, a.rk);
   }
   if (STATS) flush_counters(c, a.stats);
 }
