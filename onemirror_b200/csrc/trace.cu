@@ -89,9 +89,9 @@ static int sm_count() {
   return v;
 }
 
-template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1, int RT = -1>
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1, int RT = -1, bool LEAN = false>
 static cudaError_t launch_trace(const TraceArgs& a, cudaStream_t st) {
-  auto k = trace_kernel<TABLES, RECORDS, STATS, CULL, MINB, RT>;
+  auto k = trace_kernel<TABLES, RECORDS, STATS, CULL, MINB, RT, LEAN>;
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTraceThreads, 0);
   if (e != cudaSuccess) return e;
@@ -117,10 +117,18 @@ static cudaError_t dispatch(const TraceArgs& a, bool tables, bool records, bool 
                             cudaStream_t st) {
   // the production path (no records, no statistics) is compiled for 4 resident
   // CTAs per SM (64 registers); variant 3 keeps the unconstrained build
-  // (the candidate path, one build per receiver type)
-  if (variant != 3 && !tables && !records && !stats && cull == 3)
-    return a.rtype == QMCRT_RECEIVER_CYLINDER ? launch_trace<false, false, false, 3, 4, QMCRT_RECEIVER_CYLINDER>(a, st)
-                                              : launch_trace<false, false, false, 3, 4, QMCRT_RECEIVER_FLAT>(a, st);
+  // (the candidate path, one build per receiver type, and a lean one of each
+  // for the common case: power-of-two rays per point, point masks, no
+  // attenuation, no pixel-edge quirk)
+  if (variant != 3 && !tables && !records && !stats && cull == 3) {
+    const bool lean = a.rpp_shift >= 0 && a.point_mask && a.atten == QMCRT_ATTEN_NONE &&
+                      !(a.quirks & QMCRT_QUIRK_PIXEL_EDGE);
+    if (a.rtype == QMCRT_RECEIVER_CYLINDER)
+      return lean ? launch_trace<false, false, false, 3, 4, QMCRT_RECEIVER_CYLINDER, true>(a, st)
+                  : launch_trace<false, false, false, 3, 4, QMCRT_RECEIVER_CYLINDER>(a, st);
+    return lean ? launch_trace<false, false, false, 3, 4, QMCRT_RECEIVER_FLAT, true>(a, st)
+                : launch_trace<false, false, false, 3, 4, QMCRT_RECEIVER_FLAT>(a, st);
+  }
   if (variant != 3 && !tables && !records && !stats && cull == 2) return launch_trace<false, false, false, 2, 4>(a, st);
   if (variant != 3 && !tables && !records && !stats && cull) return launch_trace<false, false, false, 1, 4>(a, st);
   if (tables) return records ? dispatch2<true, true>(a, stats, cull, st) : dispatch2<true, false>(a, stats, cull, st);

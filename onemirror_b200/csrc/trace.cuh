@@ -344,7 +344,8 @@ __device__ __forceinline__ bool list_blocked(const TraceArgs& a, int h, int whic
 // (-1 when the hit falls outside the map, QMCRT_QUIRK_PIXEL_EDGE only).
 // RT: the receiver type when known at compile time (QMCRT_RECEIVER_*), -1
 // to read it from the arguments.
-template <int RT = -1>
+// LEAN: QMCRT_QUIRK_PIXEL_EDGE is off (the pixel is clamped to the map).
+template <int RT = -1, bool LEAN = false>
 __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int& pix, double* t_out = nullptr) {
   double u, v = 0.0;
   int col = -1;  // set directly by the cylinder
@@ -421,7 +422,7 @@ __device__ __forceinline__ bool receiver_hit(const TraceArgs& a, d3 o, d3 d, int
   }
   int row = (int)(u * a.res_y);  // rectgrid_raytracing.cu:144
   if (col < 0) col = (int)(v * a.res_x);
-  if (a.quirks & QMCRT_QUIRK_PIXEL_EDGE) {
+  if (!LEAN && (a.quirks & QMCRT_QUIRK_PIXEL_EDGE)) {
     if (row >= a.res_y || col >= a.res_x) {
       pix = -1;
       return true;
@@ -521,17 +522,19 @@ __device__ __forceinline__ void philox_samples(const TraceArgs& a, const float4*
 }
 
 // Returns false for a ray to skip (table mode with an out-of-range heliostat id).
-template <bool TABLES>
+// LEAN (Philox traces only): a power-of-two count of rays per point and the
+// per-point mask records present, so neither is tested per ray.
+template <bool TABLES, bool LEAN = false>
 __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_tab, uint32_t ray,
                                           RaySetup& R, const uint2* rk) {
-  const uint32_t g = a.rpp_shift >= 0 ? a.g_hi + (ray >> a.rpp_shift) : ray / (uint32_t)a.rpp;
+  const uint32_t g = (LEAN || a.rpp_shift >= 0) ? a.g_hi + (ray >> a.rpp_shift) : ray / (uint32_t)a.rpp;
   const uint32_t j = ray - g * (uint32_t)a.rpp;  // table mode (ray_hi 0)
   const int h = __ldg(a.point_helio + g);
   if (TABLES && (h < 0 || h >= a.n_helio)) return false;  // caller-provided ids: never index out of range
   R.h = h;
   R.xz = __ldg(a.point_xz + g);
   float sigma_h = 0.f;
-  if (a.point_mask) {
+  if (LEAN || a.point_mask) {
     const uint4 pm = __ldg(a.point_mask + g);
     R.reach = make_uint2(pm.x, pm.y);
     sigma_h = __uint_as_float(pm.z);
@@ -582,12 +585,15 @@ __device__ __forceinline__ bool ray_setup(const TraceArgs& a, const float4* s_ta
 // CULL: 0 no culling, 1 vertical culling, 2 vertical culling on both levels
 // of a two-level grid, 3 the per-heliostat occluder candidates (Philox
 // sampling only: their cones bound the sampler's directions).
-template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep, int RT = -1>
+// LEAN (Philox traces only): power-of-two rays per point, per-point masks,
+// no attenuation and no QMCRT_QUIRK_PIXEL_EDGE, so none of them is tested
+// per ray.
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, class Dep, int RT = -1, bool LEAN = false>
 __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_tab, uint32_t ray,
                                           float fy0, float fy1, RayCounters& c, const Dep& deposit,
                                           const uint2* rk) {
   RaySetup R;
-  if (!ray_setup<TABLES>(a, s_tab, ray, R, rk)) {
+  if (!ray_setup<TABLES, LEAN>(a, s_tab, ray, R, rk)) {
     if (RECORDS) {
       if (a.flags) a.flags[ray] = 0;
       if (a.pixel) a.pixel[ray] = -1;
@@ -642,10 +648,10 @@ __device__ __forceinline__ void trace_ray(const TraceArgs& a, const float4* s_ta
     flag = QMCRT_RAY_SHADOWED;
   } else if (blocked) {
     flag = QMCRT_RAY_BLOCKED;
-  } else if (receiver_hit<RT>(a, o, rd, pix, &th)) {
+  } else if (receiver_hit<RT, LEAN>(a, o, rd, pix, &th)) {
     flag = QMCRT_RAY_HIT;
     if (pix < 0) flag |= QMCRT_RAY_OFFMAP;
-    else deposit(pix, a.atten ? e * atten_eta(a.atten, (float)th) : e);  // times eta(t) (:147)
+    else deposit(pix, !LEAN && a.atten ? e * atten_eta(a.atten, (float)th) : e);  // times eta(t) (:147)
   }
   if (RECORDS) {
     if (a.flags) a.flags[ray] = flag;
@@ -672,8 +678,8 @@ __device__ __forceinline__ void flush_counters(const RayCounters& c, unsigned lo
 }
 
 // The plain tracer: one grid-stride pass over the rays of one trace.  RT:
-// the receiver type, or -1 to read it from the arguments.
-template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1, int RT = -1>
+// the receiver type, or -1 to read it from the arguments; LEAN: as trace_ray.
+template <bool TABLES, bool RECORDS, bool STATS, int CULL, int MINB = 1, int RT = -1, bool LEAN = false>
 __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceArgs a) {
   pdl_wait();
   __shared__ float4 s_tab[kBuieRecords];
@@ -695,7 +701,7 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) trace_kernel(const TraceA
     const uint64_t b64 = a.ray0 + ch * chunk;
     const uint32_t base = (uint32_t)b64, len = (uint32_t)(min(b64 + chunk, a.rays) - b64);
     for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
-      trace_ray<TABLES, RECORDS, STATS, CULL, GlobalDeposit, RT>(a, s_tab, base + j, fy0, fy1, c, dep, a.rk);
+      trace_ray<TABLES, RECORDS, STATS, CULL, GlobalDeposit, RT, LEAN>(a, s_tab, base + j, fy0, fy1, c, dep, a.rk);
   }
   if (STATS) flush_counters(c, a.stats);
 }
