@@ -417,6 +417,30 @@ def test_attenuation_equals_oracle(name):
     sc.close()
 
 
+@pytest.mark.parametrize("name", ["small", "mid", "large"])
+def test_lean_builds_equal_the_general_build(name):
+    """The production launch picks a build compiled for its receiver type and,
+    in the common case, a lean one (power-of-two rays per point, point masks,
+    no attenuation, no pixel-edge quirk: none of them tested per ray); kernel_variant 3 runs the general build,
+    which reads the receiver type and tests every case per ray.  (Per-ray
+    records and statistics take the general build too, so the production
+    launch is compared through its maps.)  The count maps are bit-identical
+    and the energy maps equal to the order of their float additions (flat
+    receivers on the small and mid fields, the cylinder on the large field)."""
+    w = W.small() if name == "small" else W.BUILDERS[name](rays=1 << 22)
+    sc = SolarScene.from_workload(w)
+    p = w.params
+    g = sc.trace(w.sun, p, records=False, stats=False)
+    cnt, en = g["counts"].clone(), g["energy"].clone()
+    p.kernel_variant = 3
+    g3 = sc.trace(w.sun, p, records=False, stats=False)
+    p.kernel_variant = 0
+    assert torch.equal(cnt, g3["counts"]) and int(cnt.sum()) > 0
+    # the energy map is a sum of float atomics: equal to float reordering
+    assert torch.allclose(en, g3["energy"], rtol=1e-5, atol=1e-6 * float(en.max()))
+    sc.close()
+
+
 @pytest.mark.parametrize("name,elev", [("small", 45.0), ("small", 12.0), ("mid", 30.0), ("mid", 8.0), ("large", 20.0)])
 def test_candidate_lists_equal_the_grid_walk(name, elev):
     """Philox rays test only their heliostat's occluder candidates (the
