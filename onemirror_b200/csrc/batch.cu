@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <vector>
 
 #include "internal.hpp"
@@ -74,7 +75,10 @@ struct PhiloxKeys {
   uint2 rk[10];
 };
 
-template <int T>
+// LEAN: every item has a flat receiver and takes the plain tracer's lean
+// build (power-of-two rays per point, point masks, no attenuation, no
+// quirks).
+template <int T, bool LEAN = false>
 __global__ void __launch_bounds__(kBatchThreads, 4)
     batch_trace_kernel(const TraceArgs* __restrict__ items, const unsigned long long* __restrict__ chunk_begin,
                        int n_items, uint32_t chunk_rays, unsigned long long total_chunks,
@@ -142,7 +146,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
       const TileDeposit<T> dep{s_cnt, s_en, s_anchor[2] ? s_anchor[0] : -(1 << 30), s_anchor[1], s_a.res_x,
                                s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, 3>(s_a, s_tab, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
+        trace_ray<false, false, false, 3, std::decay_t<decltype(dep)>, LEAN ? QMCRT_RECEIVER_FLAT : -1, LEAN>(
+            s_a, s_tab, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
       __syncthreads();
       if (s_anchor[2]) {  // flush the tile's non-zero pixels, then clear it
         for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
@@ -160,7 +165,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4)
     } else {
       const GlobalDeposit dep{s_a.counts, s_a.energy};
       for (unsigned long long r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-        trace_ray<false, false, false, 3>(s_a, s_tab, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
+        trace_ray<false, false, false, 3, std::decay_t<decltype(dep)>, LEAN ? QMCRT_RECEIVER_FLAT : -1, LEAN>(
+            s_a, s_tab, (uint32_t)r, fy0, fy1, cnt, dep, keys.rk);
     }
     __syncthreads();  // everyone is done with s_c / s_a / the tile before the next chunk
   }
@@ -197,6 +203,7 @@ static qmcrt_status balloc(T** p, size_t count) {
 }  // namespace qm
 
 struct qmcrt_batch {
+  bool lean = false;  // every item takes the lean build of the tracer (batch_trace_kernel's LEAN)
   struct Item {
     qmcrt_scene* scene = nullptr;
     qmcrt_sun sun{};
@@ -269,15 +276,24 @@ static cudaError_t batch_allow_tiles() {
   if (ce == cudaSuccess)
     ce = cudaFuncSetAttribute(batch_trace_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               batch_tile_bytes<48>());
+  if (ce == cudaSuccess)
+    ce = cudaFuncSetAttribute(batch_trace_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              batch_tile_bytes<32>());
+  if (ce == cudaSuccess)
+    ce = cudaFuncSetAttribute(batch_trace_kernel<48, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              batch_tile_bytes<48>());
   return ce;
 }
 
 // One launch of the batched kernel with a T x T tile (T = 0: none).
 template <int T>
 static cudaError_t launch_batch(qmcrt_batch* b, int ctas, int items, unsigned long long total, cudaStream_t st) {
-  batch_trace_kernel<T><<<ctas, kBatchThreads, batch_tile_bytes<T>(), st>>>(b->d_args, b->d_chunk_begin, items,
-                                                                           b->tuning.chunk_rays, total, b->d_counter,
-                                                                           b->keys);
+  if (b->lean)
+    batch_trace_kernel<T, true><<<ctas, kBatchThreads, batch_tile_bytes<T>(), st>>>(
+        b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays, total, b->d_counter, b->keys);
+  else
+    batch_trace_kernel<T><<<ctas, kBatchThreads, batch_tile_bytes<T>(), st>>>(
+        b->d_args, b->d_chunk_begin, items, b->tuning.chunk_rays, total, b->d_counter, b->keys);
   return cudaGetLastError();
 }
 
@@ -469,6 +485,12 @@ qmcrt_status qmcrt_batch_create(qmcrt_scene* const* scenes, int32_t n_scenes, co
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (ce != cudaSuccess) { e = cuda_error(ce, "batch upload"); goto fail; }
   }
+  // the lean build when every item allows it: flat receivers, power-of-two
+  // rays per point, no attenuation (items carry no quirks; every item has
+  // point masks)
+  b->lean = (params->rays_per_point & (params->rays_per_point - 1)) == 0 &&
+            params->attenuation == QMCRT_ATTEN_NONE;
+  for (auto& it : b->items) b->lean = b->lean && it.scene->rg.type == QMCRT_RECEIVER_FLAT;
   if ((e = upload_chunks(b, nullptr))) goto fail;
   *out = b;
   return QMCRT_OK;
