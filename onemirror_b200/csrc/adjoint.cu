@@ -238,7 +238,9 @@ __device__ __forceinline__ bool ray_hits(const TraceArgs& a, const RaySetup& R, 
 // only read.  The deposits are 64-bit fixed point with 2^-40 resolution,
 // added with integer atomics: the sums are exact in any order, so the
 // replayed loss is the same bit for bit from run to run.
-template <bool CULL, bool REPLAY = false>
+// LEAN: a power-of-two count of rays per point and the point masks present
+// (the plain tracer's lean ray setup).
+template <bool CULL, bool REPLAY = false, bool LEAN = false>
 __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_forward_kernel(const AdjArgs A) {
   __shared__ float4 s_tab[kBuieRecords];
   // block-private tile of the energy map: many heliostats aim at the same
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjCtasPerSm) adjoint_forward_ke
     const uint64_t r64 = i;
     if (REPLAY && A.tape[r64] == 0) continue;
     RaySetup R;
-    ray_setup<false>(a, s_tab, ray0 + i, R, a.rk);
+    ray_setup<false, LEAN>(a, s_tab, ray0 + i, R, a.rk);
     Refl g;
     double u, v, t;
     float e;
@@ -736,12 +738,14 @@ qmcrt_status qmcrt_adjoint_forward(qmcrt_scene* s, const qmcrt_sun* sun, const q
   A.tile_r0 = (s->rg.res_y - A.tile) / 2;
   A.tile_c0 = (s->rg.res_x - A.tile) / 2;
   const size_t tile_bytes = (size_t)A.tile * (A.tile + 1) * sizeof(float);  // rows T + 1 floats apart
-  QM_CUDA(cudaFuncSetAttribute(adjoint_forward_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes));
-  const int blocks = adj_blocks(adjoint_forward_kernel<true>, count, tile_bytes);
+  const bool lean = A.t.rpp_shift >= 0 && A.t.point_mask;
+  auto fwd = lean ? adjoint_forward_kernel<true, false, true> : adjoint_forward_kernel<true>;
+  QM_CUDA(cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_bytes));
+  const int blocks = adj_blocks(fwd, count, tile_bytes);
   *tape = t;  // from here on the caller owns it, also when a launch below fails
   QM_CUDA(cudaMemcpyAsync(t->d_buie, t->buie.host.data(), t->buie.host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   QM_CUDA(cudaMemsetAsync(t->d_energy, 0, res * sizeof(float), st));
-  adjoint_forward_kernel<true><<<blocks, kAdjThreads, tile_bytes, st>>>(A);
+  fwd<<<blocks, kAdjThreads, tile_bytes, st>>>(A);
   QM_CUDA(cudaGetLastError());
   return qm::tape_loss_pass(t, d_target, d_flux, loss, st);
 }
