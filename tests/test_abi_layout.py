@@ -87,3 +87,37 @@ def test_every_declared_function_has_a_prototype():
     text = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
     declared = set(re.findall(r"\b(qmcrt_\w+)\s*\(", text))
     assert declared == set(capi.PROTOTYPES), declared ^ set(capi.PROTOTYPES)
+
+
+def header_enum_values():
+    """{name: value} of every QMCRT_* enumerator of the header (values are
+    integer literals, shifts and ors)."""
+    text = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    out = {}
+    for body in re.findall(r"enum(?:\s+\w+)?\s*\{(.*?)\}", text, flags=re.S):
+        for item in body.split(","):
+            m = re.match(r"\s*(QMCRT_\w+)\s*=\s*([0-9xXa-fA-Fu<>| ()]+?)\s*$", item)
+            if m:
+                expr = re.sub(r"(?<=[0-9a-fA-F])[uU]\b", "", m.group(2))
+                assert re.fullmatch(r"[0-9xXa-fA-F<>| ()]+", expr), expr
+                out[m.group(1)] = eval(expr)  # noqa: S307  (checked above: literals, shifts and ors only)
+    return out
+
+
+def test_header_constants_equal_the_bindings():
+    """The binding's constants (QUIRK_*, TIMING_*, TRIM_*, ...) carry the
+    header's values, so a caller through ctypes passes the same bits as one
+    compiled against include/qmcrt.h."""
+    values = header_enum_values()
+    assert values["QMCRT_TIMING_ALL"] == values["QMCRT_TIMING_TRACE"] | values["QMCRT_TIMING_SETUP"] | \
+        values["QMCRT_TIMING_FINALIZE"]
+    checked = 0
+    for name, v in values.items():
+        short = name[len("QMCRT_"):]
+        if hasattr(capi, short):
+            assert getattr(capi, short) == v, name
+            checked += 1
+    for short in ("TIMING_TRACE", "TIMING_SETUP", "TIMING_FINALIZE", "TIMING_ALL", "TRIM_SORTED", "SMOOTH_COUNTS",
+                  "QUIRK_PIXEL_EDGE", "QUIRKS_REFERENCE"):
+        assert hasattr(capi, short) and "QMCRT_" + short in values, short
+    assert checked >= 20, checked
